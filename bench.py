@@ -1,0 +1,371 @@
+"""Benchmark of the rigid-fiber time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--fibers 4000] [--radius 18] [--precision auto|fp32|mixed_fp16|mixed_bf16]
+
+A "step" is the reference's time step (src/simulation.cu:286-329):
+assemble -> solve -> update velocities -> update fibers, on a seeded
+synthetic sphere layout (N fibers, centres uniform in a ball of radius R,
+min centre distance 0.2, orientations uniform on S^2; M=5, 8x3 quadrature,
+eps=0.01, dt=0.1, numerical integration, GMRES tol 1e-5).  Multi-GPU runs are
+independent replicas (one per rank, no collective on the data path); value
+is the whole-job fiber-steps/s over the max time across ranks.
+
+Prints ONE JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "fiber-steps/s @N=4000 mixed vs FP32 (err<=1e-4 vs FP64); served p50/p99 step lat"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fibers", type=int, default=4000)
+    ap.add_argument("--radius", type=float, default=18.0)
+    ap.add_argument("--precision", default="auto")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+def workload(args):
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    pos, ori = sphere_layout(args.fibers, args.radius, 0.2, seed=layout_seed(3, args.fibers))
+    return pos, ori
+
+
+def workload_name(args):
+    return ("N=%d fibers in a sphere of radius %g (min centre distance 0.2, S^2 orientations), M=5, 8x3 "
+            "quadrature, eps=0.01, dt=0.1, numerical integration, GMRES(10) tol 1e-5" % (args.fibers, args.radius))
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, want):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
+        self.pg.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (a C++ restatement of the reference's Fortran
+# path; the Fortran itself cannot be built here) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample(pos, ori, iterations, cycles, target_s):
+    from oracle import oracle as O
+    p = O.Params()
+    N = pos.shape[0]
+    R = 15 * N
+    threads = O.lib().rfo_num_threads()
+    rng = np.random.default_rng(0)
+    coeff = (1e-3 * rng.standard_normal(R)).astype(np.float32)
+
+    def rows_cost(ns):
+        t0 = time.perf_counter()
+        slab, _ = O.assemble_rows(pos, ori, p, 0, ns, dtype=np.float32)
+        t1 = time.perf_counter()
+        O.update_velocities(pos, ori, coeff, p, 0, ns, dtype=np.float32)
+        t2 = time.perf_counter()
+        xg = rng.standard_normal(R).astype(np.float32)
+        reps = 3
+        t3 = time.perf_counter()
+        for _ in range(reps):
+            O.gemv(slab, xg)
+        t4 = time.perf_counter()
+        return t1 - t0, t2 - t1, (t4 - t3) / reps
+
+    ns = max(1, min(N, threads))
+    ta, tv, tg = rows_cost(ns)
+    per = (ta + tv + (iterations + cycles) * tg) / ns
+    ns2 = int(min(N, max(ns, target_s / max(per, 1e-9))))
+    if ns2 > ns:
+        ns = ns2
+        ta, tv, tg = rows_cost(ns)
+    scale = N / ns
+    step_s = scale * (ta + tv + (iterations + cycles) * tg)
+    t0 = time.perf_counter()
+    z = np.zeros((N, 3), np.float32)
+    O.update_fibers(False, 0.1, pos.astype(np.float32), pos.astype(np.float32), ori.astype(np.float32),
+                    ori.astype(np.float32), z, z, z, z)
+    step_s += time.perf_counter() - t0
+    return {
+        "value": N / step_s, "unit": "fiber-steps/s", "cores": threads, "kind": "port",
+        "sample": ("C++ restatement of the reference's Fortran/OpenMP step (FP32, OpenMP over fibers): assembly and "
+                   "velocity rows of %d of %d fibers and a dense FP32 gemv over that row slab, scaled by N/%d; "
+                   "%d GMRES matvecs per step (iterations + restart residuals, from the GPU run)"
+                   % (ns, N, ns, iterations + cycles)),
+        "seconds_per_step": step_s,
+        "breakdown_s": {"assemble_system": scale * ta, "update_velocities": scale * tv,
+                        "solve_system": scale * (iterations + cycles) * tg},
+    }
+
+
+def run_reference(args):
+    pos, ori = workload(args)
+    iters = 20
+    cycles = 3
+    for _ in range(args.warmup):
+        cpu_sample(pos, ori, iters, cycles, 2.0)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_sample(pos, ori, iters, cycles, max(1.0, args.cpu_seconds / 2)))
+    v = statistics.median(r["value"] for r in vals)
+    last = vals[-1]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "fiber-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.fibers / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(args), "fibers": args.fibers, "radius": args.radius,
+                   "assumed_gmres_matvecs_per_step": iters + cycles},
+        "cpu_baseline": {k: last[k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "fiber-steps/s"},
+        "e2e": {"value": v, "unit": "fiber-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, dist):
+    import ctypes
+
+    import torch
+
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200 import _capi as C
+
+    torch.cuda.set_device(dist.local)
+    pos, ori = workload(args)
+    N = args.fibers
+    precision = "fp32" if args.precision == "auto" else args.precision
+    cfg = Config(precision=precision)
+    sim = Simulation(cfg, pos, ori)
+    lib = C.load()
+    sp = ctypes.c_void_p()
+    lib.rf_get_stream(sim._h, ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value)
+
+    # warm-up
+    for t in range(args.warmup):
+        sim.step(t)
+    # device-timed region
+    lib.rf_set_profiling(sim._h, 1)
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stage = {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0}
+    iters, launches, mv_launches, mv_ms, restarts = 0, 0, 0, 0.0, 0
+    for t in range(args.warmup, args.warmup + args.steps):
+        sim.step(t)
+        st = sim.stats()
+        for k in stage:
+            stage[k] += st["ms_" + k]
+        iters += st["iterations"]
+        restarts += st["restarts"]
+        launches += st["kernel_launches"]
+        nl, tm = ctypes.c_int(), ctypes.c_double()
+        lib.rf_matvec_profile(sim._h, ctypes.byref(nl), ctypes.byref(tm))
+        mv_launches += nl.value
+        mv_ms += tm.value
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    lib.rf_set_profiling(sim._h, 0)
+    dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ms_max = dist.max(ms)
+    total_fiber_steps = dist.sum(N * args.steps)
+    value = total_fiber_steps / (ms_max / 1000.0)
+
+    # end-to-end through the C ABI with host buffers: every step copies the
+    # fiber state in from pinned host memory and the new state out
+    hpos = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).pin_memory()
+    hori = torch.from_numpy(np.ascontiguousarray(ori, np.float64)).pin_memory()
+    out_pos = torch.empty_like(hpos).pin_memory()
+    out_ori = torch.empty_like(hori).pin_memory()
+    sim2 = Simulation(cfg, pos, ori)
+    sim2.step(0)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for t in range(1, 1 + args.steps):
+        C.check(lib.rf_set_state(sim2._h, ctypes.c_void_p(hpos.data_ptr()), ctypes.c_void_p(hori.data_ptr())),
+                "rf_set_state")
+        sim2.step(t)
+        C.check(lib.rf_get_state(sim2._h, ctypes.c_void_p(out_pos.data_ptr()), ctypes.c_void_p(out_ori.data_ptr())),
+                "rf_get_state")
+    torch.cuda.synchronize()
+    e2e_s = dist.max(time.perf_counter() - t0)
+    e2e_value = total_fiber_steps / e2e_s
+    sim2.close()
+    # bytes the C ABI moves per step: rf_set_state uploads double4 prev+cur
+    # position/orientation and their float4 copies; rf_get_state reads double4 pos/ori
+    h2d = N * (2 * 2 * 32 + 2 * 16)
+    d2h = N * 2 * 32
+
+    R = 15 * N
+    hbm, peak_kind = peaks()
+    mv_avg_ms = mv_ms / max(mv_launches, 1)
+    bytes_per_matvec = 4.0 * R * R
+    achieved = bytes_per_matvec / (mv_avg_ms / 1000.0) / 1e9 if mv_launches else None
+    roof = {"kernel": "k_gemv_cm_f32 (dense FP32 column-major matvec, GMRES)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "algorithmic_bytes_per_launch": bytes_per_matvec, "avg_launch_ms": mv_avg_ms,
+            "launches": mv_launches, "share_of_step_time": mv_ms / ms if ms else None}
+    out = {
+        "metric": METRIC, "value": value, "unit": "fiber-steps/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if precision == "fp32" else "f16/bf16 storage, f32 accumulate, f64 refine",
+        "data": "synthetic",
+        "config": {"workload": workload_name(args), "fibers": N, "radius": args.radius, "precision": precision,
+                   "parallelism": "replicas x%d" % dist.world,
+                   "l2": "inputs larger than L2: the %.1f GB matrix is re-assembled and re-read every step"
+                         % (4.0 * R * R / 1e9)},
+        "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
+        "gmres_iterations_per_step": iters / args.steps, "gmres_restarts_per_step": restarts / args.steps,
+        "roofline": roof, "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "fiber-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+    }
+    sim.close()
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_sample(pos, ori, max(1, iters // args.steps), max(1, restarts // args.steps),
+                                         args.cpu_seconds)
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # the reference arm runs on host cores only; ranks > 0 exit without work
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference(args)
+        return
+    dist = Dist(args.gpus)
+    try:
+        run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

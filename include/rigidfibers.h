@@ -1,0 +1,170 @@
+/*
+ * rigidfibers.h -- C ABI of the B200 rigid-fiber time step.
+ *
+ * Drop-in boundary for the reference's per-step seam, the C++ class
+ * `Simulation` of ericwolter/rigidfibers (src/simulation.h:38-97), whose
+ * step() (src/simulation.cu:286-329) calls assembleSystem / solveSystem /
+ * updateVelocities / updateFibers.  The reference has no FFI; this header is
+ * what such an FFI binds (ctypes / cgo / JNI / N-API stubs in INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every function returns an int status (RF_OK == 0).  rf_last_error()
+ *    returns a message for the last failure on the calling thread.
+ *  - Host arrays are owned by the caller and copied in or out; the handle
+ *    owns all device memory and one CUDA stream.  A handle is not
+ *    thread-safe; distinct handles may be used from distinct threads.
+ *  - Fiber arrays are 3N doubles, fiber-major xyz (the layout of the
+ *    reference's Fortran path and of its validate dumps,
+ *    fortran/fibers.f95:26-35,205-303).  The force-coefficient vector b / x
+ *    has R = 3*M*N entries, index j*3M + 3k + d.  The dense matrix A is
+ *    column-major R x R, entry (r, c) at A[r + c*R] (src/simulation.cu:64-110).
+ */
+#ifndef RIGIDFIBERS_H_
+#define RIGIDFIBERS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference prints or asserts instead
+ * (src/common.h:11-25, src/simulation.cu:414,441-442). */
+enum rf_status {
+  RF_OK = 0,
+  RF_E_INPUT = 1,       /* invalid argument, size or configuration */
+  RF_E_CUDA = 2,        /* CUDA runtime error */
+  RF_E_OOM = 3,         /* device allocation failed */
+  RF_E_NOCONV = 4,      /* iterative solver hit its iteration limit */
+  RF_E_NAN = 5,         /* NaN / Inf in b, x or the velocities */
+  RF_E_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+  RF_E_UNSUPPORTED = 7, /* combination not built (e.g. M > 8) */
+  RF_E_STATE = 8,       /* call out of order (e.g. solve before assemble) */
+  RF_E_SINGULAR = 9     /* direct solver met a zero pivot */
+};
+
+/* `--gmres | --bicgstab | --magma` of fibers_runner.py (fibers_runner.py:97-100). */
+enum rf_solver { RF_SOLVER_GMRES = 0, RF_SOLVER_BICGSTAB = 1, RF_SOLVER_DIRECT = 2 };
+
+/* `--numerical | --analytical` (fibers_runner.py:102-104). */
+enum rf_integration { RF_NUMERICAL = 0, RF_ANALYTICAL = 1 };
+
+/* Storage / arithmetic of the solve.
+ *  RF_PREC_FP32:  dense FP32 A (the reference's layout), FP32 Krylov solve.
+ *  RF_PREC_MIXED_FP16 / _BF16: structured operator A = I + C T, T stored once
+ *      per unordered fiber pair in FP32 and in 16 bits; the Krylov matvec runs
+ *      on the 16-bit copy with FP32 accumulation inside FP64-residual
+ *      iterative refinement (numerical integration only). */
+enum rf_precision { RF_PREC_FP32 = 0, RF_PREC_MIXED_FP16 = 1, RF_PREC_MIXED_BF16 = 2 };
+
+/* Mirrors the reference's .ini keys (tests/config.ini:18-37, read by
+ * runner/cuda_runner.py:18-47) plus the runtime choices the reference made
+ * at compile time (runner/cuda_runner.py:49-117). */
+typedef struct rf_config {
+  int number_of_timesteps;                      /* [RUN] */
+  int state_save_interval;
+  int velocity_save_interval;
+  double timestep;                              /* [SIMULATION] */
+  double slenderness;
+  int number_of_terms_in_force_expansion;       /* M, 1..8 */
+  int number_of_quadrature_intervals;           /* Q = 3 * intervals */
+  int number_of_quadrature_points_per_interval; /* must be 3 */
+  int gmres_restart;                            /* [GMRES] */
+  int gmres_max_iterations;
+  double gmres_tolerance;
+  int bicgstab_max_iterations;                  /* [BICGSTAB] */
+  double bicgstab_tolerance;
+  int solver;                                   /* enum rf_solver */
+  int integration;                              /* enum rf_integration */
+  int precision;                                /* enum rf_precision */
+  int velocity_integration;                     /* -1: same as `integration` (what
+                                                   the reference's golden files were
+                                                   made with); 0 numerical (what its
+                                                   committed code does); 1 analytical */
+  double refinement_tolerance;                  /* mixed precision: outer target on
+                                                   ||b - A x|| / ||b|| */
+  int refinement_max_iterations;
+} rf_config;
+
+typedef struct rf_stats {
+  int iterations;            /* Krylov iterations of the last solve (inner total) */
+  int restarts;
+  int refinement_steps;      /* outer FP64-residual corrections (mixed precision) */
+  double relative_residual;  /* ||b - A x|| / ||b|| at exit, FP64 */
+  /* milliseconds of the last call of each stage, CUDA events on the handle's
+   * stream (names as in src/performance.cc: assemble_system, solve_system,
+   * update_velocities, update_fibers) */
+  double ms_assemble_system;
+  double ms_solve_system;
+  double ms_update_velocities;
+  double ms_update_fibers;
+  int64_t device_bytes;      /* device memory held by the handle */
+  int kernel_launches;       /* kernels launched by the last rf_step */
+} rf_stats;
+
+typedef struct rf_handle rf_handle;
+
+/* Defaults of tests/config.ini with GMRES, numerical, FP32. */
+int rf_config_default(rf_config* cfg);
+
+/* Replaces Simulation::Simulation + initializeGPUMemory +
+ * writeFiberStateToDevice + precomputeLegendrePolynomials
+ * (src/simulation.cu:44-284).  pos / ori: 3N doubles. */
+int rf_create(const rf_config* cfg, int number_of_fibers, const double* pos, const double* ori,
+              rf_handle** out);
+int rf_destroy(rf_handle* h);
+
+/* Simulation::assembleSystem (src/simulation.cu:331-399). */
+int rf_assemble(rf_handle* h);
+/* Simulation::solveSystem (src/simulation.cu:401-445). */
+int rf_solve(rf_handle* h);
+/* Simulation::updateVelocities (src/simulation.cu:447-489). */
+int rf_update_velocities(rf_handle* h);
+/* Simulation::updateFibers (src/simulation.cu:491-528); first_step selects
+ * the Euler step of the first time step.  Also rotates the
+ * previous/current/next buffers (src/simulation.cu:307-311). */
+int rf_update_fibers(rf_handle* h, int first_step);
+/* Simulation::step (src/simulation.cu:286-329): the four stages above. */
+int rf_step(rf_handle* h, int current_timestep);
+/* rf_step over `nsteps` steps starting at `first_timestep`. */
+int rf_run(rf_handle* h, int first_timestep, int nsteps);
+
+/* State and dumps (src/simulation.cu:530-822 write these to files). */
+int rf_get_state(rf_handle* h, double* pos, double* ori);
+int rf_set_state(rf_handle* h, const double* pos, const double* ori);
+int rf_get_velocities(rf_handle* h, double* tvel, double* rvel);
+/* b after assemble (before solve); A (R*R floats, column-major) only in
+ * RF_PREC_FP32 mode, pass NULL to skip it. */
+int rf_get_system(rf_handle* h, float* A, double* b);
+/* x, the force coefficients, after solve. */
+int rf_get_solution(rf_handle* h, double* x);
+int rf_last_stats(rf_handle* h, rf_stats* s);
+int rf_get_config(rf_handle* h, rf_config* cfg);
+int rf_number_of_fibers(rf_handle* h);
+
+/* The handle's CUDA stream (cudaStream_t), for callers that order their
+ * own work or events after the handle's (the reference used the default
+ * stream synchronously, src/simulation.cu). */
+int rf_get_stream(rf_handle* h, void** stream);
+/* Per-launch timing of the solve's matvec kernels (CUDA events around each
+ * launch, the role of src/performance.cc's trackers for that kernel).
+ * rf_matvec_profile returns launches and summed milliseconds of the last
+ * solve. */
+int rf_set_profiling(rf_handle* h, int enable);
+int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
+
+/* Device-pointer entry points (no host copies; pointers are device memory
+ * on the current device, the stream may be 0).
+ * rf_dense_matvec: y = A x for column-major FP32 A (R x R); replaces the
+ * ViennaCL prod(A, x) behind the reference's GMRES
+ * (lib/viennacl/linalg/cuda/matrix_operations_col.hpp:1251-1278). */
+int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream);
+
+const char* rf_status_string(int status);
+const char* rf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIGIDFIBERS_H_ */

@@ -1,0 +1,339 @@
+// Assembly of the rigid-fiber linear system (numerical inner integrals).
+//
+// Reference: fortran/assemble_matrix.incl:1-161 with
+// fortran/compute_inner_integral_numerically.incl:1-40, and the CUDA kernels
+// src/kernels/assemble_system_2D.cu:8-367 + compute_inner_integral_numerically.cu.
+//
+// What is computed is the reference's: for every ordered pair (i, j), i != j,
+//   T^{ij}_{ki,kj} = sum_qi sum_qj W[ki][qi] K(R_ij(qi,qj)) W[kj][qj]      (3x3 sym)
+// with W[k][q] = w_q P_k(s_q), then the 15x15 block A_(i,j) = C_i T^{ij} and
+// b_i -= C_i T^{ij}_{.,P0} F/2, where C_i is D1 t t^T (force index 0) or
+// gamma_k (I - E_k t t^T).  How it is computed is not the reference's:
+//  * K is even in R, so T^{ji}_{kj,ki} = T^{ij}_{ki,kj}: one CTA tile of
+//    unordered fiber pairs evaluates K once per (qi, qj) and writes both
+//    blocks (i,j) and (j,i)  -- half the kernel evaluations;
+//  * the reference re-evaluates K once per k_j (M times); here once;
+//  * the quadrature is mirror-symmetric (s_{Q-1-q} = -s_q, w equal, P_k of
+//    parity k), so both contractions fold q with Q-1-q into an even and an
+//    odd part and use half the multiply-adds;
+//  * b is reduced deterministically (per-tile partial rows, then a fixed
+//    order sum) instead of float atomics.
+// Layout: A column-major with leading dimension lda >= R (padded to 32 so
+// every column starts on a 128-byte boundary), entry (r, c) at A[r + c*lda].
+#include "rf_common.cuh"
+#include "rf_kernels.cuh"
+
+namespace rf {
+
+// Decode a linear index over the upper triangle (I <= J) of T x T tiles.
+__device__ __forceinline__ void tile_pair(int64_t L, int& I, int& J) {
+  int64_t j = (int64_t)((sqrt(8.0 * (double)L + 1.0) - 1.0) * 0.5);
+  while ((j + 1) * (j + 2) / 2 <= L) ++j;
+  while (j * (j + 1) / 2 > L) --j;
+  J = (int)j;
+  I = (int)(L - j * (j + 1) / 2);
+}
+
+template <int M, int Q>
+struct AsmShape {
+  static constexpr int TI = 192 / Q;     // fibers per tile side
+  static constexpr int U = TI * Q;       // (fiber, quadrature point) units = threads used
+  static constexpr int K1 = M + 1;       // P_0..P_M
+  static constexpr int NC = 6 * K1;      // G columns per unit
+  static constexpr int H = Q / 2;        // folded quadrature points
+  // dynamic shared memory: G columns per unit, then the T blocks (6 floats each)
+  static constexpr size_t kGBytes = sizeof(float) * NC * U;
+  static constexpr size_t kTBytes = sizeof(float) * TI * K1 * K1 * 6;
+  static constexpr size_t kSmem = kGBytes + kTBytes;
+};
+
+// One CTA = one tile pair (I, J), I <= J, of TI x TI fibers.  192 threads:
+// thread u < TI*Q owns (fiber il = u / Q of tile I, quadrature point qi).
+template <int M, int Q>
+__global__ void __launch_bounds__(192, 3)
+k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+                     float* __restrict__ A, int64_t lda, float* __restrict__ bpart, int64_t R) {
+  using S = AsmShape<M, Q>;
+  constexpr int TI = S::TI, K1 = S::K1, NC = S::NC, H = S::H;
+  constexpr int M3 = 3 * M;
+  static_assert(Q % 2 == 0, "mirror folding needs an even number of quadrature points");
+
+  __shared__ float4 sPj[TI][Q];          // x_j + s_q t_j for the J tile
+  __shared__ float4 sTi[TI], sTj[TI];    // orientations
+  extern __shared__ __align__(16) float smem_dyn[];
+  float (*sG)[S::U] = reinterpret_cast<float (*)[S::U]>(smem_dyn);                            // [NC][U]
+  float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(smem_dyn + NC * S::U);      // [TI][K1][K1][6]
+  __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
+  __shared__ float sbJ[TI][M3];
+
+  int I, J;
+  tile_pair(blockIdx.x, I, J);
+  const bool diag = (I == J);
+  const int tid = threadIdx.x;
+  const int i0 = I * TI, j0 = J * TI;
+
+  if (tid < M) { sCoef[tid] = tab.gamma[tid]; sEig[tid] = tab.eigen[tid]; }
+  if (tid < TI) {
+    const int i = min(i0 + tid, N - 1), j = min(j0 + tid, N - 1);
+    sTi[tid] = ori[i];
+    sTj[tid] = ori[j];
+  }
+  if (tid < S::U) {
+    const int jl = tid / Q, q = tid % Q;
+    const int j = min(j0 + jl, N - 1);
+    const float4 x = pos[j], t = ori[j];
+    const float s = tab.pts[q];
+    sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
+  }
+  for (int k = tid; k < TI * M3; k += blockDim.x) (&sbJ[0][0])[k] = 0.f;
+
+  // own unit
+  const int il = tid / Q, qi = tid % Q;
+  const int i = i0 + il;
+  const bool unit_ok = (tid < S::U) && (i < N);
+  float pix = 0.f, piy = 0.f, piz = 0.f;
+  if (unit_ok) {
+    const float4 x = pos[i], t = ori[i];
+    const float s = tab.pts[qi];
+    pix = fmaf(s, t.x, x.x); piy = fmaf(s, t.y, x.y); piz = fmaf(s, t.z, x.z);
+  }
+  const float e2 = tab.e2;
+  const float e2x3 = -3.f * e2;
+
+  // b_i accumulator for task (il_b, kI) = (tid / M, tid % M)
+  float bacc[3] = {0.f, 0.f, 0.f};
+  __syncthreads();
+
+  const int jcount = min(TI, N - j0);
+  for (int jl = 0; jl < jcount; ++jl) {
+    const bool pair_ok = unit_ok && (!diag || il < jl);
+    // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj], mirror-folded over qj
+    float g[6][K1];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+#pragma unroll
+      for (int k = 0; k < K1; ++k) g[c][k] = 0.f;
+    if (pair_ok) {
+#pragma unroll
+      for (int q = 0; q < H; ++q) {
+        float Kp[6], Km[6];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          const float4 pj = sPj[jl][side == 0 ? q : Q - 1 - q];
+          const float rx = pix - pj.x, ry = piy - pj.y, rz = piz - pj.z;
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float inv = rsqrtf(r2);
+          const float inv2 = inv * inv;
+          const float inv3 = inv2 * inv;
+          const float inv5 = inv3 * inv2;
+          const float a = fmaf(e2, inv3, inv);        // inv + 2eps^2 inv^3
+          const float bb = fmaf(e2x3, inv5, inv3);    // inv^3 - 6eps^2 inv^5
+          const float bx = bb * rx, by = bb * ry, bz = bb * rz;
+          float* K = side == 0 ? Kp : Km;
+          K[0] = fmaf(bx, rx, a);
+          K[1] = fmaf(by, ry, a);
+          K[2] = fmaf(bz, rz, a);
+          K[3] = bx * ry;
+          K[4] = bx * rz;
+          K[5] = by * rz;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const float ev = Kp[c] + Km[c], od = Kp[c] - Km[c];
+#pragma unroll
+          for (int k = 0; k < K1; ++k) g[c][k] = fmaf((k & 1) ? od : ev, tab.W[k][q], g[c][k]);
+        }
+      }
+    }
+    if (tid < S::U) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+#pragma unroll
+        for (int k = 0; k < K1; ++k) sG[c * K1 + k][tid] = g[c][k];
+    }
+    __syncthreads();
+
+    // ---- phase 2: T[ki][kj][c] = sum_qi W[ki][qi] G[qi][c][kj], folded over qi
+    for (int task = tid; task < TI * NC; task += blockDim.x) {
+      const int tl = task / NC, col = task % NC;
+      const int c = col / K1, kj = col % K1;
+      const float* gp = &sG[col][tl * Q];
+      float acc[K1];
+#pragma unroll
+      for (int k = 0; k < K1; ++k) acc[k] = 0.f;
+#pragma unroll
+      for (int q = 0; q < H; ++q) {
+        const float lo = gp[q], hi = gp[Q - 1 - q];
+        const float ev = lo + hi, od = lo - hi;
+#pragma unroll
+        for (int k = 0; k < K1; ++k) acc[k] = fmaf((k & 1) ? od : ev, tab.W[k][q], acc[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < K1; ++k) sT[tl][k][kj][c] = acc[k];
+    }
+    __syncthreads();
+
+    // ---- phase 3a: block (i, j) -- rows of fiber i, columns of fiber j
+    const int j = j0 + jl;
+    {
+      for (int task = tid; task < TI * M * M; task += blockDim.x) {
+        const int kJp = task / (TI * M), rem = task % (TI * M);
+        const int tl = rem / M, kIp = rem % M;
+        const int ii = i0 + tl;
+        if (ii >= N || (diag && tl > jl)) continue;
+        float* dst = A + (int64_t)(i0 * M3 + 3 * rem) + (int64_t)(j * M3 + 3 * kJp) * lda;
+        if (diag && tl == jl) {
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) dst[a + b * lda] = (kIp == kJp && a == b) ? 1.f : 0.f;
+          continue;
+        }
+        const float* T6 = sT[tl][kIp + 1][kJp + 1];
+        const float4 ti = sTi[tl];
+        const float t3[3] = {ti.x, ti.y, ti.z};
+        float Qv[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          Qv[b] = sym_get(T6, b, 0) * t3[0] + sym_get(T6, b, 1) * t3[1] + sym_get(T6, b, 2) * t3[2];
+        const float coef = sCoef[kIp], E = sEig[kIp];
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            dst[a + b * lda] = kIp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
+      }
+    }
+    // ---- phase 3b: block (j, i) -- rows of fiber j, columns of fiber i
+    {
+      const float4 tj = sTj[jl];
+      const float t3[3] = {tj.x, tj.y, tj.z};
+      for (int task = tid; task < TI * M * M; task += blockDim.x) {
+        const int tl = task / (M * M), rem = task % (M * M);
+        const int kIp = rem / M, kJp = rem % M;
+        const int ii = i0 + tl;
+        if (ii >= N || (diag && tl >= jl)) continue;
+        float* dst = A + (int64_t)(j * M3 + 3 * kJp) + (int64_t)(ii * M3 + 3 * kIp) * lda;
+        const float* T6 = sT[tl][kIp + 1][kJp + 1];
+        float Qv[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          Qv[b] = sym_get(T6, b, 0) * t3[0] + sym_get(T6, b, 1) * t3[1] + sym_get(T6, b, 2) * t3[2];
+        const float coef = sCoef[kJp], E = sEig[kJp];
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            dst[a + b * lda] = kJp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
+      }
+    }
+    // ---- phase 3c: right-hand side, b_i from (i,j) and b_j from (j,i)
+    const float fz = tab.fz_half;
+    if (tid < TI * M) {
+      const int tl = tid / M, kIp = tid % M;
+      if (i0 + tl < N && (!diag || tl < jl)) {
+        const float* T6 = sT[tl][kIp + 1][0];
+        const float4 ti = sTi[tl];
+        const float t3[3] = {ti.x, ti.y, ti.z};
+        const float TF[3] = {T6[4] * fz, T6[5] * fz, T6[2] * fz};   // T (0,0,fz)
+        const float QF = TF[0] * t3[0] + TF[1] * t3[1] + TF[2] * t3[2];
+        const float coef = sCoef[kIp], E = sEig[kIp];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) bacc[a] -= kIp == 0 ? coef * t3[a] * QF : coef * (TF[a] - E * t3[a] * QF);
+      }
+    }
+    if (tid < M) {
+      const int kJp = tid;
+      const float4 tj = sTj[jl];
+      const float t3[3] = {tj.x, tj.y, tj.z};
+      const float coef = sCoef[kJp], E = sEig[kJp];
+      float s[3] = {0.f, 0.f, 0.f};
+      for (int tl = 0; tl < TI; ++tl) {
+        if (i0 + tl >= N || (diag && tl >= jl)) continue;
+        const float* T6 = sT[tl][0][kJp + 1];
+        const float TF[3] = {T6[4] * fz, T6[5] * fz, T6[2] * fz};
+        const float QF = TF[0] * t3[0] + TF[1] * t3[1] + TF[2] * t3[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s[a] -= kJp == 0 ? coef * t3[a] * QF : coef * (TF[a] - E * t3[a] * QF);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) sbJ[jl][3 * kJp + a] += s[a];
+    }
+    __syncthreads();
+  }
+
+  // ---- partial right-hand sides: bpart[X][rows of Y] written exactly once
+  if (tid < TI * M) {
+    const int tl = tid / M;
+    if (i0 + tl < N) {
+      float v[3] = {bacc[0], bacc[1], bacc[2]};
+      if (diag) {
+        const int kIp = tid % M;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) v[a] += sbJ[tl][3 * kIp + a];
+      }
+      float* dst = bpart + (int64_t)J * R + (int64_t)i0 * M3 + 3 * tid;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) dst[a] = v[a];
+    }
+  }
+  if (!diag) {
+    for (int k = tid; k < TI * M3; k += blockDim.x) {
+      const int jl = k / M3;
+      if (j0 + jl < N) bpart[(int64_t)I * R + (int64_t)j0 * M3 + k] = (&sbJ[0][0])[k];
+    }
+  }
+}
+
+// b[r] = sum over tiles X of bpart[X][r], fixed order.
+__global__ void k_reduce_rows(const float* __restrict__ part, int nparts, int64_t R, float* __restrict__ out) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int p = 0; p < nparts; ++p) s += part[(int64_t)p * R + r];
+    out[r] = s;
+  }
+}
+
+int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st);
+
+template <int M, int Q>
+static int launch_assemble_numerical_mq(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
+                                        int64_t lda, float* bpart, float* b, cudaStream_t st) {
+  using S = AsmShape<M, Q>;
+  const int64_t T = ceil_div(N, S::TI);
+  const int64_t ntp = T * (T + 1) / 2;
+  const int64_t R = (int64_t)3 * M * N;
+  static bool attr_set = false;  // per process; the attribute is per function
+  if (!attr_set) {
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_numerical<M, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)S::kSmem));
+    attr_set = true;
+  }
+  k_assemble_numerical<M, Q><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, A, lda, bpart, R);
+  RF_LAUNCH_CHECK();
+  return launch_reduce_rows(bpart, (int)T, R, b, st);
+}
+
+int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st) {
+  const int threads = 256;
+  const int blocks = (int)std::min<int64_t>(ceil_div(R, threads), 148 * 8);
+  k_reduce_rows<<<blocks, threads, 0, st>>>(part, nparts, R, out);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int assemble_tiles(int M, int Q, int N) {
+  return (int)ceil_div(N, 192 / Q);
+}
+
+int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
+                              int64_t lda, float* bpart, float* b, cudaStream_t st) {
+#define RF_ASM_CASE(MM, QQ) \
+  if (tab.M == MM && tab.Q == QQ) return launch_assemble_numerical_mq<MM, QQ>(tab, N, pos, ori, A, lda, bpart, b, st);
+  RF_FOR_EACH_MQ(RF_ASM_CASE)
+#undef RF_ASM_CASE
+  set_last_error_str("assemble: (M, Q) combination not instantiated");
+  return RF_E_UNSUPPORTED;
+}
+
+}  // namespace rf

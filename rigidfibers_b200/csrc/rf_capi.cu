@@ -1,0 +1,585 @@
+// C ABI of the rigid-fiber time step: the handle owns the device state and
+// one stream, and runs the reference's step
+// (src/simulation.cu:286-329: assembleSystem -> solveSystem ->
+// updateVelocities -> updateFibers -> buffer rotation).
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "rf_common.cuh"
+#include "rf_kernels.cuh"
+#include "rf_krylov.cuh"
+
+namespace rf {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const char* msg, const char* file, int line) {
+  g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
+}
+void set_last_error_str(const char* msg) { g_last_error = msg; }
+
+bool mq_supported(int M, int Q) {
+#define RF_MQ_CASE(MM, QQ) \
+  if (M == MM && Q == QQ) return true;
+  RF_FOR_EACH_MQ(RF_MQ_CASE)
+#undef RF_MQ_CASE
+  return false;
+}
+
+// fortran/fibers.f95:141-145,353-476: quadrature, Legendre, lambda and E_k
+// in double, then the working-precision constants as the REAL*4 program
+// forms them (c, d, D1 and gamma in single precision).
+static Tables make_tables(const rf_config& c) {
+  Tables t;
+  std::memset(&t, 0, sizeof(t));
+  const int M = c.number_of_terms_in_force_expansion;
+  const int nint = c.number_of_quadrature_intervals;
+  const int Q = 3 * nint;
+  t.M = M;
+  t.Q = Q;
+  const double p[3] = {-std::sqrt(15.0) / 5.0, 0.0, std::sqrt(15.0) / 5.0};
+  const double w[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  const double h = 2.0 / nint;
+  double lower = -1.0;
+  std::vector<double> pts, wts;
+  for (int iv = 0; iv < nint; ++iv) {
+    for (int k = 0; k < 3; ++k) {
+      pts.push_back((2.0 * lower + h + p[k] * h) / 2.0);
+      wts.push_back(w[k] / nint);
+    }
+    lower += h;
+  }
+  auto P = [](double x, int n) -> double {
+    switch (n) {
+      case 0: return 1.0;
+      case 1: return x;
+      case 2: return 0.5 * (3.0 * x * x - 1.0);
+      case 3: return 0.5 * (5.0 * x * x * x - 3.0 * x);
+      case 4: return 0.125 * (35.0 * std::pow(x, 4) - 30.0 * x * x + 3.0);
+      case 5: return 0.125 * (63.0 * std::pow(x, 5) - 70.0 * std::pow(x, 3) + 15.0 * x);
+      case 6: return 0.0625 * (231.0 * std::pow(x, 6) - 315.0 * std::pow(x, 4) + 105.0 * x * x - 5.0);
+      case 7: return 0.0625 * (429.0 * std::pow(x, 7) - 693.0 * std::pow(x, 5) + 315.0 * std::pow(x, 3) - 35.0 * x);
+      case 8:
+        return (1.0 / 128.0) *
+               (6435.0 * std::pow(x, 8) - 12012.0 * std::pow(x, 6) + 6930.0 * std::pow(x, 4) - 1260.0 * x * x + 35.0);
+    }
+    return 0.0;
+  };
+  for (int q = 0; q < Q; ++q) {
+    t.pts[q] = (float)pts[q];
+    for (int k = 0; k <= M; ++k) {
+      // weight and Legendre value rounded separately, as the REAL*4 tables are
+      t.W[k][q] = (float)wts[q] * (float)P(pts[q], k);
+    }
+  }
+  const double eps = c.slenderness;
+  const double cd = std::log(eps * eps * std::exp(1.0));
+  const double dd = -cd;
+  std::vector<double> lam(M), eig(M);
+  lam[0] = 2.0;
+  eig[0] = ((dd - 2.0 - lam[0]) / 2.0) / (dd - lam[0]);
+  for (int k = 1; k < M; ++k) {
+    lam[k] = lam[k - 1] + 2.0 / (k + 1);
+    eig[k] = ((dd - 2.0 - lam[k]) / 2.0) / (dd - lam[k]);
+  }
+  const float epsf = (float)eps;
+  const float cf = std::log(epsf * epsf * std::exp(1.0f));
+  const float df = -cf;
+  t.d = df;
+  t.e2 = 2.0f * epsf * epsf;
+  t.fz_half = -0.5f;
+  t.gamma[0] = 0.75f / (df - 2.0f * 1.0f);  // D1
+  t.eigen[0] = (float)eig[0];
+  for (int k = 1; k < M; ++k) {
+    t.gamma[k] = 0.5f * (2.0f * (float)(k + 1) + 1.0f) / (df + 2.0f - 1.0f * (float)lam[k]);
+    t.eigen[k] = (float)eig[k];
+  }
+  return t;
+}
+
+}  // namespace rf
+
+using namespace rf;
+
+struct rf_handle {
+  rf_config cfg;
+  int N = 0, M = 0, Q = 0;
+  int64_t R = 0, lda = 0;
+  Tables tab;
+  cudaStream_t st = nullptr;
+  int dev = 0, num_sms = 148;
+  // fiber state: FP64 master copies (prev, cur, next rotate) and FP32 views
+  double4* pos64[3] = {nullptr, nullptr, nullptr};
+  double4* ori64[3] = {nullptr, nullptr, nullptr};
+  int iprev = 0, icur = 1, inext = 2;
+  float4* pos32 = nullptr;
+  float4* ori32 = nullptr;
+  float4* tv[2] = {nullptr, nullptr};
+  float4* rv[2] = {nullptr, nullptr};
+  int vprev = 0, vcur = 1;   // velocity buffers; vcur is written by update_velocities
+  int vlast = -1;            // buffer holding the most recent velocities
+  // linear system
+  float* A = nullptr;
+  float* b = nullptr;
+  float* x = nullptr;
+  float* bpart = nullptr;
+  // Krylov scratch
+  float* V = nullptr;
+  float* ypart = nullptr;
+  double* part = nullptr;
+  double* H = nullptr;
+  double* cs = nullptr;
+  double* sn = nullptr;
+  double* g = nullptr;
+  GmresCtl* ctl = nullptr;
+  GmresCtl* host_ctl = nullptr;
+  DenseGemvPlan gemv_plan;
+  int coop_blocks = 1;
+  // velocity scratch
+  float4* fw = nullptr;
+  float* vpart = nullptr;
+  cudaEvent_t ev[8];
+  rf_stats stats;
+  // optional per-launch timing of the solve's matvec kernels
+  bool profile = false;
+  std::vector<cudaEvent_t> mv_events;
+  int mv_used = 0;
+  int launches = 0;
+  bool assembled = false, solved = false;
+  int64_t device_bytes = 0;
+  std::vector<void*> allocations;
+
+  int alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+      return e == cudaErrorMemoryAllocation ? RF_E_OOM : RF_E_CUDA;
+    }
+    allocations.push_back(*p);
+    device_bytes += (int64_t)bytes;
+    return RF_OK;
+  }
+  ~rf_handle() {
+    for (auto e : mv_events) cudaEventDestroy(e);
+    for (void* p : allocations) cudaFree(p);
+    if (host_ctl) cudaFreeHost(host_ctl);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+#define RF_TRY(expr)        \
+  do {                      \
+    int _rc = (expr);       \
+    if (_rc != RF_OK) return _rc; \
+  } while (0)
+
+static int validate_config(const rf_config* c, int N) {
+  if (!c || N < 1) { set_last_error_str("rf_create: null config or N < 1"); return RF_E_INPUT; }
+  const int M = c->number_of_terms_in_force_expansion;
+  if (M < 1 || M > kMaxTerms) { set_last_error_str("M must be in [1, 8]"); return RF_E_INPUT; }
+  if (c->number_of_quadrature_points_per_interval != 3) {
+    set_last_error_str("only 3 Gauss points per interval are defined (fortran/fibers.f95:370-376)");
+    return RF_E_INPUT;
+  }
+  const int Q = 3 * c->number_of_quadrature_intervals;
+  if (Q < 2 || Q > kMaxQuad) { set_last_error_str("quadrature intervals out of range"); return RF_E_INPUT; }
+  if (!mq_supported(M, Q)) { set_last_error_str("(M, intervals) combination not built"); return RF_E_UNSUPPORTED; }
+  if (!(c->slenderness > 0.0) || !(c->timestep > 0.0)) { set_last_error_str("slenderness / timestep"); return RF_E_INPUT; }
+  if (c->solver < 0 || c->solver > 2 || c->integration < 0 || c->integration > 1) {
+    set_last_error_str("solver / integration"); return RF_E_INPUT;
+  }
+  if (c->precision != RF_PREC_FP32) { set_last_error_str("precision mode not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->integration == RF_ANALYTICAL) { set_last_error_str("analytical integration not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->solver != RF_SOLVER_GMRES) { set_last_error_str("solver not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->gmres_restart < 1 || c->gmres_restart > kMaxRestart) { set_last_error_str("gmres restart in [1, 64]"); return RF_E_INPUT; }
+  return RF_OK;
+}
+
+extern "C" {
+
+int rf_config_default(rf_config* c) {
+  if (!c) return RF_E_INPUT;
+  std::memset(c, 0, sizeof(*c));
+  c->number_of_timesteps = 10;
+  c->state_save_interval = 1;
+  c->velocity_save_interval = 1;
+  c->timestep = 0.1;
+  c->slenderness = 0.01;
+  c->number_of_terms_in_force_expansion = 5;
+  c->number_of_quadrature_intervals = 8;
+  c->number_of_quadrature_points_per_interval = 3;
+  c->gmres_restart = 10;
+  c->gmres_max_iterations = 1000;
+  c->gmres_tolerance = 1e-5;
+  c->bicgstab_max_iterations = 1000;
+  c->bicgstab_tolerance = 1e-5;
+  c->solver = RF_SOLVER_GMRES;
+  c->integration = RF_NUMERICAL;
+  c->precision = RF_PREC_FP32;
+  c->velocity_integration = -1;
+  c->refinement_tolerance = 1e-6;
+  c->refinement_max_iterations = 20;
+  return RF_OK;
+}
+
+const char* rf_status_string(int s) {
+  switch (s) {
+    case RF_OK: return "ok";
+    case RF_E_INPUT: return "invalid input";
+    case RF_E_CUDA: return "CUDA error";
+    case RF_E_OOM: return "out of device memory";
+    case RF_E_NOCONV: return "solver did not converge";
+    case RF_E_NAN: return "non-finite values";
+    case RF_E_TIMEOUT: return "device wait timed out";
+    case RF_E_UNSUPPORTED: return "unsupported configuration";
+    case RF_E_STATE: return "call out of order";
+    case RF_E_SINGULAR: return "singular matrix";
+  }
+  return "unknown status";
+}
+
+const char* rf_last_error(void) { return g_last_error.c_str(); }
+
+static void to_double4(const double* src, int N, std::vector<double>& out) {
+  out.assign((size_t)N * 4, 0.0);
+  for (int i = 0; i < N; ++i)
+    for (int a = 0; a < 3; ++a) out[(size_t)i * 4 + a] = src[(size_t)i * 3 + a];
+}
+
+int rf_set_state(rf_handle* h, const double* pos, const double* ori) {
+  if (!h || !pos || !ori) return RF_E_INPUT;
+  std::vector<double> p4, o4;
+  to_double4(pos, h->N, p4);
+  to_double4(ori, h->N, o4);
+  std::vector<float> p32((size_t)h->N * 4), o32((size_t)h->N * 4);
+  for (size_t k = 0; k < p4.size(); ++k) { p32[k] = (float)p4[k]; o32[k] = (float)o4[k]; }
+  const size_t b64 = (size_t)h->N * sizeof(double4), b32 = (size_t)h->N * sizeof(float4);
+  for (int s = 0; s < 2; ++s) {   // previous == current at the first step
+    const int idx = s == 0 ? h->icur : h->iprev;
+    RF_CUDA_TRY(cudaMemcpyAsync(h->pos64[idx], p4.data(), b64, cudaMemcpyHostToDevice, h->st));
+    RF_CUDA_TRY(cudaMemcpyAsync(h->ori64[idx], o4.data(), b64, cudaMemcpyHostToDevice, h->st));
+  }
+  RF_CUDA_TRY(cudaMemcpyAsync(h->pos32, p32.data(), b32, cudaMemcpyHostToDevice, h->st));
+  RF_CUDA_TRY(cudaMemcpyAsync(h->ori32, o32.data(), b32, cudaMemcpyHostToDevice, h->st));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->assembled = h->solved = false;
+  return RF_OK;
+}
+
+int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori, rf_handle** out) {
+  if (!out) return RF_E_INPUT;
+  *out = nullptr;
+  RF_TRY(validate_config(cfg, N));
+  if (!pos || !ori) { set_last_error_str("rf_create: null fiber arrays"); return RF_E_INPUT; }
+  rf_handle* h = new rf_handle();
+  h->cfg = *cfg;
+  h->N = N;
+  h->M = cfg->number_of_terms_in_force_expansion;
+  h->Q = 3 * cfg->number_of_quadrature_intervals;
+  h->R = (int64_t)3 * h->M * N;
+  h->lda = ceil_div(h->R, 32) * 32;
+  h->tab = make_tables(*cfg);
+  std::memset(&h->stats, 0, sizeof(h->stats));
+  for (auto& e : h->ev) e = nullptr;
+  auto fail = [&](int rc) { delete h; return rc; };
+  cudaError_t e = cudaGetDevice(&h->dev);
+  if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return fail(RF_E_CUDA); }
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev);
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(RF_E_CUDA);
+  for (auto& ev : h->ev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(RF_E_CUDA);
+  const int64_t R = h->R;
+  const size_t b64 = (size_t)N * sizeof(double4), b32 = (size_t)N * sizeof(float4);
+  int rc = RF_OK;
+  for (int s = 0; s < 3 && !rc; ++s) {
+    rc = h->alloc((void**)&h->pos64[s], b64);
+    if (!rc) rc = h->alloc((void**)&h->ori64[s], b64);
+  }
+  if (!rc) rc = h->alloc((void**)&h->pos32, b32);
+  if (!rc) rc = h->alloc((void**)&h->ori32, b32);
+  for (int s = 0; s < 2 && !rc; ++s) {
+    rc = h->alloc((void**)&h->tv[s], b32);
+    if (!rc) rc = h->alloc((void**)&h->rv[s], b32);
+  }
+  if (!rc) rc = h->alloc((void**)&h->A, (size_t)h->lda * (size_t)R * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->b, (size_t)R * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->x, (size_t)R * sizeof(float));
+  const int tiles = assemble_tiles(h->M, h->Q, N);
+  if (!rc) rc = h->alloc((void**)&h->bpart, (size_t)tiles * (size_t)R * sizeof(float));
+  // Krylov
+  const int m = cfg->gmres_restart;
+  h->gemv_plan = plan_dense_gemv(R, h->num_sms);
+  h->coop_blocks = krylov_coop_blocks(R, h->num_sms);
+  const int64_t ldv = ceil_div(R, 32) * 32;
+  if (!rc) rc = h->alloc((void**)&h->V, (size_t)(m + 1) * (size_t)ldv * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->ypart, (size_t)h->gemv_plan.splits * (size_t)R * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->part, (size_t)3 * h->coop_blocks * (kMaxRestart + 2) * sizeof(double));
+  if (!rc) rc = h->alloc((void**)&h->H, (size_t)(m + 1) * m * sizeof(double));
+  if (!rc) rc = h->alloc((void**)&h->cs, (size_t)m * sizeof(double));
+  if (!rc) rc = h->alloc((void**)&h->sn, (size_t)m * sizeof(double));
+  if (!rc) rc = h->alloc((void**)&h->g, (size_t)(m + 1) * sizeof(double));
+  if (!rc) rc = h->alloc((void**)&h->ctl, sizeof(GmresCtl));
+  if (!rc && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
+  // velocities
+  if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
+  if (!rc) rc = h->alloc((void**)&h->vpart, (size_t)velocity_chunks(N) * N * 6 * sizeof(float));
+  if (rc) return fail(rc);
+  h->stats.device_bytes = h->device_bytes;
+  rc = rf_set_state(h, pos, ori);
+  if (rc) return fail(rc);
+  *out = h;
+  return RF_OK;
+}
+
+int rf_destroy(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  cudaStreamSynchronize(h->st);
+  delete h;
+  return RF_OK;
+}
+
+static float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+int rf_assemble(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
+  RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->bpart, h->b, h->st));
+  h->launches += 2;
+  RF_CUDA_TRY(cudaEventRecord(h->ev[1], h->st));
+  h->assembled = true;
+  h->solved = false;
+  return RF_OK;
+}
+
+int rf_solve(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  if (!h->assembled) { set_last_error_str("rf_solve before rf_assemble"); return RF_E_STATE; }
+  RF_CUDA_TRY(cudaEventRecord(h->ev[2], h->st));
+  GmresSetup s;
+  s.R = h->R;
+  s.m = h->cfg.gmres_restart;
+  s.maxit = h->cfg.gmres_max_iterations;
+  s.tol = h->cfg.gmres_tolerance;
+  s.V = h->V;
+  s.ldv = ceil_div(h->R, 32) * 32;
+  s.ypart = h->ypart;
+  s.nsplit = h->gemv_plan.splits;
+  s.part = h->part;
+  s.H = h->H;
+  s.cs = h->cs;
+  s.sn = h->sn;
+  s.g = h->g;
+  s.ctl = h->ctl;
+  s.host_ctl = h->host_ctl;
+  s.coop_blocks = h->coop_blocks;
+  h->mv_used = 0;
+  int mv_launches = 0;
+  MatvecFn mv = [h, &mv_launches](const float* xin, const int* skip, cudaStream_t st) -> int {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (h->profile) {
+      while ((int)h->mv_events.size() < h->mv_used + 2) {
+        cudaEvent_t e;
+        RF_CUDA_TRY(cudaEventCreate(&e));
+        h->mv_events.push_back(e);
+      }
+      e0 = h->mv_events[h->mv_used];
+      e1 = h->mv_events[h->mv_used + 1];
+      h->mv_used += 2;
+      RF_CUDA_TRY(cudaEventRecord(e0, st));
+    }
+    ++mv_launches;
+    int rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
+    if (h->profile) RF_CUDA_TRY(cudaEventRecord(e1, st));
+    return rc;
+  };
+  GmresResult res;
+  int rc = gmres_solve(s, mv, h->b, h->x, h->st, &res);
+  RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
+  h->launches += res.launches + mv_launches;
+  h->stats.iterations = res.iterations;
+  h->stats.restarts = res.restarts;
+  h->stats.refinement_steps = 0;
+  h->stats.relative_residual = res.relative_residual;
+  if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
+  h->solved = true;
+  return rc;
+}
+
+int rf_update_velocities(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  if (!h->solved) { set_last_error_str("rf_update_velocities before rf_solve"); return RF_E_STATE; }
+  RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
+  RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos32, h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
+                                   h->rv[h->vcur], h->st));
+  h->launches += 3;
+  RF_CUDA_TRY(cudaEventRecord(h->ev[5], h->st));
+  h->vlast = h->vcur;
+  return RF_OK;
+}
+
+int rf_update_fibers(rf_handle* h, int first_step) {
+  if (!h) return RF_E_INPUT;
+  if (h->vlast != h->vcur) { set_last_error_str("rf_update_fibers before rf_update_velocities"); return RF_E_STATE; }
+  RF_CUDA_TRY(cudaEventRecord(h->ev[6], h->st));
+  RF_TRY(launch_update_fibers(h->N, first_step, h->cfg.timestep, h->pos64[h->iprev], h->pos64[h->icur],
+                              h->ori64[h->iprev], h->ori64[h->icur], h->tv[h->vprev], h->tv[h->vcur],
+                              h->rv[h->vprev], h->rv[h->vcur], h->pos64[h->inext], h->ori64[h->inext], h->pos32,
+                              h->ori32, h->st));
+  h->launches += 1;
+  RF_CUDA_TRY(cudaEventRecord(h->ev[7], h->st));
+  // rotate (src/simulation.cu:307-311; fortran/fibers.f95:325-341)
+  const int p = h->iprev;
+  h->iprev = h->icur;
+  h->icur = h->inext;
+  h->inext = p;
+  std::swap(h->vprev, h->vcur);
+  h->assembled = h->solved = false;
+  return RF_OK;
+}
+
+int rf_step(rf_handle* h, int t) {
+  if (!h) return RF_E_INPUT;
+  h->launches = 0;
+  RF_TRY(rf_assemble(h));
+  int rc = rf_solve(h);
+  if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
+  RF_TRY(rf_update_velocities(h));
+  RF_TRY(rf_update_fibers(h, t == 0));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
+  h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
+  h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
+  h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
+  h->stats.kernel_launches = h->launches;
+  return rc;
+}
+
+int rf_run(rf_handle* h, int first_timestep, int nsteps) {
+  for (int k = 0; k < nsteps; ++k) {
+    int rc = rf_step(h, first_timestep + k);
+    if (rc != RF_OK) return rc;
+  }
+  return RF_OK;
+}
+
+static int fetch3(rf_handle* h, const void* dev, bool is_double, double* out) {
+  const int N = h->N;
+  if (is_double) {
+    std::vector<double> tmp((size_t)N * 4);
+    RF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    for (int i = 0; i < N; ++i)
+      for (int a = 0; a < 3; ++a) out[(size_t)i * 3 + a] = tmp[(size_t)i * 4 + a];
+  } else {
+    std::vector<float> tmp((size_t)N * 4);
+    RF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    for (int i = 0; i < N; ++i)
+      for (int a = 0; a < 3; ++a) out[(size_t)i * 3 + a] = tmp[(size_t)i * 4 + a];
+  }
+  return RF_OK;
+}
+
+int rf_get_state(rf_handle* h, double* pos, double* ori) {
+  if (!h || !pos || !ori) return RF_E_INPUT;
+  RF_TRY(fetch3(h, h->pos64[h->icur], true, pos));
+  return fetch3(h, h->ori64[h->icur], true, ori);
+}
+
+int rf_get_velocities(rf_handle* h, double* tvel, double* rvel) {
+  if (!h || !tvel || !rvel) return RF_E_INPUT;
+  if (h->vlast < 0) { set_last_error_str("no velocities computed yet"); return RF_E_STATE; }
+  RF_TRY(fetch3(h, h->tv[h->vlast], false, tvel));
+  return fetch3(h, h->rv[h->vlast], false, rvel);
+}
+
+static int fetch_vec(rf_handle* h, const float* dev, double* out) {
+  std::vector<float> tmp((size_t)h->R);
+  RF_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  for (int64_t r = 0; r < h->R; ++r) out[r] = tmp[r];
+  return RF_OK;
+}
+
+int rf_get_system(rf_handle* h, float* A, double* b) {
+  if (!h) return RF_E_INPUT;
+  if (!h->assembled) { set_last_error_str("no assembled system"); return RF_E_STATE; }
+  if (A) {
+    RF_CUDA_TRY(cudaMemcpy2DAsync(A, (size_t)h->R * sizeof(float), h->A, (size_t)h->lda * sizeof(float),
+                                  (size_t)h->R * sizeof(float), (size_t)h->R, cudaMemcpyDeviceToHost, h->st));
+  }
+  if (b) RF_TRY(fetch_vec(h, h->b, b));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return RF_OK;
+}
+
+int rf_get_solution(rf_handle* h, double* x) {
+  if (!h || !x) return RF_E_INPUT;
+  if (!h->solved && h->vlast < 0) { set_last_error_str("no solution yet"); return RF_E_STATE; }
+  return fetch_vec(h, h->x, x);
+}
+
+int rf_last_stats(rf_handle* h, rf_stats* s) {
+  if (!h || !s) return RF_E_INPUT;
+  *s = h->stats;
+  s->device_bytes = h->device_bytes;
+  return RF_OK;
+}
+
+int rf_get_config(rf_handle* h, rf_config* c) {
+  if (!h || !c) return RF_E_INPUT;
+  *c = h->cfg;
+  return RF_OK;
+}
+
+int rf_number_of_fibers(rf_handle* h) { return h ? h->N : -1; }
+
+int rf_get_stream(rf_handle* h, void** stream) {
+  if (!h || !stream) return RF_E_INPUT;
+  *stream = (void*)h->st;
+  return RF_OK;
+}
+
+int rf_set_profiling(rf_handle* h, int enable) {
+  if (!h) return RF_E_INPUT;
+  h->profile = enable != 0;
+  return RF_OK;
+}
+
+int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms) {
+  if (!h || !launches || !total_ms) return RF_E_INPUT;
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  double t = 0.0;
+  for (int k = 0; k + 1 < h->mv_used; k += 2) t += elapsed(h->mv_events[k], h->mv_events[k + 1]);
+  *launches = h->mv_used / 2;
+  *total_ms = t;
+  return RF_OK;
+}
+
+int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream) {
+  if (!A || !x || !y || R < 1) { set_last_error_str("rf_dense_matvec: bad arguments"); return RF_E_INPUT; }
+  int dev = 0, sms = 148;
+  RF_CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  DenseGemvPlan p = plan_dense_gemv(R, sms);
+  float* ypart = nullptr;
+  RF_CUDA_TRY(cudaMallocAsync((void**)&ypart, (size_t)p.splits * R * sizeof(float), st));
+  int rc = launch_dense_gemv(p, A, R, R, x, ypart, nullptr, st);
+  if (rc == RF_OK) rc = launch_reduce_rows(ypart, p.splits, R, y, st);
+  cudaFreeAsync(ypart, st);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Shared definitions of the rigid-fiber CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/rigidfibers.h"
+
+namespace rf {
+
+constexpr int kMaxTerms = 8;      // Legendre terms supported (closed forms to P_8)
+constexpr int kMaxQuad = 48;      // quadrature points per fiber (16 intervals x 3)
+
+// Per-launch tables, passed by value so every kernel sees them through the
+// constant parameter bank (no module-global state: handles with different
+// slenderness / M / Q can run side by side).
+//   W[k][q] = w_q * P_k(s_q) for k = 0..M (P_0 = 1 carries the force term,
+//   P_k, k>=1, carries force index k-1, as in fortran/fibers.f95:403-408).
+struct Tables {
+  float pts[kMaxQuad];
+  float W[kMaxTerms + 1][kMaxQuad];   // W[0][q] = w_q
+  float gamma[kMaxTerms];   // gamma[0] = D1 (force index 0), gamma[k] for k>=1
+  float eigen[kMaxTerms];   // E_k; unused for k = 0
+  float e2;                 // 2 * eps^2
+  float fz_half;            // external force z / 2 = -0.5 (fortran/fibers.f95:149)
+  float d;                  // -log(eps^2 e)
+  int M, Q;
+};
+
+
+// Error plumbing: every launch is checked; the C ABI maps failures to codes.
+#define RF_CUDA_TRY(expr)                                                          \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      ::rf::set_last_error(cudaGetErrorString(_e), __FILE__, __LINE__);            \
+      return _e == cudaErrorMemoryAllocation ? RF_E_OOM : RF_E_CUDA;               \
+    }                                                                              \
+  } while (0)
+
+#define RF_LAUNCH_CHECK() RF_CUDA_TRY(cudaGetLastError())
+
+void set_last_error(const char* msg, const char* file, int line);
+void set_last_error_str(const char* msg);
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Symmetric 3x3 stored as (11, 22, 33, 12, 13, 23) -- the order of
+// fortran/compute_inner_integral_numerically.incl:179-184.
+__device__ __forceinline__ float sym_get(const float* s6, int a, int b) {
+  const int idx[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+  return s6[idx[a][b]];
+}
+
+}  // namespace rf

@@ -1,0 +1,70 @@
+// Krylov solver interfaces (device-resident GMRES / BiCGSTAB).
+#pragma once
+#include <functional>
+
+#include "rf_common.cuh"
+
+namespace rf {
+
+constexpr int kMaxRestart = 64;
+
+// Device control block of one solve; the host reads it once per cycle.
+struct GmresCtl {
+  int cycle_done;     // skip the rest of this restart cycle
+  int converged;      // true residual <= tol * ||b||
+  int nan;            // non-finite residual seen
+  int jconv;          // Arnoldi steps taken in the current cycle
+  int total_iters;
+  int maxit;
+  int restarts;
+  int pad;
+  double tol;
+  double bnorm;
+  double beta;        // true residual norm at the last cycle start
+  double estimate;    // Arnoldi residual estimate after the last step
+};
+
+// ypart = partial rows of A x (nsplit of them); `skip` is a device flag the
+// matvec kernels read first and return on when set.
+using MatvecFn = std::function<int(const float* x, const int* skip, cudaStream_t st)>;
+
+struct GmresSetup {
+  int64_t R;
+  int m;               // restart length
+  int maxit;
+  double tol;
+  float* V;            // (m+1) x ldv
+  int64_t ldv;
+  const float* ypart;  // written by the matvec
+  int nsplit;
+  double* part;        // 3 * coop_blocks * (kMaxRestart + 2)
+  double* H;           // (m+1) * m
+  double* cs;
+  double* sn;
+  double* g;
+  GmresCtl* ctl;       // device
+  GmresCtl* host_ctl;  // pinned host
+  int coop_blocks;
+};
+
+struct GmresResult {
+  int iterations = 0;
+  int restarts = 0;
+  double relative_residual = 0.0;
+  int launches = 0;       // kernels launched (matvec launches counted by the caller's MatvecFn)
+};
+
+int krylov_coop_blocks(int64_t R, int num_sms);
+int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
+                GmresResult* res);
+
+struct DenseGemvPlan {
+  int row_blocks;
+  int splits;
+  int64_t cps;  // columns per split
+};
+DenseGemvPlan plan_dense_gemv(int64_t R, int num_sms);
+int launch_dense_gemv(const DenseGemvPlan& p, const float* A, int64_t lda, int64_t R, const float* x, float* ypart,
+                      const int* skip, cudaStream_t st);
+
+}  // namespace rf

@@ -1,0 +1,206 @@
+// Velocity update (numerical inner integrals) and the fiber time integrator.
+//
+// Reference: fortran/update_velocities.incl:1-89 (and the CUDA kernels
+// src/kernels/reset_velocities.cu:6-39, update_velocities_2D.cu:6-166):
+//   U_i = (0.5/d) [ (d+2) F + (d-2)(t_i.F) t_i + sum_{j!=i} sum_qi w_qi GF_ij(qi) ]
+//   W_i = (1.5/d) (I - t_i t_i^T) sum_{j!=i} sum_qi w_qi P_1(s_qi) GF_ij(qi)
+//   GF_ij(qi) = sum_qj w_qj K(R_ij(qi,qj)) f_j(qj),  f_j = F/2 + sum_k a_{j,k} P_{k+1}
+// fortran/update_fibers_firststep.incl:1-10 and update_fibers.incl:1-17 for
+// the time step, here accumulated in FP64 on FP64 state.
+// Reductions are deterministic: per-(j-chunk, fiber) partial sums, then a
+// fixed-order sum; no atomics.
+#include "rf_common.cuh"
+#include "rf_kernels.cuh"
+
+namespace rf {
+
+// fw[j*Q + q] = w_q f_j(s_q) = W[0][q] F/2 + sum_k a_{j,k} W[k+1][q]
+__global__ void k_source_density(const Tables tab, int N, const float* __restrict__ x, float4* __restrict__ fw) {
+  const int Q = tab.Q, M = tab.M;
+  const int64_t n = (int64_t)N * Q;
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(u / Q), q = (int)(u % Q);
+    float f0 = 0.f, f1 = 0.f, f2 = tab.W[0][q] * tab.fz_half;
+    const float* a = x + (int64_t)j * 3 * M;
+    for (int k = 0; k < M; ++k) {
+      const float w = tab.W[k + 1][q];
+      f0 = fmaf(a[3 * k + 0], w, f0);
+      f1 = fmaf(a[3 * k + 1], w, f1);
+      f2 = fmaf(a[3 * k + 2], w, f2);
+    }
+    fw[u] = make_float4(f0, f1, f2, 0.f);
+  }
+}
+
+// One CTA = TI fibers i x one chunk of source fibers j.  Thread u < TI*Q owns
+// (fiber il, quadrature point qi) and accumulates sum_j GF_ij(qi).
+template <int Q>
+__global__ void __launch_bounds__(192, 4)
+k_velocity_numerical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+                     const float4* __restrict__ fw, int jchunk, float* __restrict__ vpart) {
+  constexpr int TI = 192 / Q;
+  constexpr int U = TI * Q;
+  __shared__ float4 sP[TI][Q], sF[TI][Q];
+  __shared__ float sGs[3][U];
+  const int tid = threadIdx.x;
+  const int il = tid / Q, qi = tid % Q;
+  const int i0 = blockIdx.x * TI;
+  const int i = i0 + il;
+  const bool unit_ok = tid < U && i < N;
+  float pix = 0.f, piy = 0.f, piz = 0.f;
+  if (unit_ok) {
+    const float4 x = pos[i], t = ori[i];
+    const float s = tab.pts[qi];
+    pix = fmaf(s, t.x, x.x); piy = fmaf(s, t.y, x.y); piz = fmaf(s, t.z, x.z);
+  }
+  const float e2 = tab.e2, e2x3 = -3.f * tab.e2;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+  const int jbeg = blockIdx.y * jchunk, jend = min(N, jbeg + jchunk);
+  for (int js = jbeg; js < jend; js += TI) {
+    __syncthreads();
+    if (tid < U) {
+      const int jl = tid / Q, q = tid % Q;
+      const int j = min(js + jl, N - 1);
+      const float4 x = pos[j], t = ori[j];
+      const float s = tab.pts[q];
+      sP[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
+      sF[jl][q] = fw[(int64_t)j * Q + q];
+    }
+    __syncthreads();
+    const int jn = min(TI, jend - js);
+    if (unit_ok) {
+      for (int jl = 0; jl < jn; ++jl) {
+        if (js + jl == i) continue;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const float4 pj = sP[jl][q];
+          const float4 f = sF[jl][q];
+          const float rx = pix - pj.x, ry = piy - pj.y, rz = piz - pj.z;
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float inv = rsqrtf(r2);
+          const float inv2 = inv * inv;
+          const float inv3 = inv2 * inv;
+          const float inv5 = inv3 * inv2;
+          const float a = fmaf(e2, inv3, inv);
+          const float bb = fmaf(e2x3, inv5, inv3);
+          // K f = a f + bb R (R.f)
+          const float rf = fmaf(rx, f.x, fmaf(ry, f.y, rz * f.z)) * bb;
+          g0 = fmaf(a, f.x, fmaf(rf, rx, g0));
+          g1 = fmaf(a, f.y, fmaf(rf, ry, g1));
+          g2 = fmaf(a, f.z, fmaf(rf, rz, g2));
+        }
+      }
+    }
+  }
+  if (tid < U) { sGs[0][tid] = g0; sGs[1][tid] = g1; sGs[2][tid] = g2; }
+  __syncthreads();
+  // per fiber: sum_qi w_qi gs(qi) and sum_qi w_qi P_1(s_qi) gs(qi)
+  if (tid < TI * 6) {
+    const int fl = tid / 6, comp = tid % 6;
+    const int a = comp % 3;
+    const bool rot = comp >= 3;
+    float s = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s = fmaf(rot ? tab.W[1][q] : tab.W[0][q], sGs[a][fl * Q + q], s);
+    if (i0 + fl < N) vpart[((int64_t)blockIdx.y * N + i0 + fl) * 6 + comp] = s;
+  }
+}
+
+// Self term, fixed-order sum over chunks, projection and scaling.
+__global__ void k_velocity_finalize(const Tables tab, int N, const float4* __restrict__ ori,
+                                    const float* __restrict__ vpart, int nchunks, float4* __restrict__ tvel,
+                                    float4* __restrict__ rvel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float4 t = ori[i];
+  const float d = tab.d;
+  const float Fz = 2.f * tab.fz_half;            // F = (0, 0, -1)
+  const float tF = t.z * Fz;
+  float U[3] = {(d - 2.f) * tF * t.x, (d - 2.f) * tF * t.y, (d + 2.f) * Fz + (d - 2.f) * tF * t.z};
+  float W[3] = {0.f, 0.f, 0.f};
+  for (int c = 0; c < nchunks; ++c) {
+    const float* p = vpart + ((int64_t)c * N + i) * 6;
+    U[0] += p[0]; U[1] += p[1]; U[2] += p[2];
+    W[0] += p[3]; W[1] += p[4]; W[2] += p[5];
+  }
+  const float tW = t.x * W[0] + t.y * W[1] + t.z * W[2];
+  const float su = 0.5f / d, sr = 1.5f / d;
+  tvel[i] = make_float4(U[0] * su, U[1] * su, U[2] * su, 0.f);
+  rvel[i] = make_float4((W[0] - t.x * tW) * sr, (W[1] - t.y * tW) * sr, (W[2] - t.z * tW) * sr, 0.f);
+}
+
+int velocity_chunks(int N) {
+  // enough CTAs to fill 148 SMs several times over for any N
+  const int tiles = (int)ceil_div(N, 8);
+  int chunks = (int)ceil_div(148 * 8, tiles);
+  chunks = std::max(1, std::min(chunks, (int)ceil_div(N, 8)));
+  return chunks;
+}
+
+int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
+                              float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
+  const int Q = tab.Q;
+  k_source_density<<<(unsigned)std::min<int64_t>(ceil_div((int64_t)N * Q, 256), 148 * 16), 256, 0, st>>>(tab, N, x, fw);
+  RF_LAUNCH_CHECK();
+  const int chunks = velocity_chunks(N);
+  const int jchunk = (int)ceil_div(N, chunks);
+  const int TI = 192 / Q;
+  dim3 grid((unsigned)ceil_div(N, TI), (unsigned)chunks);
+  switch (Q) {
+    case 12: k_velocity_numerical<12><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
+    case 24: k_velocity_numerical<24><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
+    case 48: k_velocity_numerical<48><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
+    default: set_last_error_str("velocity: quadrature size not instantiated"); return RF_E_UNSUPPORTED;
+  }
+  RF_LAUNCH_CHECK();
+  k_velocity_finalize<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(tab, N, ori, vpart, chunks, tvel, rvel);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+// first != 0: x1 = x0 + dt U0, t1 = normalize(t0 + dt W0)
+// otherwise: x^{n+1} = 4/3 x^n - 1/3 x^{n-1} + 2/3 dt (2 U^n - U^{n-1}), same for t, normalised.
+__global__ void k_update_fibers(int N, int first, double dt, const double4* __restrict__ prev_pos,
+                                const double4* __restrict__ cur_pos, const double4* __restrict__ prev_ori,
+                                const double4* __restrict__ cur_ori, const float4* __restrict__ prev_tv,
+                                const float4* __restrict__ cur_tv, const float4* __restrict__ prev_rv,
+                                const float4* __restrict__ cur_rv, double4* __restrict__ next_pos,
+                                double4* __restrict__ next_ori, float4* __restrict__ pos32, float4* __restrict__ ori32) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double4 xc = cur_pos[i], tc = cur_ori[i];
+  const float4 u = cur_tv[i], w = cur_rv[i];
+  double4 xn, tn;
+  if (first) {
+    xn = make_double4(xc.x + dt * u.x, xc.y + dt * u.y, xc.z + dt * u.z, 0.0);
+    tn = make_double4(tc.x + dt * w.x, tc.y + dt * w.y, tc.z + dt * w.z, 0.0);
+  } else {
+    const double4 xp = prev_pos[i], tp = prev_ori[i];
+    const float4 up = prev_tv[i], wp = prev_rv[i];
+    const double c43 = 4.0 / 3.0, c13 = 1.0 / 3.0, c23 = (2.0 / 3.0) * dt;
+    xn = make_double4(c43 * xc.x - c13 * xp.x + c23 * (2.0 * u.x - up.x),
+                      c43 * xc.y - c13 * xp.y + c23 * (2.0 * u.y - up.y),
+                      c43 * xc.z - c13 * xp.z + c23 * (2.0 * u.z - up.z), 0.0);
+    tn = make_double4(c43 * tc.x - c13 * tp.x + c23 * (2.0 * w.x - wp.x),
+                      c43 * tc.y - c13 * tp.y + c23 * (2.0 * w.y - wp.y),
+                      c43 * tc.z - c13 * tp.z + c23 * (2.0 * w.z - wp.z), 0.0);
+  }
+  const double inv = 1.0 / sqrt(tn.x * tn.x + tn.y * tn.y + tn.z * tn.z);
+  tn.x *= inv; tn.y *= inv; tn.z *= inv;
+  next_pos[i] = xn;
+  next_ori[i] = tn;
+  pos32[i] = make_float4((float)xn.x, (float)xn.y, (float)xn.z, 0.f);
+  ori32[i] = make_float4((float)tn.x, (float)tn.y, (float)tn.z, 0.f);
+}
+
+int launch_update_fibers(int N, int first, double dt, const double4* pp, const double4* cp, const double4* po,
+                         const double4* co, const float4* ptv, const float4* ctv, const float4* prv,
+                         const float4* crv, double4* np, double4* no, float4* pos32, float4* ori32,
+                         cudaStream_t st) {
+  k_update_fibers<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(N, first, dt, pp, cp, po, co, ptv, ctv, prv, crv, np,
+                                                              no, pos32, ori32);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+}  // namespace rf

@@ -1,0 +1,171 @@
+"""Host-side mirror of the reference's `Simulation` class
+(src/simulation.h:38-97, src/simulation.cu:44-528) over the C ABI.
+
+    sim = Simulation(config, positions, orientations)
+    for t in range(config.number_of_timesteps):
+        sim.step(t)                      # assembleSystem -> solveSystem ->
+                                         # updateVelocities -> updateFibers
+
+Every method raises RigidFibersError on a non-zero status; a solver that
+hits its iteration limit raises unless `allow_noconv` is set (the reference
+prints and continues, src/simulation.cu:441-442).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+
+class Config:
+    """The reference's .ini keys plus the runtime choices it fixed at compile
+    time (solver, integration) and the precision mode."""
+
+    def __init__(self, **kw):
+        lib = C.load()
+        self._c = C.rf_config()
+        C.check(lib.rf_config_default(ctypes.byref(self._c)), "rf_config_default")
+        for k, v in kw.items():
+            self[k] = v
+
+    def __setitem__(self, key, value):
+        if key == "solver":
+            value = C.SOLVERS[value] if isinstance(value, str) else value
+        elif key == "integration":
+            value = C.INTEGRATIONS[value] if isinstance(value, str) else value
+        elif key == "precision":
+            value = C.PRECISIONS[value] if isinstance(value, str) else value
+        elif key == "velocity_integration" and isinstance(value, str):
+            value = {"same": -1, "numerical": 0, "analytical": 1}[value]
+        if not hasattr(self._c, key):
+            raise KeyError(key)
+        setattr(self._c, key, value)
+
+    def __getitem__(self, key):
+        return getattr(self._c, key)
+
+    def __getattr__(self, key):
+        if key.startswith("_"):
+            raise AttributeError(key)
+        return getattr(self._c, key)
+
+    @classmethod
+    def from_ini(cls, params, **kw):
+        """From formats.read_config() output (reference key names)."""
+        c = cls(
+            number_of_timesteps=params["NUMBER_OF_TIMESTEPS"],
+            state_save_interval=params["STATE_SAVE_INTERVAL"],
+            velocity_save_interval=params["VELOCITY_SAVE_INTERVAL"],
+            timestep=params["TIMESTEP"],
+            slenderness=params["SLENDERNESS"],
+            number_of_terms_in_force_expansion=params["NUMBER_OF_TERMS_IN_FORCE_EXPANSION"],
+            number_of_quadrature_intervals=params["NUMBER_OF_QUADRATURE_INTERVALS"],
+            number_of_quadrature_points_per_interval=params["NUMBER_OF_QUADRATURE_POINTS_PER_INTERVAL"],
+            gmres_restart=params["GMRES_RESTART"],
+            gmres_max_iterations=params["GMRES_MAX_ITERATIONS"],
+            gmres_tolerance=params["GMRES_TOLERANCE"],
+            bicgstab_max_iterations=params["BICGSTAB_MAX_ITERATIONS"],
+            bicgstab_tolerance=params["BICGSTAB_TOLERANCE"],
+        )
+        for k, v in kw.items():
+            c[k] = v
+        return c
+
+
+class Simulation:
+    def __init__(self, config, positions, orientations, allow_noconv=False):
+        self._lib = C.load()
+        pos = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+        ori = np.ascontiguousarray(orientations, np.float64).reshape(-1, 3)
+        if pos.shape != ori.shape:
+            raise ValueError("positions and orientations differ in shape")
+        self.N = pos.shape[0]
+        self.config = config if isinstance(config, Config) else Config(**config)
+        M = self.config.number_of_terms_in_force_expansion
+        self.R = 3 * M * self.N
+        self.allow_noconv = allow_noconv
+        h = ctypes.c_void_p()
+        C.check(self._lib.rf_create(ctypes.byref(self.config._c), self.N, C.ptr(pos), C.ptr(ori), ctypes.byref(h)),
+                "rf_create")
+        self._h = h
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- the reference's step seam (src/simulation.h:86-89) ------------------
+    def assembleSystem(self):
+        C.check(self._lib.rf_assemble(self._h), "assembleSystem")
+
+    def solveSystem(self):
+        allow = (C.RF_E_NOCONV,) if self.allow_noconv else ()
+        return C.check(self._lib.rf_solve(self._h), "solveSystem", allow)
+
+    def updateVelocities(self):
+        C.check(self._lib.rf_update_velocities(self._h), "updateVelocities")
+
+    def updateFibers(self, first_timestep):
+        C.check(self._lib.rf_update_fibers(self._h, int(bool(first_timestep))), "updateFibers")
+
+    def step(self, current_timestep):
+        allow = (C.RF_E_NOCONV,) if self.allow_noconv else ()
+        return C.check(self._lib.rf_step(self._h, int(current_timestep)), "step", allow)
+
+    def run(self, nsteps, first_timestep=0):
+        for t in range(first_timestep, first_timestep + nsteps):
+            self.step(t)
+
+    # snake_case aliases
+    assemble_system = assembleSystem
+    solve_system = solveSystem
+    update_velocities = updateVelocities
+    update_fibers = updateFibers
+
+    # -- state and dumps ----------------------------------------------------
+    def state(self):
+        pos = np.zeros(3 * self.N)
+        ori = np.zeros(3 * self.N)
+        C.check(self._lib.rf_get_state(self._h, C.ptr(pos), C.ptr(ori)), "rf_get_state")
+        return pos.reshape(-1, 3), ori.reshape(-1, 3)
+
+    def set_state(self, positions, orientations):
+        pos = C.f64(positions, 3 * self.N)
+        ori = C.f64(orientations, 3 * self.N)
+        C.check(self._lib.rf_set_state(self._h, C.ptr(pos), C.ptr(ori)), "rf_set_state")
+
+    def velocities(self):
+        t = np.zeros(3 * self.N)
+        r = np.zeros(3 * self.N)
+        C.check(self._lib.rf_get_velocities(self._h, C.ptr(t), C.ptr(r)), "rf_get_velocities")
+        return t.reshape(-1, 3), r.reshape(-1, 3)
+
+    def system(self, with_matrix=True):
+        """(A, b): A column-major (R, R) float32 Fortran-ordered, or None."""
+        b = np.zeros(self.R)
+        A = np.zeros((self.R, self.R), np.float32, order="F") if with_matrix else None
+        C.check(self._lib.rf_get_system(self._h, C.ptr(A) if A is not None else None, C.ptr(b)), "rf_get_system")
+        return A, b
+
+    def solution(self):
+        x = np.zeros(self.R)
+        C.check(self._lib.rf_get_solution(self._h, C.ptr(x)), "rf_get_solution")
+        return x
+
+    def stats(self):
+        s = C.rf_stats()
+        C.check(self._lib.rf_last_stats(self._h, ctypes.byref(s)), "rf_last_stats")
+        return {k: getattr(s, k) for k, _ in C.rf_stats._fields_}

@@ -1,0 +1,135 @@
+"""CUDA path against the oracle and the reference's golden vectors.
+
+Tolerances (FP32 plain path; north star: 1e-5 relative):
+  * assembled A and b vs the FP64 oracle: 2e-6 of the largest |entry|
+  * golden fields: relative to the field's largest magnitude, 1e-5
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rigidfibers_b200.generate import sphere_layout
+
+pytestmark = pytest.mark.gpu
+
+
+def _sim(pos, ori, **kw):
+    from rigidfibers_b200 import Config, Simulation
+    return Simulation(Config(**kw), pos, ori)
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 8, 9, 16, 33, 100])
+def test_assembly_matches_oracle(n):
+    pos, ori = sphere_layout(n, radius=max(1.5, 0.8 * n ** (1 / 3)), seed=11 + n)
+    sim = _sim(pos, ori)
+    sim.assembleSystem()
+    A, b = sim.system()
+    p = O.Params()
+    A64, b64 = O.assemble(pos, ori, p, False, np.float64)
+    assert np.abs(A - A64).max() <= 2e-6 * max(1.0, np.abs(A64).max())
+    if n > 1:
+        assert _rel(b, b64) <= 2e-6
+    # every entry written: the diagonal blocks are exactly identity
+    R = 15 * n
+    for i in range(n):
+        blk = A[15 * i:15 * i + 15, 15 * i:15 * i + 15]
+        assert np.array_equal(blk, np.eye(15, dtype=np.float32))
+    assert np.isfinite(A).all() and A.shape == (R, R)
+
+
+FIELDS = [("BVec", "b"), ("XVec", "x"), ("TRANSVel", "tvel"), ("ROTVel", "rvel"), ("POS", "pos"), ("ORIENT", "ori")]
+
+
+def _run_validate(sim, nsteps):
+    out = []
+    for t in range(nsteps):
+        sim.assembleSystem()
+        _, b = sim.system(with_matrix=False)
+        sim.solveSystem()
+        x = sim.solution()
+        sim.updateVelocities()
+        tv, rv = sim.velocities()
+        sim.updateFibers(t == 0)
+        pos, ori = sim.state()
+        out.append(dict(b=b, x=x, tvel=tv, rvel=rv, pos=pos, ori=ori, stats=sim.stats()))
+    return out
+
+
+def test_golden_numeric_gmres(golden):
+    sim = _sim(golden["positions"], golden["orientations"])
+    res = _run_validate(sim, 2)
+    for t in range(2):
+        for f, k in FIELDS:
+            ref = golden["numeric_gmres/%d_%s" % (t, f)]
+            assert _rel(res[t][k], ref) <= 1e-5, (t, f, _rel(res[t][k], ref))
+        assert 0 < res[t]["stats"]["iterations"] <= 20
+        assert res[t]["stats"]["relative_residual"] <= 1e-5
+
+
+def test_step_matches_fp64_oracle_three_steps():
+    pos, ori = sphere_layout(37, radius=2.5, seed=5)
+    p = O.Params()
+    ref = O.run_steps(pos, ori, p, 3, solver="direct", dtype=np.float64)
+    sim = _sim(pos, ori, gmres_tolerance=1e-7)
+    res = _run_validate(sim, 3)
+    for t in range(3):
+        for k in ("b", "x", "tvel", "rvel", "pos", "ori"):
+            assert _rel(res[t][k], ref[t][k]) <= 1e-5, (t, k, _rel(res[t][k], ref[t][k]))
+
+
+def test_step_api_equals_stagewise():
+    pos, ori = sphere_layout(20, radius=2.0, seed=9)
+    a = _sim(pos, ori)
+    b = _sim(pos, ori)
+    for t in range(3):
+        a.step(t)
+    _run_validate(b, 3)
+    pa, oa = a.state()
+    pb, ob = b.state()
+    assert np.array_equal(pa, pb) and np.array_equal(oa, ob)
+
+
+def test_deterministic_repeat():
+    pos, ori = sphere_layout(64, radius=3.0, seed=3)
+    outs = []
+    for _ in range(2):
+        s = _sim(pos, ori)
+        s.run(2)
+        outs.append(s.state())
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_gmres_iteration_limit_reports_noconv():
+    from rigidfibers_b200 import RigidFibersError
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(30, radius=1.6, seed=2)
+    s = _sim(pos, ori, gmres_max_iterations=2, gmres_tolerance=1e-12)
+    s.assembleSystem()
+    with pytest.raises(RigidFibersError) as e:
+        s.solveSystem()
+    assert e.value.status == C.RF_E_NOCONV
+    assert s.stats()["iterations"] == 2
+
+
+def test_dense_matvec_entry_point():
+    import torch
+    from rigidfibers_b200 import _capi as C
+    g = torch.Generator(device="cpu").manual_seed(0)
+    for R in (1, 7, 1500, 4099):
+        A = torch.randn(R, R, generator=g, dtype=torch.float32)
+        x = torch.randn(R, generator=g, dtype=torch.float32)
+        Ad = A.t().contiguous().cuda()  # column-major storage of A
+        xd = x.cuda()
+        yd = torch.empty(R, device="cuda")
+        rc = C.load().rf_dense_matvec(Ad.data_ptr(), xd.data_ptr(), yd.data_ptr(), R,
+                                      torch.cuda.current_stream().cuda_stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        ref = (A.double() @ x.double()).float()
+        assert torch.allclose(yd.cpu(), ref, rtol=1e-4, atol=1e-4 * float(A.abs().max()) * R ** 0.5)
