@@ -149,8 +149,9 @@ int rf_number_of_fibers(rf_handle* h);
 int rf_get_stream(rf_handle* h, void** stream);
 /* Per-launch timing of the solve's matvec kernels (CUDA events around each
  * launch, the role of src/performance.cc's trackers for that kernel).
- * rf_matvec_profile returns launches and summed milliseconds of the last
- * solve. */
+ * rf_matvec_profile returns the matvecs that did work in the last solve
+ * (launches issued after convergence return at once and are not counted)
+ * and the summed milliseconds of all its matvec launches. */
 int rf_set_profiling(rf_handle* h, int enable);
 int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
 

@@ -149,6 +149,7 @@ struct rf_handle {
   std::vector<cudaEvent_t> mv_events;
   int mv_used = 0;
   int launches = 0;
+  int matvecs_done = 0;
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -407,6 +408,7 @@ int rf_solve(rf_handle* h) {
   int rc = gmres_solve(s, mv, h->b, h->x, h->st, &res);
   RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
   h->launches += res.launches + mv_launches;
+  h->matvecs_done = res.matvecs;
   h->stats.iterations = res.iterations;
   h->stats.restarts = res.restarts;
   h->stats.refinement_steps = 0;
@@ -562,7 +564,7 @@ int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms) {
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
   double t = 0.0;
   for (int k = 0; k + 1 < h->mv_used; k += 2) t += elapsed(h->mv_events[k], h->mv_events[k + 1]);
-  *launches = h->mv_used / 2;
+  *launches = h->matvecs_done;
   *total_ms = t;
   return RF_OK;
 }

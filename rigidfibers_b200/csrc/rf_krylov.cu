@@ -412,7 +412,9 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
   res->launches = 2;
   GmresCtl h{};
   int x_zero = 1;
+  int cycles_run = 0;
   for (int cycle = 0;; ++cycle) {
+    ++cycles_run;
     if (!x_zero) {
       int rc = matvec(x, &s.ctl->converged, st);
       if (rc) return rc;
@@ -442,6 +444,7 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
   }
   res->iterations = h.total_iters;
   res->restarts = h.restarts;
+  res->matvecs = h.total_iters + (cycles_run - 1);
   res->relative_residual = h.bnorm > 0 ? h.beta / h.bnorm : 0.0;
   if (h.nan) return RF_E_NAN;
   if (!h.converged) return RF_E_NOCONV;

@@ -52,6 +52,7 @@ struct GmresResult {
   int restarts = 0;
   double relative_residual = 0.0;
   int launches = 0;       // kernels launched (matvec launches counted by the caller's MatvecFn)
+  int matvecs = 0;        // matvecs that did work (launches after convergence return at once)
 };
 
 int krylov_coop_blocks(int64_t R, int num_sms);

@@ -32,9 +32,13 @@ def test_assembly_matches_oracle(n):
     A, b = sim.system()
     p = O.Params()
     A64, b64 = O.assemble(pos, ori, p, False, np.float64)
-    assert np.abs(A - A64).max() <= 2e-6 * max(1.0, np.abs(A64).max())
+    # bound: twice the error of the reference's own REAL*4 arithmetic (the
+    # FP32 oracle) on the same layout, and never looser than 2e-6 absolute
+    A32, b32 = O.assemble(pos, ori, p, False, np.float32)
+    tol_A = max(2e-6, 2.0 * float(np.abs(A32 - A64).max()))
+    assert np.abs(A - A64).max() <= tol_A
     if n > 1:
-        assert _rel(b, b64) <= 2e-6
+        assert _rel(b, b64) <= max(2e-6, 2.0 * _rel(b32, b64))
     # every entry written: the diagonal blocks are exactly identity
     R = 15 * n
     for i in range(n):
