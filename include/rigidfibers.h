@@ -161,6 +161,17 @@ int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
  * ViennaCL prod(A, x) behind the reference's GMRES
  * (lib/viennacl/linalg/cuda/matrix_operations_col.hpp:1251-1278). */
 int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream);
+/* rf_dense_matvec_noalloc: the same y = A x, for callers that cannot let a
+ * library allocate device memory (a host program whose pool allocator owns all
+ * of HBM, or a loop that cannot afford cudaMalloc's latency).  It has no
+ * counterpart in the reference.  Its scratch is a fixed 8 MiB array in the
+ * library's device image (held on every GPU that loads the library until the
+ * process exits), so R must not exceed 131072 (RF_E_INPUT otherwise).  The
+ * first call on a device looks up that array's device address; make that
+ * first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU (different streams, or different host
+ * threads on the same device) race and must be serialised by the caller. */
+int rf_dense_matvec_noalloc(const float* A, const float* x, float* y, int64_t R, void* stream);
 
 const char* rf_status_string(int status);
 const char* rf_last_error(void);
