@@ -239,116 +239,188 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, dist):
+def time_path(args, dist, cfg, pos, ori, clocks=None):
+    """Warm-up, then K device-timed steps (CUDA events on the handle's stream)."""
     import ctypes
 
     import torch
 
-    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200 import Simulation
     from rigidfibers_b200 import _capi as C
-
-    torch.cuda.set_device(dist.local)
-    pos, ori = workload(args)
-    N = args.fibers
-    precision = "fp32" if args.precision == "auto" else args.precision
-    cfg = Config(precision=precision)
-    sim = Simulation(cfg, pos, ori)
     lib = C.load()
+    sim = Simulation(cfg, pos, ori)
     sp = ctypes.c_void_p()
     lib.rf_get_stream(sim._h, ctypes.byref(sp))
     stream = torch.cuda.ExternalStream(sp.value)
-
-    # warm-up
     for t in range(args.warmup):
         sim.step(t)
-    # device-timed region
     lib.rf_set_profiling(sim._h, 1)
-    clocks = Clocks(dist.local)
     dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    if clocks:
+        clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    stage = {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0}
-    iters, launches, mv_launches, mv_ms, restarts = 0, 0, 0, 0.0, 0
+    acc = {"stage": {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0},
+           "iters": 0, "restarts": 0, "refinements": 0, "launches": 0, "mv_launches": 0, "mv_ms": 0.0, "relres": 0.0}
     for t in range(args.warmup, args.warmup + args.steps):
         sim.step(t)
         st = sim.stats()
-        for k in stage:
-            stage[k] += st["ms_" + k]
-        iters += st["iterations"]
-        restarts += st["restarts"]
-        launches += st["kernel_launches"]
+        for k in acc["stage"]:
+            acc["stage"][k] += st["ms_" + k]
+        acc["iters"] += st["iterations"]
+        acc["restarts"] += st["restarts"]
+        acc["refinements"] += st["refinement_steps"]
+        acc["launches"] += st["kernel_launches"]
+        acc["relres"] = max(acc["relres"], st["relative_residual"])
         nl, tm = ctypes.c_int(), ctypes.c_double()
         lib.rf_matvec_profile(sim._h, ctypes.byref(nl), ctypes.byref(tm))
-        mv_launches += nl.value
-        mv_ms += tm.value
+        acc["mv_launches"] += nl.value
+        acc["mv_ms"] += tm.value
     e1.record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    acc["clocks"] = clocks.stop() if clocks else None
     lib.rf_set_profiling(sim._h, 0)
     dist.barrier()
-    ms = e0.elapsed_time(e1)
-    ms_max = dist.max(ms)
-    total_fiber_steps = dist.sum(N * args.steps)
-    value = total_fiber_steps / (ms_max / 1000.0)
+    acc["ms"] = e0.elapsed_time(e1)
+    acc["device_bytes"] = sim.stats()["device_bytes"]
+    sim.close()
+    return acc
 
-    # end-to-end through the C ABI with host buffers: every step copies the
-    # fiber state in from pinned host memory and the new state out
+
+def e2e_path(args, dist, cfg, pos, ori):
+    """Through the C ABI with host buffers: every step uploads the fiber state
+    from pinned host memory and reads the new state back."""
+    import ctypes
+
+    import torch
+
+    from rigidfibers_b200 import Simulation
+    from rigidfibers_b200 import _capi as C
+    lib = C.load()
     hpos = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).pin_memory()
     hori = torch.from_numpy(np.ascontiguousarray(ori, np.float64)).pin_memory()
     out_pos = torch.empty_like(hpos).pin_memory()
     out_ori = torch.empty_like(hori).pin_memory()
-    sim2 = Simulation(cfg, pos, ori)
-    sim2.step(0)
+    sim = Simulation(cfg, pos, ori)
+    sim.step(0)
     dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for t in range(1, 1 + args.steps):
-        C.check(lib.rf_set_state(sim2._h, ctypes.c_void_p(hpos.data_ptr()), ctypes.c_void_p(hori.data_ptr())),
+        C.check(lib.rf_set_state(sim._h, ctypes.c_void_p(hpos.data_ptr()), ctypes.c_void_p(hori.data_ptr())),
                 "rf_set_state")
-        sim2.step(t)
-        C.check(lib.rf_get_state(sim2._h, ctypes.c_void_p(out_pos.data_ptr()), ctypes.c_void_p(out_ori.data_ptr())),
+        sim.step(t)
+        C.check(lib.rf_get_state(sim._h, ctypes.c_void_p(out_pos.data_ptr()), ctypes.c_void_p(out_ori.data_ptr())),
                 "rf_get_state")
     torch.cuda.synchronize()
-    e2e_s = dist.max(time.perf_counter() - t0)
+    s = dist.max(time.perf_counter() - t0)
+    sim.close()
+    return s
+
+
+def error_vs_fp64(precision, n=300):
+    """Relative error of the given path against the FP64 oracle (direct
+    solve) on a seeded layout of n fibers at the workload's density, 2 steps."""
+    from oracle import oracle as O
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    radius = 18.0 * (n / 4000.0) ** (1.0 / 3.0)
+    pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(3, n))
+    ref = O.run_steps(pos, ori, O.Params(), 2, solver="direct", dtype=np.float64)
+    sim = Simulation(Config(precision=precision), pos, ori)
+    err = {"fibers": n, "steps": 2}
+    for t in range(2):
+        sim.assembleSystem()
+        sim.solveSystem()
+        x = sim.solution()
+        sim.updateVelocities()
+        tv, rv = sim.velocities()
+        sim.updateFibers(t == 0)
+        p1, o1 = sim.state()
+        for k, v in (("forces", x), ("tvel", tv), ("rvel", rv), ("pos", p1), ("ori", o1)):
+            r = np.asarray(ref[t][{"forces": "x"}.get(k, k)]).reshape(-1)
+            e = float(np.abs(np.asarray(v).reshape(-1) - r).max() / np.abs(r).max())
+            err[k] = max(err.get(k, 0.0), e)
+    sim.close()
+    return err
+
+
+def run_ours(args, dist):
+    import torch
+
+    from rigidfibers_b200 import Config
+
+    torch.cuda.set_device(dist.local)
+    pos, ori = workload(args)
+    N = args.fibers
+    R = 15 * N
+    precision = "mixed_fp16" if args.precision == "auto" else args.precision
+    cfg = Config(precision=precision)
+    head = time_path(args, dist, cfg, pos, ori, clocks=Clocks(dist.local))
+    ms_max = dist.max(head["ms"])
+    total_fiber_steps = dist.sum(N * args.steps)
+    value = total_fiber_steps / (ms_max / 1000.0)
+    e2e_s = e2e_path(args, dist, cfg, pos, ori)
     e2e_value = total_fiber_steps / e2e_s
-    sim2.close()
     # bytes the C ABI moves per step: rf_set_state uploads double4 prev+cur
     # position/orientation and their float4 copies; rf_get_state reads double4 pos/ori
     h2d = N * (2 * 2 * 32 + 2 * 16)
     d2h = N * 2 * 32
 
-    R = 15 * N
+    comparison = None
+    if precision != "fp32":
+        plain = time_path(args, dist, Config(precision="fp32"), pos, ori)
+        plain_ms = dist.max(plain["ms"])
+        comparison = {"precision": "fp32", "value": total_fiber_steps / (plain_ms / 1000.0),
+                      "ms_per_step": plain_ms / args.steps,
+                      "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
+                      "gmres_iterations_per_step": plain["iters"] / args.steps,
+                      "matvec_ms": plain["mv_ms"] / max(plain["mv_launches"], 1)}
+
     hbm, peak_kind = peaks()
-    mv_avg_ms = mv_ms / max(mv_launches, 1)
-    bytes_per_matvec = 4.0 * R * R
-    achieved = bytes_per_matvec / (mv_avg_ms / 1000.0) / 1e9 if mv_launches else None
-    roof = {"kernel": "k_gemv_cm_f32 (dense FP32 column-major matvec, GMRES)", "bound": "hbm",
-            "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-            "frac": (achieved / hbm) if achieved else None, "traffic": None,
+    mvn = max(head["mv_launches"], 1)
+    mv_avg_ms = head["mv_ms"] / mvn
+    if precision == "fp32":
+        kernel = "k_gemv_cm_f32 (dense FP32 column-major matvec, GMRES)"
+        bytes_per_matvec = 4.0 * R * R
+    else:
+        kernel = "k_struct_z<5,8,FP16> + k_struct_finalize (16-bit structured matvec, GMRES)"
+        bytes_per_matvec = 2.0 * 150 * N * (N - 1) / 2
+    achieved = bytes_per_matvec / (mv_avg_ms / 1000.0) / 1e9 if head["mv_launches"] else None
+    roof = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
             "algorithmic_bytes_per_launch": bytes_per_matvec, "avg_launch_ms": mv_avg_ms,
-            "launches": mv_launches, "share_of_step_time": mv_ms / ms if ms else None}
+            "launches": head["mv_launches"], "share_of_step_time": head["mv_ms"] / head["ms"] if head["ms"] else None}
     out = {
         "metric": METRIC, "value": value, "unit": "fiber-steps/s", "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if precision == "fp32" else "f16/bf16 storage, f32 accumulate, f64 refine",
+        "vs_baseline": None,
+        "dtype": "f32" if precision == "fp32" else "%s storage, f32 accumulate, f64 refinement" % precision[6:],
         "data": "synthetic",
         "config": {"workload": workload_name(args), "fibers": N, "radius": args.radius, "precision": precision,
                    "parallelism": "replicas x%d" % dist.world,
-                   "l2": "inputs larger than L2: the %.1f GB matrix is re-assembled and re-read every step"
-                         % (4.0 * R * R / 1e9)},
-        "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
-        "gmres_iterations_per_step": iters / args.steps, "gmres_restarts_per_step": restarts / args.steps,
-        "roofline": roof, "clocks": clk,
+                   "l2": "inputs larger than L2: the operator (%.1f GB) is re-assembled and re-read every step"
+                         % (head["device_bytes"] / 1e9)},
+        "stage_ms_per_step": {k: v / args.steps for k, v in head["stage"].items()},
+        "gmres_iterations_per_step": head["iters"] / args.steps,
+        "gmres_restarts_per_step": head["restarts"] / args.steps,
+        "refinements_per_step": head["refinements"] / args.steps,
+        "max_relative_residual": head["relres"],
+        "roofline": roof, "clocks": head["clocks"],
         "e2e": {"value": e2e_value, "unit": "fiber-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
+        "gpu_launches": head["launches"],
     }
-    sim.close()
+    if comparison:
+        out["fp32_path"] = comparison
+        out["speedup_vs_fp32"] = value / comparison["value"]
     if dist.rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_sample(pos, ori, max(1, iters // args.steps), max(1, restarts // args.steps),
-                                         args.cpu_seconds)
+        out["error_vs_fp64"] = error_vs_fp64(precision)
+        # the CPU port runs the reference's FP32 GMRES: its matvec count is the FP32 path's
+        src = plain if comparison else head
+        out["cpu_baseline"] = cpu_sample(pos, ori, max(1, src["iters"] // args.steps),
+                                         max(1, src["restarts"] // args.steps), args.cpu_seconds)
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
 

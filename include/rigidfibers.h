@@ -143,6 +143,14 @@ int rf_last_stats(rf_handle* h, rf_stats* s);
 int rf_get_config(rf_handle* h, rf_config* cfg);
 int rf_number_of_fibers(rf_handle* h);
 
+/* y = A x with the assembled operator (3MN doubles in and out; after
+ * rf_assemble).  which = 0: the working-precision operator (dense FP32 A, or
+ * the FP32 pair blocks with FP64 accumulation in mixed mode); which = 1: the
+ * 16-bit pair blocks of mixed mode.  Replaces the product inside the
+ * reference's solver (ViennaCL prod(A, x), fortran/solve_system.incl:152)
+ * for callers that run their own iteration.  Invalidates the last solution. */
+int rf_operator_apply(rf_handle* h, const double* x, double* y, int which);
+
 /* The handle's CUDA stream (cudaStream_t), for callers that order their
  * own work or events after the handle's (the reference used the default
  * stream synchronously, src/simulation.cu). */

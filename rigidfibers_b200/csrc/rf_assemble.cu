@@ -10,16 +10,25 @@
 // b_i -= C_i T^{ij}_{.,P0} F/2, where C_i is D1 t t^T (force index 0) or
 // gamma_k (I - E_k t t^T).  How it is computed is not the reference's:
 //  * K is even in R, so T^{ji}_{kj,ki} = T^{ij}_{ki,kj}: one CTA tile of
-//    unordered fiber pairs evaluates K once per (qi, qj) and writes both
+//    unordered fiber pairs evaluates K once per (qi, qj) and serves both
 //    blocks (i,j) and (j,i)  -- half the kernel evaluations;
 //  * the reference re-evaluates K once per k_j (M times); here once;
 //  * the quadrature is mirror-symmetric (s_{Q-1-q} = -s_q, w equal, P_k of
 //    parity k), so both contractions fold q with Q-1-q into an even and an
 //    odd part and use half the multiply-adds;
-//  * b is reduced deterministically (per-tile partial rows, then a fixed
-//    order sum) instead of float atomics.
-// Layout: A column-major with leading dimension lda >= R (padded to 32 so
-// every column starts on a 128-byte boundary), entry (r, c) at A[r + c*lda].
+//  * the force terms F_i[k] = sum_j T^{ij}_{k,P0} F/2 are reduced
+//    deterministically (per-tile partial rows, then a fixed-order sum)
+//    instead of with float atomics; b_i = -C_i F_i.
+//
+// Two outputs share the pair-tile core:
+//  * dense:      A column-major with leading dimension lda >= R (padded to 32
+//                so every column starts on a 128-byte boundary), A[r + c*lda];
+//  * structured: the blocks T^{ij}_{k,kj}, k,kj = P_0..P_M, once per
+//                unordered pair, in FP32 (all (M+1)^2 blocks) and in 16 bits
+//                (the M^2 blocks of the operator), laid out per 16x16 fiber
+//                storage tile as [tile][sub-tile][j][value][i] so that one
+//                CTA's writes for one j are contiguous and the matvec reads
+//                whole 32-byte sectors (see rf_struct.cu).
 #include "rf_common.cuh"
 #include "rf_kernels.cuh"
 
@@ -34,6 +43,8 @@ __device__ __forceinline__ void tile_pair(int64_t L, int& I, int& J) {
   I = (int)(L - j * (j + 1) / 2);
 }
 
+enum AsmMode { kAsmDense = 0, kAsmStructF16 = 1, kAsmStructBF16 = 2 };
+
 template <int M, int Q>
 struct AsmShape {
   static constexpr int TI = 192 / Q;     // fibers per tile side
@@ -41,30 +52,48 @@ struct AsmShape {
   static constexpr int K1 = M + 1;       // P_0..P_M
   static constexpr int NC = 6 * K1;      // G columns per unit
   static constexpr int H = Q / 2;        // folded quadrature points
-  // dynamic shared memory: G columns per unit, then the T blocks (6 floats each)
-  static constexpr size_t kGBytes = sizeof(float) * NC * U;
+  // dynamic shared memory: G columns per unit (rows padded to an odd stride so
+  // that phase 2, where consecutive threads read consecutive columns, is free
+  // of bank conflicts), then the T blocks (6 floats each)
+  static constexpr int GS = U + 1;
+  static constexpr size_t kGBytes = sizeof(float) * NC * GS;
   static constexpr size_t kTBytes = sizeof(float) * TI * K1 * K1 * 6;
   static constexpr size_t kSmem = kGBytes + kTBytes;
+  // structured storage
+  static constexpr int SUB = kStoreTile / TI;      // assembly tiles per storage-tile side
+  static constexpr int NQ32 = K1 * K1 * 6;         // FP32 values per pair
+  static constexpr int NQ16 = M * M * 6 / 2;       // 16-bit pairs per pair (M*M*6 is even)
+  static_assert(kStoreTile % TI == 0, "assembly tile must divide the storage tile");
 };
 
-// One CTA = one tile pair (I, J), I <= J, of TI x TI fibers.  192 threads:
-// thread u < TI*Q owns (fiber il = u / Q of tile I, quadrature point qi).
-template <int M, int Q>
-__global__ void __launch_bounds__(192, 3)
+struct AsmOut {
+  // dense
+  float* A;
+  int64_t lda;
+  // structured
+  float* S32;
+  uint32_t* S16;
+  // both: partial force terms ffpart[X][i][k][3]
+  float* ffpart;
+};
+
+template <int M, int Q, int MODE>
+__global__ void __launch_bounds__(192, 4)
 k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
-                     float* __restrict__ A, int64_t lda, float* __restrict__ bpart, int64_t R) {
+                     AsmOut out) {
   using S = AsmShape<M, Q>;
   constexpr int TI = S::TI, K1 = S::K1, NC = S::NC, H = S::H;
   constexpr int M3 = 3 * M;
+  constexpr int FF = K1 * 3;   // force-term floats per fiber
   static_assert(Q % 2 == 0, "mirror folding needs an even number of quadrature points");
 
   __shared__ float4 sPj[TI][Q];          // x_j + s_q t_j for the J tile
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
   extern __shared__ __align__(16) float smem_dyn[];
-  float (*sG)[S::U] = reinterpret_cast<float (*)[S::U]>(smem_dyn);                            // [NC][U]
-  float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(smem_dyn + NC * S::U);      // [TI][K1][K1][6]
+  float (*sG)[S::GS] = reinterpret_cast<float (*)[S::GS]>(smem_dyn);                          // [NC][GS]
+  float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(smem_dyn + NC * S::GS);     // [TI][K1][K1][6]
   __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
-  __shared__ float sbJ[TI][M3];
+  __shared__ float sfJ[TI][FF];
 
   int I, J;
   tile_pair(blockIdx.x, I, J);
@@ -85,7 +114,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     const float s = tab.pts[q];
     sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
   }
-  for (int k = tid; k < TI * M3; k += blockDim.x) (&sbJ[0][0])[k] = 0.f;
+  for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
 
   // own unit
   const int il = tid / Q, qi = tid % Q;
@@ -99,9 +128,10 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
   }
   const float e2 = tab.e2;
   const float e2x3 = -3.f * e2;
+  const float fz = tab.fz_half;
 
-  // b_i accumulator for task (il_b, kI) = (tid / M, tid % M)
-  float bacc[3] = {0.f, 0.f, 0.f};
+  // force-term accumulator of task (tl, k) = (tid / K1, tid % K1): F_i[k]
+  float facc[3] = {0.f, 0.f, 0.f};
   __syncthreads();
 
   const int jcount = min(TI, N - j0);
@@ -173,20 +203,20 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     }
     __syncthreads();
 
-    // ---- phase 3a: block (i, j) -- rows of fiber i, columns of fiber j
     const int j = j0 + jl;
-    {
+    if constexpr (MODE == kAsmDense) {
+      // ---- phase 3a: block (i, j) -- rows of fiber i, columns of fiber j
       for (int task = tid; task < TI * M * M; task += blockDim.x) {
         const int kJp = task / (TI * M), rem = task % (TI * M);
         const int tl = rem / M, kIp = rem % M;
         const int ii = i0 + tl;
         if (ii >= N || (diag && tl > jl)) continue;
-        float* dst = A + (int64_t)(i0 * M3 + 3 * rem) + (int64_t)(j * M3 + 3 * kJp) * lda;
+        float* dst = out.A + (int64_t)(i0 * M3 + 3 * rem) + (int64_t)(j * M3 + 3 * kJp) * out.lda;
         if (diag && tl == jl) {
 #pragma unroll
           for (int b = 0; b < 3; ++b)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) dst[a + b * lda] = (kIp == kJp && a == b) ? 1.f : 0.f;
+            for (int a = 0; a < 3; ++a) dst[a + b * out.lda] = (kIp == kJp && a == b) ? 1.f : 0.f;
           continue;
         }
         const float* T6 = sT[tl][kIp + 1][kJp + 1];
@@ -201,117 +231,152 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
         for (int b = 0; b < 3; ++b)
 #pragma unroll
           for (int a = 0; a < 3; ++a)
-            dst[a + b * lda] = kIp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
+            dst[a + b * out.lda] = kIp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
+      }
+      // ---- phase 3b: block (j, i) -- rows of fiber j, columns of fiber i
+      {
+        const float4 tj = sTj[jl];
+        const float t3[3] = {tj.x, tj.y, tj.z};
+        for (int task = tid; task < TI * M * M; task += blockDim.x) {
+          const int tl = task / (M * M), rem = task % (M * M);
+          const int kIp = rem / M, kJp = rem % M;
+          const int ii = i0 + tl;
+          if (ii >= N || (diag && tl >= jl)) continue;
+          float* dst = out.A + (int64_t)(j * M3 + 3 * kJp) + (int64_t)(ii * M3 + 3 * kIp) * out.lda;
+          const float* T6 = sT[tl][kIp + 1][kJp + 1];
+          float Qv[3];
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+            Qv[b] = sym_get(T6, b, 0) * t3[0] + sym_get(T6, b, 1) * t3[1] + sym_get(T6, b, 2) * t3[2];
+          const float coef = sCoef[kJp], E = sEig[kJp];
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              dst[a + b * out.lda] = kJp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
+        }
+      }
+    } else {
+      // ---- phase 3: the pair blocks into structured storage; one j, all i of
+      // the tile: [jl][q][tl] is a contiguous run of NQ32*TI floats
+      const int I16 = I / S::SUB, J16 = J / S::SUB;
+      const int sub = (I % S::SUB) * S::SUB + (J % S::SUB);
+      const int64_t L16 = (int64_t)J16 * (J16 + 1) / 2 + I16;
+      const int64_t rec = (L16 * S::SUB * S::SUB + sub) * TI + jl;
+      float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
+      for (int v = tid; v < S::NQ32 * TI; v += blockDim.x) {
+        const int tl = v % TI, q = v / TI;
+        const int c = q % 6, kk = q / 6;
+        const bool ok = (i0 + tl < N) && (!diag || tl < jl);
+        d32[v] = ok ? sT[tl][kk / K1][kk % K1][c] : 0.f;
+      }
+      uint32_t* d16 = out.S16 + rec * (int64_t)(S::NQ16 * TI);
+      for (int v = tid; v < S::NQ16 * TI; v += blockDim.x) {
+        const int tl = v % TI, q2 = v / TI;
+        const bool ok = (i0 + tl < N) && (!diag || tl < jl);
+        float f[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int q = 2 * q2 + h;
+          const int c = q % 6, blk = q / 6;
+          f[h] = ok ? sT[tl][blk / M + 1][blk % M + 1][c] : 0.f;
+        }
+        uint32_t word;
+        if constexpr (MODE == kAsmStructF16) {
+          __half2 hv = __floats2half2_rn(f[0], f[1]);
+          word = *reinterpret_cast<uint32_t*>(&hv);
+        } else {
+          __nv_bfloat162 hv = __floats2bfloat162_rn(f[0], f[1]);
+          word = *reinterpret_cast<uint32_t*>(&hv);
+        }
+        d16[v] = word;
       }
     }
-    // ---- phase 3b: block (j, i) -- rows of fiber j, columns of fiber i
-    {
-      const float4 tj = sTj[jl];
-      const float t3[3] = {tj.x, tj.y, tj.z};
-      for (int task = tid; task < TI * M * M; task += blockDim.x) {
-        const int tl = task / (M * M), rem = task % (M * M);
-        const int kIp = rem / M, kJp = rem % M;
-        const int ii = i0 + tl;
-        if (ii >= N || (diag && tl >= jl)) continue;
-        float* dst = A + (int64_t)(j * M3 + 3 * kJp) + (int64_t)(ii * M3 + 3 * kIp) * lda;
-        const float* T6 = sT[tl][kIp + 1][kJp + 1];
-        float Qv[3];
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-          Qv[b] = sym_get(T6, b, 0) * t3[0] + sym_get(T6, b, 1) * t3[1] + sym_get(T6, b, 2) * t3[2];
-        const float coef = sCoef[kJp], E = sEig[kJp];
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            dst[a + b * lda] = kJp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
-      }
-    }
-    // ---- phase 3c: right-hand side, b_i from (i,j) and b_j from (j,i)
-    const float fz = tab.fz_half;
-    if (tid < TI * M) {
-      const int tl = tid / M, kIp = tid % M;
+    // ---- phase 3c: force terms F_i[k] += T^{ij}[k][P0] F/2 and
+    //      F_j[kj] += T^{ij}[P0][kj] F/2 (F/2 = (0, 0, fz): column z of the block)
+    if (tid < TI * K1) {
+      const int tl = tid / K1, k = tid % K1;
       if (i0 + tl < N && (!diag || tl < jl)) {
-        const float* T6 = sT[tl][kIp + 1][0];
-        const float4 ti = sTi[tl];
-        const float t3[3] = {ti.x, ti.y, ti.z};
-        const float TF[3] = {T6[4] * fz, T6[5] * fz, T6[2] * fz};   // T (0,0,fz)
-        const float QF = TF[0] * t3[0] + TF[1] * t3[1] + TF[2] * t3[2];
-        const float coef = sCoef[kIp], E = sEig[kIp];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) bacc[a] -= kIp == 0 ? coef * t3[a] * QF : coef * (TF[a] - E * t3[a] * QF);
+        const float* T6 = sT[tl][k][0];
+        facc[0] = fmaf(T6[4], fz, facc[0]);
+        facc[1] = fmaf(T6[5], fz, facc[1]);
+        facc[2] = fmaf(T6[2], fz, facc[2]);
       }
     }
-    if (tid < M) {
-      const int kJp = tid;
-      const float4 tj = sTj[jl];
-      const float t3[3] = {tj.x, tj.y, tj.z};
-      const float coef = sCoef[kJp], E = sEig[kJp];
+    if (tid < K1) {
+      const int kj = tid;
       float s[3] = {0.f, 0.f, 0.f};
       for (int tl = 0; tl < TI; ++tl) {
         if (i0 + tl >= N || (diag && tl >= jl)) continue;
-        const float* T6 = sT[tl][0][kJp + 1];
-        const float TF[3] = {T6[4] * fz, T6[5] * fz, T6[2] * fz};
-        const float QF = TF[0] * t3[0] + TF[1] * t3[1] + TF[2] * t3[2];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) s[a] -= kJp == 0 ? coef * t3[a] * QF : coef * (TF[a] - E * t3[a] * QF);
+        const float* T6 = sT[tl][0][kj];
+        s[0] = fmaf(T6[4], fz, s[0]);
+        s[1] = fmaf(T6[5], fz, s[1]);
+        s[2] = fmaf(T6[2], fz, s[2]);
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) sbJ[jl][3 * kJp + a] += s[a];
+      for (int a = 0; a < 3; ++a) sfJ[jl][3 * kj + a] += s[a];
     }
     __syncthreads();
   }
 
-  // ---- partial right-hand sides: bpart[X][rows of Y] written exactly once
-  if (tid < TI * M) {
-    const int tl = tid / M;
+  // ---- partial force terms: ffpart[X][fiber of Y][k][3] written exactly once
+  float* ffpart = out.ffpart;
+  if (tid < TI * K1) {
+    const int tl = tid / K1, k = tid % K1;
     if (i0 + tl < N) {
-      float v[3] = {bacc[0], bacc[1], bacc[2]};
+      float v[3] = {facc[0], facc[1], facc[2]};
       if (diag) {
-        const int kIp = tid % M;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) v[a] += sbJ[tl][3 * kIp + a];
+        for (int a = 0; a < 3; ++a) v[a] += sfJ[tl][3 * k + a];
       }
-      float* dst = bpart + (int64_t)J * R + (int64_t)i0 * M3 + 3 * tid;
+      float* dst = ffpart + ((int64_t)J * N + i0 + tl) * FF + 3 * k;
 #pragma unroll
       for (int a = 0; a < 3; ++a) dst[a] = v[a];
     }
   }
   if (!diag) {
-    for (int k = tid; k < TI * M3; k += blockDim.x) {
-      const int jl = k / M3;
-      if (j0 + jl < N) bpart[(int64_t)I * R + (int64_t)j0 * M3 + k] = (&sbJ[0][0])[k];
+    for (int k = tid; k < TI * FF; k += blockDim.x) {
+      const int jl = k / FF;
+      if (j0 + jl < N) ffpart[((int64_t)I * N + j0) * FF + k] = (&sfJ[0][0])[k];
     }
   }
 }
 
-// b[r] = sum over tiles X of bpart[X][r], fixed order.
+// F[i][k] = sum_X ffpart[X][i][k] (fixed order); b[i][k'] = -C_i(k') F[i][k'+1].
+__global__ void k_force_terms(const Tables tab, int N, const float4* __restrict__ ori,
+                              const float* __restrict__ ffpart, int nparts, float* __restrict__ F,
+                              float* __restrict__ b) {
+  const int M = tab.M, K1 = M + 1, FFn = 3 * K1;
+  const int64_t n = (int64_t)N * K1;
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(u / K1), k = (int)(u % K1);
+    float s[3] = {0.f, 0.f, 0.f};
+    for (int p = 0; p < nparts; ++p) {
+      const float* src = ffpart + ((int64_t)p * N + i) * FFn + 3 * k;
+      s[0] += src[0]; s[1] += src[1]; s[2] += src[2];
+    }
+    float* f = F + (int64_t)i * FFn + 3 * k;
+    f[0] = s[0]; f[1] = s[1]; f[2] = s[2];
+    if (k >= 1) {
+      const int kp = k - 1;
+      const float4 t = ori[i];
+      const float t3[3] = {t.x, t.y, t.z};
+      const float QF = s[0] * t3[0] + s[1] * t3[1] + s[2] * t3[2];
+      const float coef = tab.gamma[kp], E = tab.eigen[kp];
+      float* dst = b + (int64_t)i * 3 * M + 3 * kp;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) dst[a] = kp == 0 ? -coef * t3[a] * QF : -coef * (s[a] - E * t3[a] * QF);
+    }
+  }
+}
+
+// out[r] = sum over parts p of part[p][r], fixed order.
 __global__ void k_reduce_rows(const float* __restrict__ part, int nparts, int64_t R, float* __restrict__ out) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
     float s = 0.f;
     for (int p = 0; p < nparts; ++p) s += part[(int64_t)p * R + r];
     out[r] = s;
   }
-}
-
-int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st);
-
-template <int M, int Q>
-static int launch_assemble_numerical_mq(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                                        int64_t lda, float* bpart, float* b, cudaStream_t st) {
-  using S = AsmShape<M, Q>;
-  const int64_t T = ceil_div(N, S::TI);
-  const int64_t ntp = T * (T + 1) / 2;
-  const int64_t R = (int64_t)3 * M * N;
-  static bool attr_set = false;  // per process; the attribute is per function
-  if (!attr_set) {
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_numerical<M, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)S::kSmem));
-    attr_set = true;
-  }
-  k_assemble_numerical<M, Q><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, A, lda, bpart, R);
-  RF_LAUNCH_CHECK();
-  return launch_reduce_rows(bpart, (int)T, R, b, st);
 }
 
 int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st) {
@@ -322,18 +387,70 @@ int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cud
   return RF_OK;
 }
 
-int assemble_tiles(int M, int Q, int N) {
-  return (int)ceil_div(N, 192 / Q);
+int assemble_tiles(int M, int Q, int N) { return (int)ceil_div(N, 192 / Q); }
+
+int64_t struct_store_tiles(int N) {
+  const int64_t T16 = ceil_div(N, kStoreTile);
+  return T16 * (T16 + 1) / 2;
 }
 
-int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                              int64_t lda, float* bpart, float* b, cudaStream_t st) {
+int64_t struct_floats32(int M, int N) {
+  return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * (M + 1) * (M + 1) * 6;
+}
+
+int64_t struct_words16(int M, int N) {
+  return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * M * M * 3;
+}
+
+template <int M, int Q, int MODE>
+static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
+                              float* F, float* b, cudaStream_t st) {
+  using S = AsmShape<M, Q>;
+  const int64_t T = ceil_div(N, S::TI);
+  const int64_t ntp = T * (T + 1) / 2;
+  static bool attr_set = false;  // per process; the attribute is per function
+  if (!attr_set) {
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_numerical<M, Q, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)S::kSmem));
+    attr_set = true;
+  }
+  k_assemble_numerical<M, Q, MODE><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
+  RF_LAUNCH_CHECK();
+  const int64_t n = (int64_t)N * (M + 1);
+  k_force_terms<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 8), 256, 0, st>>>(tab, N, ori, out.ffpart,
+                                                                                         (int)T, F, b);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+template <int MODE>
+static int dispatch_assemble(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
+                             float* F, float* b, cudaStream_t st) {
 #define RF_ASM_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) return launch_assemble_numerical_mq<MM, QQ>(tab, N, pos, ori, A, lda, bpart, b, st);
+  if (tab.M == MM && tab.Q == QQ) return launch_assemble_mq<MM, QQ, MODE>(tab, N, pos, ori, out, F, b, st);
   RF_FOR_EACH_MQ(RF_ASM_CASE)
 #undef RF_ASM_CASE
   set_last_error_str("assemble: (M, Q) combination not instantiated");
   return RF_E_UNSUPPORTED;
+}
+
+int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
+                              int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
+  AsmOut out{};
+  out.A = A;
+  out.lda = lda;
+  out.ffpart = ffpart;
+  return dispatch_assemble<kAsmDense>(tab, N, pos, ori, out, F, b, st);
+}
+
+int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
+                               uint32_t* S16, bool bf16, float* ffpart, float* F, float* b, cudaStream_t st) {
+  AsmOut out{};
+  out.S32 = S32;
+  out.S16 = S16;
+  out.ffpart = ffpart;
+  if (bf16) return dispatch_assemble<kAsmStructBF16>(tab, N, pos, ori, out, F, b, st);
+  return dispatch_assemble<kAsmStructF16>(tab, N, pos, ori, out, F, b, st);
 }
 
 }  // namespace rf

@@ -123,10 +123,18 @@ struct rf_handle {
   int vprev = 0, vcur = 1;   // velocity buffers; vcur is written by update_velocities
   int vlast = -1;            // buffer holding the most recent velocities
   // linear system
-  float* A = nullptr;
+  bool mixed = false;        // structured operator + refinement (RF_PREC_MIXED_*)
+  float* A = nullptr;        // dense FP32 (RF_PREC_FP32)
+  float* S32 = nullptr;      // structured FP32 blocks (mixed)
+  uint32_t* S16 = nullptr;   // structured 16-bit blocks (mixed)
+  float* zpart = nullptr;    // structured matvec partial rows
+  double* zpart64 = nullptr; // FP64 residual partial rows
+  double* x64 = nullptr;     // FP64 solution (mixed)
   float* b = nullptr;
   float* x = nullptr;
-  float* bpart = nullptr;
+  float* ffpart = nullptr;   // force-term partials
+  float* F = nullptr;        // force terms sum_j T^{ij}[k][P0] F/2
+  float* svpart = nullptr;   // structured velocity partials
   // Krylov scratch
   float* V = nullptr;
   float* ypart = nullptr;
@@ -150,6 +158,7 @@ struct rf_handle {
   int mv_used = 0;
   int launches = 0;
   int matvecs_done = 0;
+  int refinements = 0;
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -196,7 +205,18 @@ static int validate_config(const rf_config* c, int N) {
   if (c->solver < 0 || c->solver > 2 || c->integration < 0 || c->integration > 1) {
     set_last_error_str("solver / integration"); return RF_E_INPUT;
   }
-  if (c->precision != RF_PREC_FP32) { set_last_error_str("precision mode not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->precision < RF_PREC_FP32 || c->precision > RF_PREC_MIXED_BF16) { set_last_error_str("precision"); return RF_E_INPUT; }
+  if (c->precision != RF_PREC_FP32 && c->integration != RF_NUMERICAL) {
+    set_last_error_str("mixed precision uses the symmetric pair blocks of numerical integration");
+    return RF_E_UNSUPPORTED;
+  }
+  if (c->precision != RF_PREC_FP32 && c->solver != RF_SOLVER_GMRES) {
+    set_last_error_str("mixed precision refines inside GMRES");
+    return RF_E_UNSUPPORTED;
+  }
+  if (c->precision != RF_PREC_FP32 && !(c->refinement_tolerance > 0.0)) {
+    set_last_error_str("refinement_tolerance must be positive"); return RF_E_INPUT;
+  }
   if (c->integration == RF_ANALYTICAL) { set_last_error_str("analytical integration not built yet"); return RF_E_UNSUPPORTED; }
   if (c->solver != RF_SOLVER_GMRES) { set_last_error_str("solver not built yet"); return RF_E_UNSUPPORTED; }
   if (c->gmres_restart < 1 || c->gmres_restart > kMaxRestart) { set_last_error_str("gmres restart in [1, 64]"); return RF_E_INPUT; }
@@ -309,14 +329,28 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
     rc = h->alloc((void**)&h->tv[s], b32);
     if (!rc) rc = h->alloc((void**)&h->rv[s], b32);
   }
-  if (!rc) rc = h->alloc((void**)&h->A, (size_t)h->lda * (size_t)R * sizeof(float));
+  h->mixed = cfg->precision != RF_PREC_FP32;
+  const int64_t T16 = ceil_div(N, kStoreTile);
+  if (!h->mixed) {
+    if (!rc) rc = h->alloc((void**)&h->A, (size_t)h->lda * (size_t)R * sizeof(float));
+  } else {
+    if (!rc) rc = h->alloc((void**)&h->S32, (size_t)struct_floats32(h->M, N) * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&h->S16, (size_t)struct_words16(h->M, N) * sizeof(uint32_t));
+    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)T16 * (size_t)R * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&h->zpart64, (size_t)T16 * (size_t)R * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&h->x64, (size_t)R * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&h->svpart, (size_t)T16 * N * 6 * sizeof(float));
+  }
   if (!rc) rc = h->alloc((void**)&h->b, (size_t)R * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->x, (size_t)R * sizeof(float));
   const int tiles = assemble_tiles(h->M, h->Q, N);
-  if (!rc) rc = h->alloc((void**)&h->bpart, (size_t)tiles * (size_t)R * sizeof(float));
+  const size_t ffn = (size_t)N * 3 * (h->M + 1);
+  if (!rc) rc = h->alloc((void**)&h->ffpart, (size_t)tiles * ffn * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->F, ffn * sizeof(float));
   // Krylov
   const int m = cfg->gmres_restart;
   h->gemv_plan = plan_dense_gemv(R, h->num_sms);
+  if (h->mixed) h->gemv_plan.splits = 1;  // the structured matvec writes complete rows
   h->coop_blocks = krylov_coop_blocks(R, h->num_sms);
   const int64_t ldv = ceil_div(R, 32) * 32;
   if (!rc) rc = h->alloc((void**)&h->V, (size_t)(m + 1) * (size_t)ldv * sizeof(float));
@@ -355,7 +389,11 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
 int rf_assemble(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
-  RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->bpart, h->b, h->st));
+  if (h->mixed)
+    RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->S32, h->S16,
+                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st));
+  else
+    RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
   h->launches += 2;
   RF_CUDA_TRY(cudaEventRecord(h->ev[1], h->st));
   h->assembled = true;
@@ -371,7 +409,7 @@ int rf_solve(rf_handle* h) {
   s.R = h->R;
   s.m = h->cfg.gmres_restart;
   s.maxit = h->cfg.gmres_max_iterations;
-  s.tol = h->cfg.gmres_tolerance;
+  s.tol = h->mixed ? h->cfg.refinement_tolerance : h->cfg.gmres_tolerance;
   s.V = h->V;
   s.ldv = ceil_div(h->R, 32) * 32;
   s.ypart = h->ypart;
@@ -400,18 +438,42 @@ int rf_solve(rf_handle* h) {
       RF_CUDA_TRY(cudaEventRecord(e0, st));
     }
     ++mv_launches;
-    int rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
+    int rc;
+    if (h->mixed) {
+      const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+      rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip, st);
+      ++mv_launches;
+    } else {
+      rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
+    }
     if (h->profile) RF_CUDA_TRY(cudaEventRecord(e1, st));
     return rc;
   };
   GmresResult res;
-  int rc = gmres_solve(s, mv, h->b, h->x, h->st, &res);
+  int rc;
+  if (h->mixed) {
+    ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
+      h->refinements += 1;
+      return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
+                                      h->b, r, skip, st);
+    };
+    h->refinements = 0;
+    rc = gmres_solve_ex(s, mv, resid, h->b, h->x64, true, h->st, &res);
+    if (rc == RF_OK || rc == RF_E_NOCONV) {
+      int rc2 = launch_cast_to_float(h->x64, h->x, h->R, h->st);
+      if (rc2) return rc2;
+      h->launches += 1;
+    }
+    h->launches += 2 * h->refinements;
+  } else {
+    rc = gmres_solve(s, mv, h->b, h->x, h->st, &res);
+  }
   RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
   h->launches += res.launches + mv_launches;
   h->matvecs_done = res.matvecs;
   h->stats.iterations = res.iterations;
   h->stats.restarts = res.restarts;
-  h->stats.refinement_steps = 0;
+  h->stats.refinement_steps = h->mixed ? h->refinements : 0;
   h->stats.relative_residual = res.relative_residual;
   if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
   h->solved = true;
@@ -422,9 +484,15 @@ int rf_update_velocities(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   if (!h->solved) { set_last_error_str("rf_update_velocities before rf_solve"); return RF_E_STATE; }
   RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
-  RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos32, h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
-                                   h->rv[h->vcur], h->st));
-  h->launches += 3;
+  if (h->mixed) {
+    RF_TRY(launch_struct_velocity(h->tab, h->N, h->S32, h->ori32, h->F, h->x, h->svpart, h->tv[h->vcur],
+                                  h->rv[h->vcur], h->st));
+    h->launches += 2;
+  } else {
+    RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos32, h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
+                                     h->rv[h->vcur], h->st));
+    h->launches += 3;
+  }
   RF_CUDA_TRY(cudaEventRecord(h->ev[5], h->st));
   h->vlast = h->vcur;
   return RF_OK;
@@ -517,6 +585,7 @@ static int fetch_vec(rf_handle* h, const float* dev, double* out) {
 int rf_get_system(rf_handle* h, float* A, double* b) {
   if (!h) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("no assembled system"); return RF_E_STATE; }
+  if (A && !h->A) { set_last_error_str("no dense matrix in mixed-precision mode"); return RF_E_STATE; }
   if (A) {
     RF_CUDA_TRY(cudaMemcpy2DAsync(A, (size_t)h->R * sizeof(float), h->A, (size_t)h->lda * sizeof(float),
                                   (size_t)h->R * sizeof(float), (size_t)h->R, cudaMemcpyDeviceToHost, h->st));
@@ -546,6 +615,35 @@ int rf_get_config(rf_handle* h, rf_config* c) {
 }
 
 int rf_number_of_fibers(rf_handle* h) { return h ? h->N : -1; }
+
+int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
+  if (!h || !x || !y || which < 0 || which > 1) return RF_E_INPUT;
+  if (!h->assembled) { set_last_error_str("rf_operator_apply before rf_assemble"); return RF_E_STATE; }
+  if (which == 1 && !h->mixed) { set_last_error_str("no 16-bit operator in FP32 mode"); return RF_E_STATE; }
+  const int64_t R = h->R;
+  std::vector<double> hx(x, x + R);
+  std::vector<float> hxf(R), hy(R);
+  for (int64_t r = 0; r < R; ++r) hxf[r] = (float)hx[r];
+  // the Krylov basis and solution buffers serve as staging (the handle is idle)
+  float* dxf = h->V;
+  float* dy = h->V + ceil_div(R, 32) * 32;
+  RF_CUDA_TRY(cudaMemcpyAsync(dxf, hxf.data(), R * sizeof(float), cudaMemcpyHostToDevice, h->st));
+  if (!h->mixed) {
+    RF_TRY(launch_dense_gemv(h->gemv_plan, h->A, h->lda, R, dxf, h->ypart, nullptr, h->st));
+    RF_TRY(launch_reduce_rows(h->ypart, h->gemv_plan.splits, R, dy, h->st));
+  } else if (which == 1) {
+    const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+    RF_TRY(launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, dxf, h->zpart, dy, nullptr, h->st));
+  } else {
+    RF_CUDA_TRY(cudaMemcpyAsync(h->x64, hx.data(), R * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    RF_TRY(launch_struct_apply64(h->tab, h->N, h->S32, h->ori32, h->x64, h->zpart64, dy, h->st));
+  }
+  RF_CUDA_TRY(cudaMemcpyAsync(hy.data(), dy, R * sizeof(float), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  for (int64_t r = 0; r < R; ++r) y[r] = hy[r];
+  h->solved = false;
+  return RF_OK;
+}
 
 int rf_get_stream(rf_handle* h, void** stream) {
   if (!h || !stream) return RF_E_INPUT;

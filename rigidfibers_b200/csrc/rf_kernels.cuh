@@ -9,15 +9,38 @@
 
 namespace rf {
 
+// Structured storage tile: 16 x 16 fibers (a multiple of every assembly tile side).
+constexpr int kStoreTile = 16;
+
 bool mq_supported(int M, int Q);
 // out[r] = sum_p part[p*R + r], fixed order
 int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st);
 int assemble_tiles(int M, int Q, int N);
 
-// Numerical assembly into dense column-major A (leading dimension lda) and b.
-// bpart: assemble_tiles(M,Q,N) x R floats of scratch.
+// Numerical assembly.  ffpart: assemble_tiles(M,Q,N) x N x 3(M+1) floats of
+// scratch; F: N x 3(M+1) force terms sum_j T^{ij}[k][P0] F/2; b: R.
 int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                              int64_t lda, float* bpart, float* b, cudaStream_t st);
+                              int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
+// Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
+int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
+                               uint32_t* S16, bool bf16, float* ffpart, float* F, float* b, cudaStream_t st);
+int64_t struct_store_tiles(int N);
+int64_t struct_floats32(int M, int N);
+int64_t struct_words16(int M, int N);
+// y = A v on the structured operator (smode 0 FP32 / 1 FP16 / 2 BF16 storage, FP32 accumulation);
+// zpart: ceil(N/16) x R floats.
+int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
+                         const float4* ori, const float* x, float* zpart, float* y, const int* skip, cudaStream_t st);
+// r = b - A x with the FP32 blocks, x and accumulation in FP64; zpart64: ceil(N/16) x R doubles.
+int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
+                             double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st);
+// y = A x with the FP32 blocks, x and accumulation in FP64.
+int launch_struct_apply64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
+                          double* zpart64, float* y, cudaStream_t st);
+// velocities from the FP32 blocks; vpart: ceil(N/16) x N x 6 floats.
+int launch_struct_velocity(const Tables& tab, int N, const float* S32, const float4* ori, const float* F,
+                           const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
+int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t st);
 
 }  // namespace rf
 

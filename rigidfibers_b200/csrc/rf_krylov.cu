@@ -198,7 +198,8 @@ struct GmresArgs {
   const float* ypart;  // matvec result, nsplit partial rows
   int nsplit;
   const float* b;
-  float* x;
+  void* x;             // float or double (x_double)
+  int x_double;
   float* V;            // (m+1) x ldv
   int64_t ldv;
   int64_t R;
@@ -235,14 +236,17 @@ __global__ void k_gmres_init(GmresArgs a) {
   }
 }
 
-// r = b - A x (x_zero: r = b), beta = ||r||; convergence test on the true
-// residual; V[0] = r / beta, g = (beta, 0, ...).
-__global__ void k_gmres_residual(GmresArgs a, int x_zero) {
+// r = b - A x, beta = ||r||; convergence test on the true residual;
+// V[0] = r / beta, g = (beta, 0, ...).  mode 0: x = 0 (r = b); 1: r = b - sum
+// of the matvec partials of A x; 2: V[0] already holds r (written by a
+// residual operator, e.g. FP64-accumulated).
+__global__ void k_gmres_residual(GmresArgs a, int mode) {
   cg::grid_group grid = cg::this_grid();
   if (a.ctl->converged || a.ctl->nan) return;
   float* V0 = a.V;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
-    V0[r] = x_zero ? a.b[r] : a.b[r] - sum_splits(a.ypart, a.nsplit, a.R, r);
+  if (mode != 2)
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
+      V0[r] = mode == 0 ? a.b[r] : a.b[r] - sum_splits(a.ypart, a.nsplit, a.R, r);
   grid_partial_norm(V0, a.R, a.part, a.stride, 0);
   grid.sync();
   const double beta = sqrt(sum_parts(a.part, gridDim.x, a.stride, 0));
@@ -351,16 +355,23 @@ __global__ void k_gmres_update(GmresArgs a) {
   }
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
-    double s = (double)a.x[r];
+    double s = 0.0;
     for (int k = 0; k < jc; ++k) s += y[k] * (double)a.V[(int64_t)k * a.ldv + r];
-    a.x[r] = (float)s;
+    if (a.x_double) {
+      double* x = static_cast<double*>(a.x);
+      x[r] += s;
+    } else {
+      float* x = static_cast<float*>(a.x);
+      x[r] = (float)((double)x[r] + s);
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->restarts += 1;
 }
 
-__global__ void k_fill_zero(float* __restrict__ p, int64_t n) {
+template <typename T>
+__global__ void k_fill_zero(T* __restrict__ p, int64_t n) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-    p[r] = 0.f;
+    p[r] = (T)0;
 }
 
 static int coop_launch(const void* fn, int nblk, int threads, void** args, cudaStream_t st) {
@@ -376,6 +387,11 @@ int krylov_coop_blocks(int64_t R, int num_sms) {
 
 int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
                 GmresResult* res) {
+  return gmres_solve_ex(s, matvec, ResidualFn(), b, x, false, st, res);
+}
+
+int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b, void* x,
+                   bool x_double, cudaStream_t st, GmresResult* res) {
   const int m = s.m;
   if (m < 1 || m > kMaxRestart) {
     set_last_error_str("gmres: restart length out of range");
@@ -386,6 +402,7 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
   a.nsplit = s.nsplit;
   a.b = b;
   a.x = x;
+  a.x_double = x_double ? 1 : 0;
   a.V = s.V;
   a.ldv = s.ldv;
   a.R = s.R;
@@ -402,7 +419,10 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
   init.tol = s.tol;
   init.maxit = s.maxit;
   RF_CUDA_TRY(cudaMemcpyAsync(s.ctl, &init, sizeof(GmresCtl), cudaMemcpyHostToDevice, st));
-  k_fill_zero<<<std::min<int64_t>(ceil_div(s.R, 256), 1024), 256, 0, st>>>(x, s.R);
+  if (x_double)
+    k_fill_zero<double><<<std::min<int64_t>(ceil_div(s.R, 256), 1024), 256, 0, st>>>(static_cast<double*>(x), s.R);
+  else
+    k_fill_zero<float><<<std::min<int64_t>(ceil_div(s.R, 256), 1024), 256, 0, st>>>(static_cast<float*>(x), s.R);
   RF_LAUNCH_CHECK();
   {
     void* args[] = {&a};
@@ -415,12 +435,20 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
   int cycles_run = 0;
   for (int cycle = 0;; ++cycle) {
     ++cycles_run;
+    int mode = x_zero ? 0 : 1;
     if (!x_zero) {
-      int rc = matvec(x, &s.ctl->converged, st);
+      int rc;
+      if (residual) {
+        rc = residual(x, s.V, &s.ctl->converged, st);
+        mode = 2;
+      } else {
+        rc = matvec(static_cast<const float*>(x), &s.ctl->converged, st);
+      }
       if (rc) return rc;
+      ++res->launches;
     }
     {
-      void* args[] = {&a, &x_zero};
+      void* args[] = {&a, &mode};
       int rc = coop_launch((const void*)k_gmres_residual, nblk, 256, args, st);
       if (rc) return rc;
     }

@@ -27,6 +27,9 @@ struct GmresCtl {
 // ypart = partial rows of A x (nsplit of them); `skip` is a device flag the
 // matvec kernels read first and return on when set.
 using MatvecFn = std::function<int(const float* x, const int* skip, cudaStream_t st)>;
+// r = b - A x written to `r` (FP32), for refinement with a more accurate
+// operator / accumulation than the matvec's.
+using ResidualFn = std::function<int(const void* x, float* r, const int* skip, cudaStream_t st)>;
 
 struct GmresSetup {
   int64_t R;
@@ -58,6 +61,11 @@ struct GmresResult {
 int krylov_coop_blocks(int64_t R, int num_sms);
 int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
                 GmresResult* res);
+// GMRES with iterative refinement at every restart: the Arnoldi steps use
+// `matvec` (e.g. a 16-bit operator), each restart recomputes the true residual
+// with `residual` and accumulates the correction into x (FP64 if x_double).
+int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b, void* x,
+                   bool x_double, cudaStream_t st, GmresResult* res);
 
 struct DenseGemvPlan {
   int row_blocks;

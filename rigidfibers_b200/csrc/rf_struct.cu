@@ -1,0 +1,412 @@
+// Structured operator A = I + C T: matvec, residual and velocities from the
+// pair blocks that the assembly stores once per unordered fiber pair.
+//
+// The reference builds the dense R x R matrix (src/simulation.cu:331-399,
+// fortran/assemble_matrix.incl) whose block (i,j) is C_i T^{ij} with C_i the
+// per-force-index projector (D1 t t^T, or gamma_k (I - E_k t t^T)) and
+// T^{ij}_{k,kj} a symmetric 3x3 block with T^{ji} = (T^{ij})^T.  A matvec is
+//   y_{i,k} = x_{i,k} + C_i(k) z_{i,k},   z_{i,k} = sum_{j != i} sum_kj T^{ij}_{k,kj} x_{j,kj}
+// and only the M^2 blocks of each unordered pair (150 values at M = 5) have to
+// be read: 2.4 GB in FP16 at N = 4000 against 14.4 GB for dense FP32.
+//
+// Storage (written by k_assemble_numerical in structured mode): 16x16 fiber
+// storage tiles over the upper triangle; inside, (16/TI)^2 assembly
+// sub-tiles of TI x TI pairs, each as [j][value][i], so a warp reads whole
+// 32-byte sectors.  One CTA = one storage tile = 256 pairs = 256 threads.
+// z is reduced deterministically: per-tile partial rows, fixed-order sums.
+// The velocities reuse the FP32 blocks with P_0 / P_1 on the receiving side
+// (fortran/update_velocities.incl:64-86: TFA0 and TFA1 are exactly those).
+#include <type_traits>
+
+#include "rf_common.cuh"
+#include "rf_kernels.cuh"
+
+namespace rf {
+
+__device__ __forceinline__ void tile_pair16(int64_t L, int& I, int& J) {
+  int64_t j = (int64_t)((sqrt(8.0 * (double)L + 1.0) - 1.0) * 0.5);
+  while ((j + 1) * (j + 2) / 2 <= L) ++j;
+  while (j * (j + 1) / 2 > L) --j;
+  J = (int)j;
+  I = (int)(L - j * (j + 1) / 2);
+}
+
+template <typename T>
+__device__ __forceinline__ float2 unpack16(uint32_t w);
+template <>
+__device__ __forceinline__ float2 unpack16<__half>(uint32_t w) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+template <>
+__device__ __forceinline__ float2 unpack16<__nv_bfloat16>(uint32_t w) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w));
+}
+
+// sym(T6) * v accumulated into acc
+template <typename A>
+__device__ __forceinline__ void sym_mv_acc(const A (&t)[6], const A* v, A* acc) {
+  acc[0] += t[0] * v[0] + t[3] * v[1] + t[4] * v[2];
+  acc[1] += t[3] * v[0] + t[1] * v[1] + t[5] * v[2];
+  acc[2] += t[4] * v[0] + t[5] * v[1] + t[2] * v[2];
+}
+
+// Thread -> pair of a storage tile.
+template <int TI>
+struct TileMap {
+  static constexpr int SUB = kStoreTile / TI;
+  int sub, jl, tl, a, b;
+  __device__ TileMap(int t) {
+    sub = t / (TI * TI);
+    const int rem = t % (TI * TI);
+    jl = rem / TI;
+    tl = rem % TI;
+    a = sub / SUB;
+    b = sub % SUB;
+  }
+  __device__ int i16() const { return a * TI + tl; }
+  __device__ int j16() const { return b * TI + jl; }
+};
+
+// z partials.  SMODE: 0 = FP32 storage (inner blocks of S32), 1 = FP16, 2 = BF16.
+// XT: type of x; ACC: accumulation type.
+template <int M, int ACCB>
+struct ZSmem {
+  static constexpr int M3 = 3 * M;
+  static constexpr size_t kX = (size_t)2 * kStoreTile * M3 * ACCB;                 // x of both tiles
+  static constexpr size_t kZ = (size_t)kStoreTile * kStoreTile * (M3 + 1) * ACCB;   // one side's pair partials
+  static constexpr size_t kBytes = kX + kZ;
+};
+
+template <int M, int TI, int SMODE, typename XT, typename ACC>
+__global__ void __launch_bounds__(256)
+k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S16, const XT* __restrict__ x,
+           ACC* __restrict__ zpart, const int* __restrict__ skip) {
+  if (skip != nullptr && *skip) return;
+  constexpr int K1 = M + 1, M3 = 3 * M;
+  constexpr int NQ32 = K1 * K1 * 6, NQ16 = M * M * 3;
+  constexpr int SUB = kStoreTile / TI;
+  extern __shared__ __align__(16) unsigned char zsm[];
+  ACC (*sx)[kStoreTile][M3] = reinterpret_cast<ACC (*)[kStoreTile][M3]>(zsm);
+  ACC (*sz)[kStoreTile][M3 + 1] = reinterpret_cast<ACC (*)[kStoreTile][M3 + 1]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
+  int I16, J16;
+  tile_pair16(blockIdx.x, I16, J16);
+  const bool diag = I16 == J16;
+  const int t = threadIdx.x;
+  const int64_t R = (int64_t)M3 * N;
+  for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
+    const int side = k / (kStoreTile * M3), rem = k % (kStoreTile * M3);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
+    sx[side][rem / M3][rem % M3] = f < N ? (ACC)x[(int64_t)f * M3 + rem % M3] : (ACC)0;
+  }
+  __syncthreads();
+  const TileMap<TI> mp(t);
+  const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
+  ACC zi[M3], zj[M3];
+#pragma unroll
+  for (int k = 0; k < M3; ++k) zi[k] = zj[k] = (ACC)0;
+  if (i < j && j < N) {
+    const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
+    const ACC* xi = sx[0][mp.i16()];
+    const ACC* xj = sx[1][mp.j16()];
+    if constexpr (SMODE == 0) {
+      const float* p = S32 + rec * (int64_t)(NQ32 * TI) + mp.tl;
+#pragma unroll
+      for (int kI = 0; kI < M; ++kI)
+#pragma unroll
+        for (int kJ = 0; kJ < M; ++kJ) {
+          const int q0 = ((kI + 1) * K1 + (kJ + 1)) * 6;
+          ACC tv[6];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) tv[c] = (ACC)__ldcs(p + (q0 + c) * TI);
+          sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * kI);
+          sym_mv_acc(tv, xi + 3 * kI, zj + 3 * kJ);
+        }
+    } else {
+      using H16 = typename std::conditional<SMODE == 1, __half, __nv_bfloat16>::type;
+      const uint32_t* p = S16 + rec * (int64_t)(NQ16 * TI) + mp.tl;
+      uint32_t w[NQ16];
+#pragma unroll
+      for (int q2 = 0; q2 < NQ16; ++q2) w[q2] = __ldcs(p + q2 * TI);
+#pragma unroll
+      for (int blk = 0; blk < M * M; ++blk) {
+        const int kI = blk / M, kJ = blk % M;
+        ACC tv[6];
+#pragma unroll
+        for (int h = 0; h < 3; ++h) {
+          const float2 f = unpack16<H16>(w[blk * 3 + h]);
+          tv[2 * h] = (ACC)f.x;
+          tv[2 * h + 1] = (ACC)f.y;
+        }
+        sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * kI);
+        sym_mv_acc(tv, xi + 3 * kI, zj + 3 * kJ);
+      }
+    }
+  }
+  // fixed-order sums over partner fibers, one side at a time through shared memory
+  constexpr int NT = kStoreTile * M3;              // (row fiber, value) reductions
+  constexpr int NR = (NT + 255) / 256;             // per thread
+  ACC si[NR], sj[NR];
+#pragma unroll
+  for (int k = 0; k < M3; ++k) sz[mp.i16()][mp.j16()][k] = zi[k];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NR; ++u) {
+    const int task = t + 256 * u;
+    si[u] = (ACC)0;
+    if (task < NT)
+      for (int p = 0; p < kStoreTile; ++p) si[u] += sz[task / M3][p][task % M3];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < M3; ++k) sz[mp.j16()][mp.i16()][k] = zj[k];
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < NR; ++u) {
+    const int task = t + 256 * u;
+    if (task >= NT) continue;
+    const int rf = task / M3, rv = task % M3;
+    sj[u] = (ACC)0;
+    for (int p = 0; p < kStoreTile; ++p) sj[u] += sz[rf][p][rv];
+    const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
+    if (diag) {
+      if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si[u] + sj[u];
+    } else {
+      if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si[u];
+      if (fj < N) zpart[(int64_t)I16 * R + (int64_t)fj * M3 + rv] = sj[u];
+    }
+  }
+}
+
+// y = x + C z (z = sum of partials), or r = b - (x + C z).  One thread per (fiber, k).
+template <typename XT, typename ACC, bool RESIDUAL>
+__global__ void k_struct_finalize(const Tables tab, int N, const float4* __restrict__ ori, const XT* __restrict__ x,
+                                  const ACC* __restrict__ zpart, int nparts, const float* __restrict__ b,
+                                  float* __restrict__ out, const int* __restrict__ skip) {
+  if (skip != nullptr && *skip) return;
+  const int M = tab.M;
+  const int64_t R = (int64_t)3 * M * N;
+  const int64_t n = (int64_t)N * M;
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(u / M), k = (int)(u % M);
+    const int64_t r0 = (int64_t)i * 3 * M + 3 * k;
+    ACC z[3] = {0, 0, 0};
+    for (int p = 0; p < nparts; ++p) {
+      const ACC* s = zpart + (int64_t)p * R + r0;
+      z[0] += s[0]; z[1] += s[1]; z[2] += s[2];
+    }
+    const float4 t = ori[i];
+    const ACC t3[3] = {(ACC)t.x, (ACC)t.y, (ACC)t.z};
+    const ACC tz = t3[0] * z[0] + t3[1] * z[1] + t3[2] * z[2];
+    const ACC coef = (ACC)tab.gamma[k], E = (ACC)tab.eigen[k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const ACC cz = k == 0 ? coef * t3[a] * tz : coef * (z[a] - E * t3[a] * tz);
+      const ACC y = (ACC)x[r0 + a] + cz;
+      out[r0 + a] = RESIDUAL ? (float)((ACC)b[r0 + a] - y) : (float)y;
+    }
+  }
+}
+
+// Velocity partials from the FP32 blocks:
+//   u_i += sum_kJ T^{ij}[P0][kJ+1] x_{j,kJ},  w_i += sum_kJ T^{ij}[P1][kJ+1] x_{j,kJ}
+//   u_j += sum_kI T^{ij}[kI+1][P0] x_{i,kI},  w_j += sum_kI T^{ij}[kI+1][P1] x_{i,kI}
+template <int M, int TI>
+__global__ void __launch_bounds__(256)
+k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict__ x, float* __restrict__ vpart) {
+  constexpr int K1 = M + 1, M3 = 3 * M;
+  constexpr int NQ32 = K1 * K1 * 6;
+  constexpr int SUB = kStoreTile / TI;
+  __shared__ float sx[2][kStoreTile][M3];
+  __shared__ float sz[2][kStoreTile][kStoreTile][7];
+  int I16, J16;
+  tile_pair16(blockIdx.x, I16, J16);
+  const bool diag = I16 == J16;
+  const int t = threadIdx.x;
+  for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
+    const int side = k / (kStoreTile * M3), rem = k % (kStoreTile * M3);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
+    sx[side][rem / M3][rem % M3] = f < N ? x[(int64_t)f * M3 + rem % M3] : 0.f;
+  }
+  __syncthreads();
+  const TileMap<TI> mp(t);
+  const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
+  float vi[6] = {0, 0, 0, 0, 0, 0}, vj[6] = {0, 0, 0, 0, 0, 0};
+  if (i < j && j < N) {
+    const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
+    const float* p = S32 + rec * (int64_t)(NQ32 * TI) + mp.tl;
+    const float* xi = sx[0][mp.i16()];
+    const float* xj = sx[1][mp.j16()];
+#pragma unroll
+    for (int kk = 0; kk < M; ++kk) {
+      float tv[6];
+      // receiving side i: rows P0 and P1 against x_j
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int q0 = (r * K1 + (kk + 1)) * 6;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tv[c] = __ldcs(p + (q0 + c) * TI);
+        sym_mv_acc(tv, xj + 3 * kk, vi + 3 * r);
+      }
+      // receiving side j: columns P0 and P1 against x_i
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int q0 = ((kk + 1) * K1 + r) * 6;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tv[c] = __ldcs(p + (q0 + c) * TI);
+        sym_mv_acc(tv, xi + 3 * kk, vj + 3 * r);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    sz[0][mp.i16()][mp.j16()][k] = vi[k];
+    sz[1][mp.j16()][mp.i16()][k] = vj[k];
+  }
+  __syncthreads();
+  for (int k = t; k < 2 * kStoreTile * 6; k += blockDim.x) {
+    const int side = k / (kStoreTile * 6), rem = k % (kStoreTile * 6);
+    const int f = rem / 6, v = rem % 6;
+    float s = 0.f;
+    for (int p = 0; p < kStoreTile; ++p) s += sz[side][f][p][v];
+    if (diag) {
+      if (side == 1) continue;
+      for (int p = 0; p < kStoreTile; ++p) s += sz[1][f][p][v];
+    }
+    const int fib = (side == 0 ? I16 : J16) * kStoreTile + f;
+    if (fib < N) vpart[((int64_t)(side == 0 ? J16 : I16) * N + fib) * 6 + v] = s;
+  }
+}
+
+// U_i = (0.5/d) [ (d+2)F + (d-2)(t.F)t + F_i[P0] + sum u ],
+// W_i = (1.5/d) (I - t t^T) [ F_i[P1] + sum w ]
+__global__ void k_struct_velocity_finalize(const Tables tab, int N, const float4* __restrict__ ori,
+                                           const float* __restrict__ F, const float* __restrict__ vpart, int nparts,
+                                           float4* __restrict__ tvel, float4* __restrict__ rvel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int FFn = 3 * (tab.M + 1);
+  const float4 t = ori[i];
+  const float d = tab.d;
+  const float Fz = 2.f * tab.fz_half;
+  const float tF = t.z * Fz;
+  const float* Fi = F + (int64_t)i * FFn;
+  float U[3] = {(d - 2.f) * tF * t.x + Fi[0], (d - 2.f) * tF * t.y + Fi[1], (d + 2.f) * Fz + (d - 2.f) * tF * t.z + Fi[2]};
+  float W[3] = {Fi[3], Fi[4], Fi[5]};
+  for (int p = 0; p < nparts; ++p) {
+    const float* v = vpart + ((int64_t)p * N + i) * 6;
+    U[0] += v[0]; U[1] += v[1]; U[2] += v[2];
+    W[0] += v[3]; W[1] += v[4]; W[2] += v[5];
+  }
+  const float tW = t.x * W[0] + t.y * W[1] + t.z * W[2];
+  const float su = 0.5f / d, sr = 1.5f / d;
+  tvel[i] = make_float4(U[0] * su, U[1] * su, U[2] * su, 0.f);
+  rvel[i] = make_float4((W[0] - t.x * tW) * sr, (W[1] - t.y * tW) * sr, (W[2] - t.z * tW) * sr, 0.f);
+}
+
+template <typename XT>
+__global__ void k_cast_to_float(const XT* __restrict__ in, float* __restrict__ out, int64_t n) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    out[r] = (float)in[r];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static unsigned fin_blocks(int64_t n) { return (unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 8); }
+
+template <int M, int TI, int SMODE, typename XT, typename ACC>
+static int launch_z_one(int N, const float* S32, const uint32_t* S16, const XT* x, ACC* zpart, const int* skip,
+                        cudaStream_t st) {
+  constexpr size_t smem = ZSmem<M, sizeof(ACC)>::kBytes;
+  static bool attr_set = false;
+  if (!attr_set) {
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr_set = true;
+  }
+  const unsigned grid = (unsigned)struct_store_tiles(N);
+  k_struct_z<M, TI, SMODE, XT, ACC><<<grid, 256, smem, st>>>(N, S32, S16, x, zpart, skip);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+template <int M, int TI>
+static int launch_z(int smode, bool fp64, int N, const float* S32, const uint32_t* S16, const void* x, void* zpart,
+                    const int* skip, cudaStream_t st) {
+  if (fp64) return launch_z_one<M, TI, 0, double, double>(N, S32, S16, (const double*)x, (double*)zpart, skip, st);
+  if (smode == 0) return launch_z_one<M, TI, 0, float, float>(N, S32, S16, (const float*)x, (float*)zpart, skip, st);
+  if (smode == 1) return launch_z_one<M, TI, 1, float, float>(N, S32, S16, (const float*)x, (float*)zpart, skip, st);
+  return launch_z_one<M, TI, 2, float, float>(N, S32, S16, (const float*)x, (float*)zpart, skip, st);
+}
+
+int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
+                         const float4* ori, const float* x, float* zpart, float* y, const int* skip, cudaStream_t st) {
+  int rc = RF_E_UNSUPPORTED;
+#define RF_Z_CASE(MM, QQ) \
+  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(smode, false, N, S32, S16, x, zpart, skip, st);
+  RF_FOR_EACH_MQ(RF_Z_CASE)
+#undef RF_Z_CASE
+  if (rc != RF_OK) return rc;
+  const int64_t n = (int64_t)N * tab.M;
+  k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(
+      tab, N, ori, x, zpart, (int)ceil_div(N, kStoreTile), nullptr, y, skip);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
+                             double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st) {
+  int rc = RF_E_UNSUPPORTED;
+#define RF_Z_CASE(MM, QQ) \
+  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(0, true, N, S32, nullptr, x, zpart64, skip, st);
+  RF_FOR_EACH_MQ(RF_Z_CASE)
+#undef RF_Z_CASE
+  if (rc != RF_OK) return rc;
+  const int64_t n = (int64_t)N * tab.M;
+  k_struct_finalize<double, double, true><<<fin_blocks(n), 256, 0, st>>>(
+      tab, N, ori, x, zpart64, (int)ceil_div(N, kStoreTile), b, r, skip);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int launch_struct_apply64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
+                          double* zpart64, float* y, cudaStream_t st) {
+  int rc = RF_E_UNSUPPORTED;
+#define RF_Z_CASE(MM, QQ) \
+  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(0, true, N, S32, nullptr, x, zpart64, nullptr, st);
+  RF_FOR_EACH_MQ(RF_Z_CASE)
+#undef RF_Z_CASE
+  if (rc != RF_OK) return rc;
+  const int64_t n = (int64_t)N * tab.M;
+  k_struct_finalize<double, double, false><<<fin_blocks(n), 256, 0, st>>>(
+      tab, N, ori, x, zpart64, (int)ceil_div(N, kStoreTile), nullptr, y, nullptr);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int launch_struct_velocity(const Tables& tab, int N, const float* S32, const float4* ori, const float* F,
+                           const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
+  const unsigned grid = (unsigned)struct_store_tiles(N);
+  bool done = false;
+#define RF_V_CASE(MM, QQ)                                                                 \
+  if (!done && tab.M == MM && tab.Q == QQ) {                                              \
+    k_struct_velocity<MM, 192 / QQ><<<grid, 256, 0, st>>>(N, S32, x, vpart);              \
+    done = true;                                                                          \
+  }
+  RF_FOR_EACH_MQ(RF_V_CASE)
+#undef RF_V_CASE
+  if (!done) return RF_E_UNSUPPORTED;
+  RF_LAUNCH_CHECK();
+  k_struct_velocity_finalize<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(tab, N, ori, F, vpart,
+                                                                          (int)ceil_div(N, kStoreTile), tvel, rvel);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t st) {
+  k_cast_to_float<double><<<fin_blocks(n), 256, 0, st>>>(in, out, n);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+}  // namespace rf

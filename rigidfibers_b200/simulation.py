@@ -165,6 +165,13 @@ class Simulation:
         C.check(self._lib.rf_get_solution(self._h, C.ptr(x)), "rf_get_solution")
         return x
 
+    def apply_operator(self, x, which=0):
+        """y = A x with the assembled operator (which=1: the 16-bit copy)."""
+        xx = C.f64(x, self.R)
+        y = np.zeros(self.R)
+        C.check(self._lib.rf_operator_apply(self._h, C.ptr(xx), C.ptr(y), int(which)), "rf_operator_apply")
+        return y
+
     def stats(self):
         s = C.rf_stats()
         C.check(self._lib.rf_last_stats(self._h, ctypes.byref(s)), "rf_last_stats")

@@ -1,0 +1,102 @@
+"""Mixed-precision path: structured operator (FP32 + 16-bit pair blocks),
+GMRES with FP64-residual refinement, velocities from the stored blocks.
+
+Bounds (written here, from the north star): forces, velocities and fiber
+state within 1e-4 relative of the FP64 oracle; the structured FP32 operator
+within twice the REAL*4 oracle's own error; the 16-bit operators within
+their storage precision (FP16 2e-3, BF16 1.5e-2 of the largest |y|).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rigidfibers_b200.generate import sphere_layout
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _sim(pos, ori, **kw):
+    from rigidfibers_b200 import Config, Simulation
+    return Simulation(Config(**kw), pos, ori)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 16, 17, 40, 100])
+@pytest.mark.parametrize("prec", ["mixed_fp16", "mixed_bf16"])
+def test_structured_operator_matches_dense(n, prec):
+    pos, ori = sphere_layout(n, radius=max(1.5, 0.8 * n ** (1 / 3)), seed=21 + n)
+    sim = _sim(pos, ori, precision=prec)
+    sim.assembleSystem()
+    p = O.Params()
+    A64, b64 = O.assemble(pos, ori, p, False, np.float64)
+    A32, b32 = O.assemble(pos, ori, p, False, np.float32)
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal(15 * n)
+    yref = A64 @ x
+    y32ref = A32.astype(np.float64) @ x
+    y = sim.apply_operator(x, 0)
+    assert _rel(y, yref) <= max(2e-6, 2 * _rel(y32ref, yref))
+    y16 = sim.apply_operator(x, 1)
+    assert _rel(y16, yref) <= (2e-3 if prec == "mixed_fp16" else 1.5e-2)
+    _, b = sim.system(with_matrix=False)
+    if n > 1:
+        assert _rel(b, b64) <= max(2e-6, 2 * _rel(b32, b64))
+
+
+def _run(sim, nsteps):
+    out = []
+    for t in range(nsteps):
+        sim.assembleSystem()
+        sim.solveSystem()
+        x = sim.solution()
+        sim.updateVelocities()
+        tv, rv = sim.velocities()
+        sim.updateFibers(t == 0)
+        pos, ori = sim.state()
+        out.append(dict(x=x, tvel=tv, rvel=rv, pos=pos, ori=ori, stats=sim.stats()))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["mixed_fp16", "mixed_bf16"])
+def test_mixed_steps_within_1e4_of_fp64(prec):
+    pos, ori = sphere_layout(200, radius=4.0, seed=7)
+    ref = O.run_steps(pos, ori, O.Params(), 3, solver="direct", dtype=np.float64)
+    res = _run(_sim(pos, ori, precision=prec, refinement_tolerance=1e-6), 3)
+    for t in range(3):
+        for k in ("x", "tvel", "rvel", "pos", "ori"):
+            assert _rel(res[t][k], ref[t][k]) <= 1e-4, (prec, t, k, _rel(res[t][k], ref[t][k]))
+        st = res[t]["stats"]
+        assert st["relative_residual"] <= 1e-6
+        assert st["refinement_steps"] >= 1
+
+
+def test_mixed_golden(golden):
+    """The reference's golden files (FP64 runs) through the mixed path."""
+    res = _run(_sim(golden["positions"], golden["orientations"], precision="mixed_fp16"), 2)
+    for t in range(2):
+        for f, k in [("XVec", "x"), ("TRANSVel", "tvel"), ("ROTVel", "rvel"), ("POS", "pos"), ("ORIENT", "ori")]:
+            ref = golden["numeric_direct/%d_%s" % (t, f)]
+            assert _rel(res[t][k], ref) <= 1e-4, (t, f)
+
+
+def test_mixed_and_fp32_agree():
+    pos, ori = sphere_layout(150, radius=3.5, seed=8)
+    a = _run(_sim(pos, ori, precision="mixed_fp16"), 2)
+    b = _run(_sim(pos, ori, gmres_tolerance=1e-7), 2)
+    for t in range(2):
+        for k in ("x", "tvel", "rvel", "pos"):
+            assert _rel(a[t][k], b[t][k]) <= 2e-5, (t, k)
+
+
+def test_mixed_requires_numerical_integration():
+    from rigidfibers_b200 import RigidFibersError
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(4, radius=1.5, seed=1)
+    with pytest.raises(RigidFibersError) as e:
+        _sim(pos, ori, precision="mixed_fp16", integration="analytical")
+    assert e.value.status == C.RF_E_UNSUPPORTED
