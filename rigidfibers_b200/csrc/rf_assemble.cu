@@ -58,7 +58,7 @@ struct AsmShape {
   static constexpr int GS = U + 1;
   static constexpr size_t kGBytes = sizeof(float) * NC * GS;
   static constexpr size_t kTBytes = sizeof(float) * TI * K1 * K1 * 6;
-  static constexpr size_t kSmem = kGBytes + kTBytes;
+  static constexpr size_t kSmem = kGBytes + 2 * kTBytes;   // T double-buffered across j
   // structured storage
   static constexpr int SUB = kStoreTile / TI;      // assembly tiles per storage-tile side
   static constexpr int NQ32 = K1 * K1 * 6;         // FP32 values per pair
@@ -91,9 +91,10 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
   extern __shared__ __align__(16) float smem_dyn[];
   float (*sG)[S::GS] = reinterpret_cast<float (*)[S::GS]>(smem_dyn);                          // [NC][GS]
-  float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(smem_dyn + NC * S::GS);     // [TI][K1][K1][6]
+  float* const sTbase = smem_dyn + NC * S::GS;                                               // 2 x [TI][K1][K1][6]
   __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
   __shared__ float sfJ[TI][FF];
+  __shared__ short sMap16[S::NQ16 * 2];   // 16-bit value q' -> offset of its T entry within a pair
 
   int I, J;
   tile_pair(blockIdx.x, I, J);
@@ -115,6 +116,12 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
   }
   for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
+  if constexpr (MODE != kAsmDense) {
+    for (int q = tid; q < S::NQ16 * 2; q += blockDim.x) {
+      const int c = q % 6, blk = q / 6;
+      sMap16[q] = (short)(((blk / M + 1) * K1 + (blk % M + 1)) * 6 + c);
+    }
+  }
 
   // own unit
   const int il = tid / Q, qi = tid % Q;
@@ -136,6 +143,10 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
 
   const int jcount = min(TI, N - j0);
   for (int jl = 0; jl < jcount; ++jl) {
+    // T is double-buffered: phase 2 of step jl+1 may run while phase 3 of
+    // step jl still reads, so one barrier per step suffices after phase 2
+    float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(sTbase + (jl & 1) * (TI * K1 * K1 * 6));
+    const float* sTflat = sTbase + (jl & 1) * (TI * K1 * K1 * 6);
     const bool pair_ok = unit_ok && (!diag || il < jl);
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj], mirror-folded over qj
     float g[6][K1];
@@ -265,10 +276,9 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
       const int64_t rec = (L16 * S::SUB * S::SUB + sub) * TI + jl;
       float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
       for (int v = tid; v < S::NQ32 * TI; v += blockDim.x) {
-        const int tl = v % TI, q = v / TI;
-        const int c = q % 6, kk = q / 6;
+        const int tl = v % TI, q = v / TI;   // q is the flat (k, kj, c) index of the pair's T
         const bool ok = (i0 + tl < N) && (!diag || tl < jl);
-        d32[v] = ok ? sT[tl][kk / K1][kk % K1][c] : 0.f;
+        d32[v] = ok ? sTflat[tl * S::NQ32 + q] : 0.f;
       }
       uint32_t* d16 = out.S16 + rec * (int64_t)(S::NQ16 * TI);
       for (int v = tid; v < S::NQ16 * TI; v += blockDim.x) {
@@ -276,11 +286,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
         const bool ok = (i0 + tl < N) && (!diag || tl < jl);
         float f[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int q = 2 * q2 + h;
-          const int c = q % 6, blk = q / 6;
-          f[h] = ok ? sT[tl][blk / M + 1][blk % M + 1][c] : 0.f;
-        }
+        for (int h = 0; h < 2; ++h) f[h] = ok ? sTflat[tl * S::NQ32 + sMap16[2 * q2 + h]] : 0.f;
         uint32_t word;
         if constexpr (MODE == kAsmStructF16) {
           __half2 hv = __floats2half2_rn(f[0], f[1]);
@@ -316,8 +322,8 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
 #pragma unroll
       for (int a = 0; a < 3; ++a) sfJ[jl][3 * kj + a] += s[a];
     }
-    __syncthreads();
   }
+  __syncthreads();
 
   // ---- partial force terms: ffpart[X][fiber of Y][k][3] written exactly once
   float* ffpart = out.ffpart;

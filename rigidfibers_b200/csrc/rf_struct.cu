@@ -69,110 +69,164 @@ struct TileMap {
 
 // z partials.  SMODE: 0 = FP32 storage (inner blocks of S32), 1 = FP16, 2 = BF16.
 // XT: type of x; ACC: accumulation type.
+// Shared memory: x of both tiles, then per-warp partial sums of z for the 16
+// row fibers of each side (zero-filled; warps that do not touch a fiber leave
+// zeros), summed in a fixed order at the end.
+constexpr int kZWarps = 8;   // 256 threads
+
 template <int M, int ACCB>
 struct ZSmem {
   static constexpr int M3 = 3 * M;
-  static constexpr size_t kX = (size_t)2 * kStoreTile * M3 * ACCB;                 // x of both tiles
-  static constexpr size_t kZ = (size_t)kStoreTile * kStoreTile * (M3 + 1) * ACCB;   // one side's pair partials
-  static constexpr size_t kBytes = kX + kZ;
+  static constexpr size_t kX = (size_t)2 * kStoreTile * M3 * ACCB;
+  static constexpr size_t kW = (size_t)kStoreTile * kZWarps * M3 * ACCB;   // one side
+  static constexpr size_t kBytes = kX + 2 * kW;
 };
 
-template <int M, int TI, int SMODE, typename XT, typename ACC>
-__global__ void __launch_bounds__(256)
+// The words of block row kI of one pair (M blocks of 6 values).
+template <int M, int TI, int SMODE>
+struct RowLoader {
+  static constexpr int K1 = M + 1;
+  static constexpr int NW = SMODE == 0 ? 6 * M : 3 * M;   // 4-byte words per row
+  __device__ static void load(uint32_t (&w)[NW], const void* base, int kI) {
+    if constexpr (SMODE == 0) {
+      const float* p = static_cast<const float*>(base);
+#pragma unroll
+      for (int kJ = 0; kJ < M; ++kJ)
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+          w[kJ * 6 + c] = __float_as_uint(__ldcs(p + (((kI + 1) * K1 + (kJ + 1)) * 6 + c) * TI));
+    } else {
+      const uint32_t* p = static_cast<const uint32_t*>(base);
+#pragma unroll
+      for (int q = 0; q < 3 * M; ++q) w[q] = __ldcs(p + (kI * 3 * M + q) * TI);
+    }
+  }
+  template <typename ACC>
+  __device__ static void values(const uint32_t (&w)[NW], int kJ, ACC (&tv)[6]) {
+    if constexpr (SMODE == 0) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) tv[c] = (ACC)__uint_as_float(w[kJ * 6 + c]);
+    } else {
+      using H16 = typename std::conditional<SMODE == 1, __half, __nv_bfloat16>::type;
+#pragma unroll
+      for (int h = 0; h < 3; ++h) {
+        const float2 f = unpack16<H16>(w[kJ * 3 + h]);
+        tv[2 * h] = (ACC)f.x;
+        tv[2 * h + 1] = (ACC)f.y;
+      }
+    }
+  }
+};
+
+template <typename ACC>
+__device__ __forceinline__ ACC shfl_xor(ACC v, int m) {
+  return __shfl_xor_sync(0xffffffffu, v, m);
+}
+
+template <int M, int TI, int SMODE, typename XT, typename ACC, bool PREFETCH>
+__global__ void __launch_bounds__(256, SMODE == 0 ? 2 : 3)
 k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S16, const XT* __restrict__ x,
            ACC* __restrict__ zpart, const int* __restrict__ skip) {
   if (skip != nullptr && *skip) return;
   constexpr int K1 = M + 1, M3 = 3 * M;
   constexpr int NQ32 = K1 * K1 * 6, NQ16 = M * M * 3;
   constexpr int SUB = kStoreTile / TI;
+  constexpr int LTI = TI == 4 ? 2 : (TI == 8 ? 3 : 4);   // log2(TI)
+  using RL = RowLoader<M, TI, SMODE>;
   extern __shared__ __align__(16) unsigned char zsm[];
   ACC (*sx)[kStoreTile][M3] = reinterpret_cast<ACC (*)[kStoreTile][M3]>(zsm);
-  ACC (*sz)[kStoreTile][M3 + 1] = reinterpret_cast<ACC (*)[kStoreTile][M3 + 1]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
+  ACC (*swi)[kZWarps][M3] = reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
+  ACC (*swj)[kZWarps][M3] =
+      reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX + ZSmem<M, sizeof(ACC)>::kW);
   int I16, J16;
   tile_pair16(blockIdx.x, I16, J16);
   const bool diag = I16 == J16;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int64_t R = (int64_t)M3 * N;
+  const TileMap<TI> mp(t);
+  const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
+  const bool active = i < j && j < N;
+  const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
+  const void* base = SMODE == 0 ? (const void*)(S32 + rec * (int64_t)(NQ32 * TI) + mp.tl)
+                                : (const void*)(S16 + rec * (int64_t)(NQ16 * TI) + mp.tl);
+  // first block row in flight before the x prologue
+  uint32_t wcur[RL::NW];
+  if (active) RL::load(wcur, base, 0);
   for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
     const int side = k / (kStoreTile * M3), rem = k % (kStoreTile * M3);
     const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
     sx[side][rem / M3][rem % M3] = f < N ? (ACC)x[(int64_t)f * M3 + rem % M3] : (ACC)0;
   }
+  for (int k = t; k < 2 * kStoreTile * kZWarps * M3; k += blockDim.x) (&swi[0][0][0])[k] = (ACC)0;
   __syncthreads();
-  const TileMap<TI> mp(t);
-  const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
   ACC zi[M3], zj[M3];
 #pragma unroll
   for (int k = 0; k < M3; ++k) zi[k] = zj[k] = (ACC)0;
-  if (i < j && j < N) {
-    const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
+  if (active) {
     const ACC* xi = sx[0][mp.i16()];
     const ACC* xj = sx[1][mp.j16()];
-    if constexpr (SMODE == 0) {
-      const float* p = S32 + rec * (int64_t)(NQ32 * TI) + mp.tl;
+#pragma unroll 1
+    for (int kI = 0; kI < M; ++kI) {
+      uint32_t wnext[RL::NW];
+      if (PREFETCH && kI + 1 < M) RL::load(wnext, base, kI + 1);
+      ACC ziv[3] = {(ACC)0, (ACC)0, (ACC)0};
+      ACC xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
 #pragma unroll
-      for (int kI = 0; kI < M; ++kI)
-#pragma unroll
-        for (int kJ = 0; kJ < M; ++kJ) {
-          const int q0 = ((kI + 1) * K1 + (kJ + 1)) * 6;
-          ACC tv[6];
-#pragma unroll
-          for (int c = 0; c < 6; ++c) tv[c] = (ACC)__ldcs(p + (q0 + c) * TI);
-          sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * kI);
-          sym_mv_acc(tv, xi + 3 * kI, zj + 3 * kJ);
-        }
-    } else {
-      using H16 = typename std::conditional<SMODE == 1, __half, __nv_bfloat16>::type;
-      const uint32_t* p = S16 + rec * (int64_t)(NQ16 * TI) + mp.tl;
-      uint32_t w[NQ16];
-#pragma unroll
-      for (int q2 = 0; q2 < NQ16; ++q2) w[q2] = __ldcs(p + q2 * TI);
-#pragma unroll
-      for (int blk = 0; blk < M * M; ++blk) {
-        const int kI = blk / M, kJ = blk % M;
+      for (int kJ = 0; kJ < M; ++kJ) {
         ACC tv[6];
+        RL::values(wcur, kJ, tv);
+        sym_mv_acc(tv, xj + 3 * kJ, ziv);
+        sym_mv_acc(tv, xik, zj + 3 * kJ);
+      }
+      // register-indexed store of the row result (no local memory)
 #pragma unroll
-        for (int h = 0; h < 3; ++h) {
-          const float2 f = unpack16<H16>(w[blk * 3 + h]);
-          tv[2 * h] = (ACC)f.x;
-          tv[2 * h + 1] = (ACC)f.y;
+      for (int kk = 0; kk < M; ++kk)
+        if (kk == kI) { zi[3 * kk] = ziv[0]; zi[3 * kk + 1] = ziv[1]; zi[3 * kk + 2] = ziv[2]; }
+      if (kI + 1 < M) {
+        if (PREFETCH) {
+#pragma unroll
+          for (int q = 0; q < RL::NW; ++q) wcur[q] = wnext[q];
+        } else {
+          RL::load(wcur, base, kI + 1);
         }
-        sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * kI);
-        sym_mv_acc(tv, xi + 3 * kI, zj + 3 * kJ);
       }
     }
   }
-  // fixed-order sums over partner fibers, one side at a time through shared memory
-  constexpr int NT = kStoreTile * M3;              // (row fiber, value) reductions
-  constexpr int NR = (NT + 255) / 256;             // per thread
-  ACC si[NR], sj[NR];
+  // warp reductions: z_i over the partner lanes (lane bits >= log2 TI),
+  // z_j over the row lanes (lane bits < log2 TI)
 #pragma unroll
-  for (int k = 0; k < M3; ++k) sz[mp.i16()][mp.j16()][k] = zi[k];
-  __syncthreads();
+  for (int k = 0; k < M3; ++k) {
+    ACC a = zi[k], b = zj[k];
 #pragma unroll
-  for (int u = 0; u < NR; ++u) {
-    const int task = t + 256 * u;
-    si[u] = (ACC)0;
-    if (task < NT)
-      for (int p = 0; p < kStoreTile; ++p) si[u] += sz[task / M3][p][task % M3];
+    for (int m = TI; m < 32; m <<= 1) a += shfl_xor(a, m);
+#pragma unroll
+    for (int m = 1; m < TI; m <<= 1) b += shfl_xor(b, m);
+    zi[k] = a;
+    zj[k] = b;
+  }
+  if ((lane >> LTI) == 0) {
+#pragma unroll
+    for (int k = 0; k < M3; ++k) swi[mp.i16()][warp][k] = zi[k];
+  }
+  if ((lane & (TI - 1)) == 0) {
+#pragma unroll
+    for (int k = 0; k < M3; ++k) swj[mp.j16()][warp][k] = zj[k];
   }
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < M3; ++k) sz[mp.j16()][mp.i16()][k] = zj[k];
-  __syncthreads();
-#pragma unroll
-  for (int u = 0; u < NR; ++u) {
-    const int task = t + 256 * u;
-    if (task >= NT) continue;
+  for (int task = t; task < kStoreTile * M3; task += blockDim.x) {
     const int rf = task / M3, rv = task % M3;
-    sj[u] = (ACC)0;
-    for (int p = 0; p < kStoreTile; ++p) sj[u] += sz[rf][p][rv];
+    ACC si = (ACC)0, sj = (ACC)0;
+#pragma unroll
+    for (int w = 0; w < kZWarps; ++w) {
+      si += swi[rf][w][rv];
+      sj += swj[rf][w][rv];
+    }
     const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
     if (diag) {
-      if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si[u] + sj[u];
+      if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si + sj;
     } else {
-      if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si[u];
-      if (fj < N) zpart[(int64_t)I16 * R + (int64_t)fj * M3 + rv] = sj[u];
+      if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si;
+      if (fj < N) zpart[(int64_t)I16 * R + (int64_t)fj * M3 + rv] = sj;
     }
   }
 }
@@ -317,15 +371,16 @@ static unsigned fin_blocks(int64_t n) { return (unsigned)std::min<int64_t>(ceil_
 template <int M, int TI, int SMODE, typename XT, typename ACC>
 static int launch_z_one(int N, const float* S32, const uint32_t* S16, const XT* x, ACC* zpart, const int* skip,
                         cudaStream_t st) {
+  constexpr bool kPrefetch = SMODE != 0;   // 16-bit rows are small enough to double-buffer
   constexpr size_t smem = ZSmem<M, sizeof(ACC)>::kBytes;
   static bool attr_set = false;
   if (!attr_set) {
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
   const unsigned grid = (unsigned)struct_store_tiles(N);
-  k_struct_z<M, TI, SMODE, XT, ACC><<<grid, 256, smem, st>>>(N, S32, S16, x, zpart, skip);
+  k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch><<<grid, 256, smem, st>>>(N, S32, S16, x, zpart, skip);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
