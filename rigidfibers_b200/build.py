@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
-         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+         "--expt-relaxed-constexpr", "-ftz=true", "-Xptxas", "-warn-spills"]
 
 
 def _newer(src_list, target):

@@ -57,7 +57,10 @@ struct AsmShape {
   // of bank conflicts), then the T blocks (6 floats each)
   static constexpr int GS = U + 1;
   static constexpr size_t kGBytes = sizeof(float) * NC * GS;
-  static constexpr size_t kTBytes = sizeof(float) * TI * K1 * K1 * 6;
+  // T pair stride padded so that 8 consecutive pairs start on distinct banks
+  // that are multiples of 4 (stride = 4 * odd mod 32)
+  static constexpr int TP = (K1 * K1 * 6 + 7) / 8 * 8 + 4;
+  static constexpr size_t kTBytes = sizeof(float) * TI * TP;
   static constexpr size_t kSmem = kGBytes + 2 * kTBytes;   // T double-buffered across j
   // structured storage
   static constexpr int SUB = kStoreTile / TI;      // assembly tiles per storage-tile side
@@ -91,7 +94,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
   extern __shared__ __align__(16) float smem_dyn[];
   float (*sG)[S::GS] = reinterpret_cast<float (*)[S::GS]>(smem_dyn);                          // [NC][GS]
-  float* const sTbase = smem_dyn + NC * S::GS;                                               // 2 x [TI][K1][K1][6]
+  float* const sTbase = smem_dyn + NC * S::GS;                                               // 2 x [TI][TP]
   __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
   __shared__ float sfJ[TI][FF];
   __shared__ short sMap16[S::NQ16 * 2];   // 16-bit value q' -> offset of its T entry within a pair
@@ -145,8 +148,8 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
   for (int jl = 0; jl < jcount; ++jl) {
     // T is double-buffered: phase 2 of step jl+1 may run while phase 3 of
     // step jl still reads, so one barrier per step suffices after phase 2
-    float (*sT)[K1][K1][6] = reinterpret_cast<float (*)[K1][K1][6]>(sTbase + (jl & 1) * (TI * K1 * K1 * 6));
-    const float* sTflat = sTbase + (jl & 1) * (TI * K1 * K1 * 6);
+    float* const sTflat = sTbase + (jl & 1) * (TI * S::TP);
+    auto sT = [&](int tl, int k, int kj) -> float* { return sTflat + tl * S::TP + (k * K1 + kj) * 6; };
     const bool pair_ok = unit_ok && (!diag || il < jl);
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj], mirror-folded over qj
     float g[6][K1];
@@ -210,7 +213,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
         for (int k = 0; k < K1; ++k) acc[k] = fmaf((k & 1) ? od : ev, tab.W[k][q], acc[k]);
       }
 #pragma unroll
-      for (int k = 0; k < K1; ++k) sT[tl][k][kj][c] = acc[k];
+      for (int k = 0; k < K1; ++k) sT(tl, k, kj)[c] = acc[k];
     }
     __syncthreads();
 
@@ -230,7 +233,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
             for (int a = 0; a < 3; ++a) dst[a + b * out.lda] = (kIp == kJp && a == b) ? 1.f : 0.f;
           continue;
         }
-        const float* T6 = sT[tl][kIp + 1][kJp + 1];
+        const float* T6 = sT(tl, kIp + 1, kJp + 1);
         const float4 ti = sTi[tl];
         const float t3[3] = {ti.x, ti.y, ti.z};
         float Qv[3];
@@ -254,7 +257,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
           const int ii = i0 + tl;
           if (ii >= N || (diag && tl >= jl)) continue;
           float* dst = out.A + (int64_t)(j * M3 + 3 * kJp) + (int64_t)(ii * M3 + 3 * kIp) * out.lda;
-          const float* T6 = sT[tl][kIp + 1][kJp + 1];
+          const float* T6 = sT(tl, kIp + 1, kJp + 1);
           float Qv[3];
 #pragma unroll
           for (int b = 0; b < 3; ++b)
@@ -278,7 +281,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
       for (int v = tid; v < S::NQ32 * TI; v += blockDim.x) {
         const int tl = v % TI, q = v / TI;   // q is the flat (k, kj, c) index of the pair's T
         const bool ok = (i0 + tl < N) && (!diag || tl < jl);
-        d32[v] = ok ? sTflat[tl * S::NQ32 + q] : 0.f;
+        d32[v] = ok ? sTflat[tl * S::TP + q] : 0.f;
       }
       uint32_t* d16 = out.S16 + rec * (int64_t)(S::NQ16 * TI);
       for (int v = tid; v < S::NQ16 * TI; v += blockDim.x) {
@@ -286,7 +289,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
         const bool ok = (i0 + tl < N) && (!diag || tl < jl);
         float f[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) f[h] = ok ? sTflat[tl * S::NQ32 + sMap16[2 * q2 + h]] : 0.f;
+        for (int h = 0; h < 2; ++h) f[h] = ok ? sTflat[tl * S::TP + sMap16[2 * q2 + h]] : 0.f;
         uint32_t word;
         if constexpr (MODE == kAsmStructF16) {
           __half2 hv = __floats2half2_rn(f[0], f[1]);
@@ -303,7 +306,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     if (tid < TI * K1) {
       const int tl = tid / K1, k = tid % K1;
       if (i0 + tl < N && (!diag || tl < jl)) {
-        const float* T6 = sT[tl][k][0];
+        const float* T6 = sT(tl, k, 0);
         facc[0] = fmaf(T6[4], fz, facc[0]);
         facc[1] = fmaf(T6[5], fz, facc[1]);
         facc[2] = fmaf(T6[2], fz, facc[2]);
@@ -314,7 +317,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
       float s[3] = {0.f, 0.f, 0.f};
       for (int tl = 0; tl < TI; ++tl) {
         if (i0 + tl >= N || (diag && tl >= jl)) continue;
-        const float* T6 = sT[tl][0][kj];
+        const float* T6 = sT(tl, 0, kj);
         s[0] = fmaf(T6[4], fz, s[0]);
         s[1] = fmaf(T6[5], fz, s[1]);
         s[2] = fmaf(T6[2], fz, s[2]);

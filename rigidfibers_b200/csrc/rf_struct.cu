@@ -77,7 +77,8 @@ constexpr int kZWarps = 8;   // 256 threads
 template <int M, int ACCB>
 struct ZSmem {
   static constexpr int M3 = 3 * M;
-  static constexpr size_t kX = (size_t)2 * kStoreTile * M3 * ACCB;
+  static constexpr int M3P = (M3 + 3) / 4 * 4;                              // x rows padded for 16-byte loads
+  static constexpr size_t kX = (size_t)2 * kStoreTile * M3P * ACCB;
   static constexpr size_t kW = (size_t)kStoreTile * kZWarps * M3 * ACCB;   // one side
   static constexpr size_t kBytes = kX + 2 * kW;
 };
@@ -123,18 +124,37 @@ __device__ __forceinline__ ACC shfl_xor(ACC v, int m) {
   return __shfl_xor_sync(0xffffffffu, v, m);
 }
 
+// x row of a fiber from shared memory (padded rows, 16-byte aligned)
+template <typename ACC, int M3P>
+__device__ __forceinline__ void load_xrow(const ACC* src, ACC (&dst)[M3P]) {
+  if constexpr (sizeof(ACC) == 4) {
+#pragma unroll
+    for (int k = 0; k < M3P / 4; ++k) {
+      const float4 v = reinterpret_cast<const float4*>(src)[k];
+      dst[4 * k] = v.x; dst[4 * k + 1] = v.y; dst[4 * k + 2] = v.z; dst[4 * k + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < M3P / 2; ++k) {
+      const double2 v = reinterpret_cast<const double2*>(src)[k];
+      dst[2 * k] = v.x; dst[2 * k + 1] = v.y;
+    }
+  }
+}
+
 template <int M, int TI, int SMODE, typename XT, typename ACC, bool PREFETCH>
 __global__ void __launch_bounds__(256, SMODE == 0 ? 2 : 3)
 k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S16, const XT* __restrict__ x,
            ACC* __restrict__ zpart, const int* __restrict__ skip) {
   if (skip != nullptr && *skip) return;
   constexpr int K1 = M + 1, M3 = 3 * M;
+  constexpr int M3P = ZSmem<M, sizeof(ACC)>::M3P;
   constexpr int NQ32 = K1 * K1 * 6, NQ16 = M * M * 3;
   constexpr int SUB = kStoreTile / TI;
   constexpr int LTI = TI == 4 ? 2 : (TI == 8 ? 3 : 4);   // log2(TI)
   using RL = RowLoader<M, TI, SMODE>;
   extern __shared__ __align__(16) unsigned char zsm[];
-  ACC (*sx)[kStoreTile][M3] = reinterpret_cast<ACC (*)[kStoreTile][M3]>(zsm);
+  ACC (*sx)[kStoreTile][M3P] = reinterpret_cast<ACC (*)[kStoreTile][M3P]>(zsm);
   ACC (*swi)[kZWarps][M3] = reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
   ACC (*swj)[kZWarps][M3] =
       reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX + ZSmem<M, sizeof(ACC)>::kW);
@@ -150,63 +170,66 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
   const void* base = SMODE == 0 ? (const void*)(S32 + rec * (int64_t)(NQ32 * TI) + mp.tl)
                                 : (const void*)(S16 + rec * (int64_t)(NQ16 * TI) + mp.tl);
   // first block row in flight before the x prologue
-  uint32_t wcur[RL::NW];
-  if (active) RL::load(wcur, base, 0);
-  for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
-    const int side = k / (kStoreTile * M3), rem = k % (kStoreTile * M3);
-    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
-    sx[side][rem / M3][rem % M3] = f < N ? (ACC)x[(int64_t)f * M3 + rem % M3] : (ACC)0;
+  uint32_t wa[RL::NW], wb[RL::NW];
+  if (active) RL::load(wa, base, 0);
+  for (int k = t; k < 2 * kStoreTile * M3P; k += blockDim.x) {
+    const int side = k / (kStoreTile * M3P), rem = k % (kStoreTile * M3P);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3P, v = rem % M3P;
+    sx[side][rem / M3P][v] = (f < N && v < M3) ? (ACC)x[(int64_t)f * M3 + v] : (ACC)0;
   }
   for (int k = t; k < 2 * kStoreTile * kZWarps * M3; k += blockDim.x) (&swi[0][0][0])[k] = (ACC)0;
   __syncthreads();
-  ACC zi[M3], zj[M3];
+  ACC zj[M3];
 #pragma unroll
-  for (int k = 0; k < M3; ++k) zi[k] = zj[k] = (ACC)0;
-  if (active) {
-    const ACC* xi = sx[0][mp.i16()];
-    const ACC* xj = sx[1][mp.j16()];
-#pragma unroll 1
-    for (int kI = 0; kI < M; ++kI) {
-      uint32_t wnext[RL::NW];
-      if (PREFETCH && kI + 1 < M) RL::load(wnext, base, kI + 1);
-      ACC ziv[3] = {(ACC)0, (ACC)0, (ACC)0};
-      ACC xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
+  for (int k = 0; k < M3; ++k) zj[k] = (ACC)0;
+  // x_j in registers for FP32 accumulation; read from shared memory for FP64
+  // (register budget)
+  ACC xjr[sizeof(ACC) == 4 ? M3P : 1];
+  if constexpr (sizeof(ACC) == 4) load_xrow<ACC, M3P>(sx[1][mp.j16()], xjr);
+  const ACC* xjs = sx[1][mp.j16()];
+  const ACC* xi = sx[0][mp.i16()];
+  const bool owner_i = (lane >> LTI) == 0;
+  // one block row: z_i[kI] (reduced over the partner lanes at once) and z_j
+  auto row = [&](const uint32_t (&w)[RL::NW], int kI) {
+    ACC ziv[3] = {(ACC)0, (ACC)0, (ACC)0};
+    const ACC xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
+    if (active) {
 #pragma unroll
       for (int kJ = 0; kJ < M; ++kJ) {
         ACC tv[6];
-        RL::values(wcur, kJ, tv);
-        sym_mv_acc(tv, xj + 3 * kJ, ziv);
+        RL::values(w, kJ, tv);
+        if constexpr (sizeof(ACC) == 4) sym_mv_acc(tv, xjr + 3 * kJ, ziv);
+        else sym_mv_acc(tv, xjs + 3 * kJ, ziv);
         sym_mv_acc(tv, xik, zj + 3 * kJ);
       }
-      // register-indexed store of the row result (no local memory)
+    }
 #pragma unroll
-      for (int kk = 0; kk < M; ++kk)
-        if (kk == kI) { zi[3 * kk] = ziv[0]; zi[3 * kk + 1] = ziv[1]; zi[3 * kk + 2] = ziv[2]; }
-      if (kI + 1 < M) {
-        if (PREFETCH) {
+    for (int a = 0; a < 3; ++a) {
+      ACC v = ziv[a];
 #pragma unroll
-          for (int q = 0; q < RL::NW; ++q) wcur[q] = wnext[q];
-        } else {
-          RL::load(wcur, base, kI + 1);
-        }
-      }
+      for (int m = TI; m < 32; m <<= 1) v += shfl_xor(v, m);
+      if (owner_i) swi[mp.i16()][warp][3 * kI + a] = v;
+    }
+  };
+  // ping-pong over the block rows: the next row's loads overlap this row's math
+#pragma unroll 1
+  for (int kI = 0; kI < M; kI += 2) {
+    if (PREFETCH && active && kI + 1 < M) RL::load(wb, base, kI + 1);
+    row(wa, kI);
+    if (kI + 1 < M) {
+      if (!PREFETCH && active) RL::load(wb, base, kI + 1);
+      if (PREFETCH && active && kI + 2 < M) RL::load(wa, base, kI + 2);
+      row(wb, kI + 1);
+      if (!PREFETCH && active && kI + 2 < M) RL::load(wa, base, kI + 2);
     }
   }
-  // warp reductions: z_i over the partner lanes (lane bits >= log2 TI),
   // z_j over the row lanes (lane bits < log2 TI)
 #pragma unroll
   for (int k = 0; k < M3; ++k) {
-    ACC a = zi[k], b = zj[k];
-#pragma unroll
-    for (int m = TI; m < 32; m <<= 1) a += shfl_xor(a, m);
+    ACC b = zj[k];
 #pragma unroll
     for (int m = 1; m < TI; m <<= 1) b += shfl_xor(b, m);
-    zi[k] = a;
     zj[k] = b;
-  }
-  if ((lane >> LTI) == 0) {
-#pragma unroll
-    for (int k = 0; k < M3; ++k) swi[mp.i16()][warp][k] = zi[k];
   }
   if ((lane & (TI - 1)) == 0) {
 #pragma unroll
