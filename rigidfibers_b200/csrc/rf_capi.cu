@@ -210,6 +210,10 @@ static int validate_config(const rf_config* c, int N) {
     set_last_error_str("mixed precision uses the symmetric pair blocks of numerical integration");
     return RF_E_UNSUPPORTED;
   }
+  if (c->precision != RF_PREC_FP32 && c->number_of_quadrature_intervals != 8) {
+    set_last_error_str("mixed precision is built for 8 quadrature intervals (24 points per fiber)");
+    return RF_E_UNSUPPORTED;
+  }
   if (c->precision != RF_PREC_FP32 && c->solver != RF_SOLVER_GMRES) {
     set_last_error_str("mixed precision refines inside GMRES");
     return RF_E_UNSUPPORTED;

@@ -44,10 +44,15 @@ __device__ __forceinline__ float2 unpack16<__nv_bfloat16>(uint32_t w) {
 
 // sym(T6) * v accumulated into acc
 template <typename A>
+__device__ __forceinline__ A fma_(A a, A b, A c) { return fma(a, b, c); }
+template <>
+__device__ __forceinline__ float fma_<float>(float a, float b, float c) { return fmaf(a, b, c); }
+
+template <typename A>
 __device__ __forceinline__ void sym_mv_acc(const A (&t)[6], const A* v, A* acc) {
-  acc[0] += t[0] * v[0] + t[3] * v[1] + t[4] * v[2];
-  acc[1] += t[3] * v[0] + t[1] * v[1] + t[5] * v[2];
-  acc[2] += t[4] * v[0] + t[5] * v[1] + t[2] * v[2];
+  acc[0] = fma_(t[4], v[2], fma_(t[3], v[1], fma_(t[0], v[0], acc[0])));
+  acc[1] = fma_(t[5], v[2], fma_(t[1], v[1], fma_(t[3], v[0], acc[1])));
+  acc[2] = fma_(t[2], v[2], fma_(t[5], v[1], fma_(t[4], v[0], acc[2])));
 }
 
 // Thread -> pair of a storage tile.
@@ -74,13 +79,20 @@ struct TileMap {
 // zeros), summed in a fixed order at the end.
 constexpr int kZWarps = 8;   // 256 threads
 
+// Shared memory of the z kernel (8x8 assembly sub-tiles, 8 warps):
+//  x rows of both tiles (padded: 20 floats / 17 doubles per fiber so the
+//  rows that one warp reads start on distinct banks), then the per-warp
+//  partial sums.  Warp w covers row fibers 8(w/4)..+8 on the i side (4
+//  warps per row) and 4 fibers 8((w/2)%2) + 4(w%2)..+4 on the j side (2 warps
+//  per row), so every slot is written once and nothing is zero-filled.
 template <int M, int ACCB>
 struct ZSmem {
   static constexpr int M3 = 3 * M;
-  static constexpr int M3P = (M3 + 3) / 4 * 4;                              // x rows padded for 16-byte loads
-  static constexpr size_t kX = (size_t)2 * kStoreTile * M3P * ACCB;
-  static constexpr size_t kW = (size_t)kStoreTile * kZWarps * M3 * ACCB;   // one side
-  static constexpr size_t kBytes = kX + 2 * kW;
+  static constexpr int XS = ACCB == 4 ? ((M3 + 3) / 4 * 4 + 4) : (M3 + 2) | 1;   // x row stride
+  static constexpr size_t kX = (size_t)2 * kStoreTile * XS * ACCB;
+  static constexpr size_t kWI = (size_t)kStoreTile * 4 * M3 * ACCB;
+  static constexpr size_t kWJ = (size_t)kStoreTile * 2 * M3 * ACCB;
+  static constexpr size_t kBytes = kX + kWI + kWJ;
 };
 
 // The words of block row kI of one pair (M blocks of 6 values).
@@ -146,18 +158,18 @@ template <int M, int TI, int SMODE, typename XT, typename ACC, bool PREFETCH>
 __global__ void __launch_bounds__(256, SMODE == 0 ? 2 : 3)
 k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S16, const XT* __restrict__ x,
            ACC* __restrict__ zpart, const int* __restrict__ skip) {
+  static_assert(TI == 8, "structured operator kernels are specialised to 8x8 assembly sub-tiles (Q = 24)");
   if (skip != nullptr && *skip) return;
   constexpr int K1 = M + 1, M3 = 3 * M;
-  constexpr int M3P = ZSmem<M, sizeof(ACC)>::M3P;
+  constexpr int XS = ZSmem<M, sizeof(ACC)>::XS;
   constexpr int NQ32 = K1 * K1 * 6, NQ16 = M * M * 3;
   constexpr int SUB = kStoreTile / TI;
-  constexpr int LTI = TI == 4 ? 2 : (TI == 8 ? 3 : 4);   // log2(TI)
   using RL = RowLoader<M, TI, SMODE>;
   extern __shared__ __align__(16) unsigned char zsm[];
-  ACC (*sx)[kStoreTile][M3P] = reinterpret_cast<ACC (*)[kStoreTile][M3P]>(zsm);
-  ACC (*swi)[kZWarps][M3] = reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
-  ACC (*swj)[kZWarps][M3] =
-      reinterpret_cast<ACC (*)[kZWarps][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX + ZSmem<M, sizeof(ACC)>::kW);
+  ACC (*sx)[kStoreTile][XS] = reinterpret_cast<ACC (*)[kStoreTile][XS]>(zsm);
+  ACC (*swi)[4][M3] = reinterpret_cast<ACC (*)[4][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX);
+  ACC (*swj)[2][M3] =
+      reinterpret_cast<ACC (*)[2][M3]>(zsm + ZSmem<M, sizeof(ACC)>::kX + ZSmem<M, sizeof(ACC)>::kWI);
   int I16, J16;
   tile_pair16(blockIdx.x, I16, J16);
   const bool diag = I16 == J16;
@@ -172,24 +184,23 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
   // first block row in flight before the x prologue
   uint32_t wa[RL::NW], wb[RL::NW];
   if (active) RL::load(wa, base, 0);
-  for (int k = t; k < 2 * kStoreTile * M3P; k += blockDim.x) {
-    const int side = k / (kStoreTile * M3P), rem = k % (kStoreTile * M3P);
-    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3P, v = rem % M3P;
-    sx[side][rem / M3P][v] = (f < N && v < M3) ? (ACC)x[(int64_t)f * M3 + v] : (ACC)0;
+  for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
+    const int side = k / (kStoreTile * M3), rem = k % (kStoreTile * M3);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3, v = rem % M3;
+    sx[side][rem / M3][v] = f < N ? (ACC)x[(int64_t)f * M3 + v] : (ACC)0;
   }
-  for (int k = t; k < 2 * kStoreTile * kZWarps * M3; k += blockDim.x) (&swi[0][0][0])[k] = (ACC)0;
   __syncthreads();
   ACC zj[M3];
 #pragma unroll
   for (int k = 0; k < M3; ++k) zj[k] = (ACC)0;
   // x_j in registers for FP32 accumulation; read from shared memory for FP64
-  // (register budget)
+  constexpr int M3P = (M3 + 3) / 4 * 4;
   ACC xjr[sizeof(ACC) == 4 ? M3P : 1];
   if constexpr (sizeof(ACC) == 4) load_xrow<ACC, M3P>(sx[1][mp.j16()], xjr);
   const ACC* xjs = sx[1][mp.j16()];
   const ACC* xi = sx[0][mp.i16()];
-  const bool owner_i = (lane >> LTI) == 0;
-  // one block row: z_i[kI] (reduced over the partner lanes at once) and z_j
+  const bool owner_i = lane < TI;           // lanes 0..7 hold the i-side warp sums
+  const int slot_i = warp & 3;
   auto row = [&](const uint32_t (&w)[RL::NW], int kI) {
     ACC ziv[3] = {(ACC)0, (ACC)0, (ACC)0};
     const ACC xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
@@ -206,9 +217,9 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       ACC v = ziv[a];
-#pragma unroll
-      for (int m = TI; m < 32; m <<= 1) v += shfl_xor(v, m);
-      if (owner_i) swi[mp.i16()][warp][3 * kI + a] = v;
+      v += shfl_xor(v, 8);
+      v += shfl_xor(v, 16);
+      if (owner_i) swi[mp.i16()][slot_i][3 * kI + a] = v;
     }
   };
   // ping-pong over the block rows: the next row's loads overlap this row's math
@@ -223,27 +234,24 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
       if (!PREFETCH && active && kI + 2 < M) RL::load(wa, base, kI + 2);
     }
   }
-  // z_j over the row lanes (lane bits < log2 TI)
+  // z_j over the row lanes (lane bits 0..2)
 #pragma unroll
   for (int k = 0; k < M3; ++k) {
     ACC b = zj[k];
-#pragma unroll
-    for (int m = 1; m < TI; m <<= 1) b += shfl_xor(b, m);
+    b += shfl_xor(b, 1);
+    b += shfl_xor(b, 2);
+    b += shfl_xor(b, 4);
     zj[k] = b;
   }
   if ((lane & (TI - 1)) == 0) {
 #pragma unroll
-    for (int k = 0; k < M3; ++k) swj[mp.j16()][warp][k] = zj[k];
+    for (int k = 0; k < M3; ++k) swj[mp.j16()][warp >> 2][k] = zj[k];
   }
   __syncthreads();
   for (int task = t; task < kStoreTile * M3; task += blockDim.x) {
     const int rf = task / M3, rv = task % M3;
-    ACC si = (ACC)0, sj = (ACC)0;
-#pragma unroll
-    for (int w = 0; w < kZWarps; ++w) {
-      si += swi[rf][w][rv];
-      sj += swj[rf][w][rv];
-    }
+    const ACC si = ((swi[rf][0][rv] + swi[rf][1][rv]) + swi[rf][2][rv]) + swi[rf][3][rv];
+    const ACC sj = swj[rf][0][rv] + swj[rf][1][rv];
     const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
     if (diag) {
       if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si + sj;
@@ -421,7 +429,7 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
 #define RF_Z_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(smode, false, N, S32, S16, x, zpart, skip, st);
+  if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(smode, false, N, S32, S16, x, zpart, skip, st);
   RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
   if (rc != RF_OK) return rc;
@@ -436,7 +444,7 @@ int launch_struct_residual64(const Tables& tab, int N, const float* S32, const f
                              double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
 #define RF_Z_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(0, true, N, S32, nullptr, x, zpart64, skip, st);
+  if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(0, true, N, S32, nullptr, x, zpart64, skip, st);
   RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
   if (rc != RF_OK) return rc;
@@ -451,7 +459,7 @@ int launch_struct_apply64(const Tables& tab, int N, const float* S32, const floa
                           double* zpart64, float* y, cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
 #define RF_Z_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) rc = launch_z<MM, 192 / QQ>(0, true, N, S32, nullptr, x, zpart64, nullptr, st);
+  if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(0, true, N, S32, nullptr, x, zpart64, nullptr, st);
   RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
   if (rc != RF_OK) return rc;
