@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--precision", default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--mixed-restart", type=int, default=0,
+                    help="Arnoldi steps between FP64 residual corrections in mixed precision (0: GMRES restart)")
     return ap.parse_args()
 
 
@@ -357,7 +359,7 @@ def run_ours(args, dist):
     N = args.fibers
     R = 15 * N
     precision = "mixed_fp16" if args.precision == "auto" else args.precision
-    cfg = Config(precision=precision)
+    cfg = Config(precision=precision, refinement_restart=args.mixed_restart)
     head = time_path(args, dist, cfg, pos, ori, clocks=Clocks(dist.local))
     ms_max = dist.max(head["ms"])
     total_fiber_steps = dist.sum(N * args.steps)

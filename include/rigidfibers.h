@@ -85,6 +85,8 @@ typedef struct rf_config {
   double refinement_tolerance;                  /* mixed precision: outer target on
                                                    ||b - A x|| / ||b|| */
   int refinement_max_iterations;
+  int refinement_restart;                       /* mixed precision: Arnoldi steps between
+                                                   FP64 residual corrections; 0 = gmres_restart */
 } rf_config;
 
 typedef struct rf_stats {

@@ -39,6 +39,7 @@ class rf_config(ctypes.Structure):
         ("velocity_integration", ctypes.c_int),
         ("refinement_tolerance", ctypes.c_double),
         ("refinement_max_iterations", ctypes.c_int),
+        ("refinement_restart", ctypes.c_int),
     ]
 
 

@@ -159,6 +159,7 @@ struct rf_handle {
   int launches = 0;
   int matvecs_done = 0;
   int refinements = 0;
+  int restart = 10;          // Krylov dimension per cycle
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -224,6 +225,9 @@ static int validate_config(const rf_config* c, int N) {
   if (c->integration == RF_ANALYTICAL) { set_last_error_str("analytical integration not built yet"); return RF_E_UNSUPPORTED; }
   if (c->solver != RF_SOLVER_GMRES) { set_last_error_str("solver not built yet"); return RF_E_UNSUPPORTED; }
   if (c->gmres_restart < 1 || c->gmres_restart > kMaxRestart) { set_last_error_str("gmres restart in [1, 64]"); return RF_E_INPUT; }
+  if (c->refinement_restart < 0 || c->refinement_restart > kMaxRestart) {
+    set_last_error_str("refinement_restart in [0, 64]"); return RF_E_INPUT;
+  }
   return RF_OK;
 }
 
@@ -251,6 +255,7 @@ int rf_config_default(rf_config* c) {
   c->velocity_integration = -1;
   c->refinement_tolerance = 1e-6;
   c->refinement_max_iterations = 20;
+  c->refinement_restart = 0;
   return RF_OK;
 }
 
@@ -352,7 +357,9 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (!rc) rc = h->alloc((void**)&h->ffpart, (size_t)tiles * ffn * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->F, ffn * sizeof(float));
   // Krylov
-  const int m = cfg->gmres_restart;
+  const int m = (h->cfg.precision != RF_PREC_FP32 && cfg->refinement_restart > 0) ? cfg->refinement_restart
+                                                                                  : cfg->gmres_restart;
+  h->restart = m;
   h->gemv_plan = plan_dense_gemv(R, h->num_sms);
   if (h->mixed) h->gemv_plan.splits = 1;  // the structured matvec writes complete rows
   h->coop_blocks = krylov_coop_blocks(R, h->num_sms);
@@ -411,7 +418,7 @@ int rf_solve(rf_handle* h) {
   RF_CUDA_TRY(cudaEventRecord(h->ev[2], h->st));
   GmresSetup s;
   s.R = h->R;
-  s.m = h->cfg.gmres_restart;
+  s.m = h->restart;
   s.maxit = h->cfg.gmres_max_iterations;
   s.tol = h->mixed ? h->cfg.refinement_tolerance : h->cfg.gmres_tolerance;
   s.V = h->V;
