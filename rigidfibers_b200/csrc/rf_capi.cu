@@ -452,7 +452,8 @@ int rf_solve(rf_handle* h) {
     int rc;
     if (h->mixed) {
       const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
-      rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip, st);
+      rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
+                                &h->ctl->timeout, st);
       ++mv_launches;
     } else {
       rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
@@ -644,7 +645,9 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
     RF_TRY(launch_reduce_rows(h->ypart, h->gemv_plan.splits, R, dy, h->st));
   } else if (which == 1) {
     const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
-    RF_TRY(launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, dxf, h->zpart, dy, nullptr, h->st));
+    RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
+    RF_TRY(launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, dxf, h->zpart, dy, nullptr,
+                                &h->ctl->timeout, h->st));
   } else {
     RF_CUDA_TRY(cudaMemcpyAsync(h->x64, hx.data(), R * sizeof(double), cudaMemcpyHostToDevice, h->st));
     RF_TRY(launch_struct_apply64(h->tab, h->N, h->S32, h->ori32, h->x64, h->zpart64, dy, h->st));

@@ -466,7 +466,7 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
     RF_CUDA_TRY(cudaStreamSynchronize(st));
     h = *s.host_ctl;
     x_zero = 0;
-    if (h.converged || h.nan) break;
+    if (h.converged || h.nan || h.timeout) break;
     if (h.total_iters >= s.maxit && cycle > 0 && h.jconv == 0) break;
     if (cycle > s.maxit + 2) break;
   }
@@ -474,6 +474,10 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   res->restarts = h.restarts;
   res->matvecs = h.total_iters + (cycles_run - 1);
   res->relative_residual = h.bnorm > 0 ? h.beta / h.bnorm : 0.0;
+  if (h.timeout) {
+    set_last_error_str("a bounded device-side wait timed out");
+    return RF_E_TIMEOUT;
+  }
   if (h.nan) return RF_E_NAN;
   if (!h.converged) return RF_E_NOCONV;
   return RF_OK;

@@ -17,7 +17,7 @@ struct GmresCtl {
   int total_iters;
   int maxit;
   int restarts;
-  int pad;
+  int timeout;        // a bounded device-side wait gave up (set by kernels)
   double tol;
   double bnorm;
   double beta;        // true residual norm at the last cycle start

@@ -23,6 +23,11 @@
 
 namespace rf {
 
+__device__ __forceinline__ int64_t struct_store_tiles_dev(int N) {
+  const int64_t T16 = (N + kStoreTile - 1) / kStoreTile;
+  return T16 * (T16 + 1) / 2;
+}
+
 __device__ __forceinline__ void tile_pair16(int64_t L, int& I, int& J) {
   int64_t j = (int64_t)((sqrt(8.0 * (double)L + 1.0) - 1.0) * 0.5);
   while ((j + 1) * (j + 2) / 2 <= L) ++j;
@@ -262,6 +267,189 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
   }
 }
 
+// ---------------------------------------------------------------------------
+// 16-bit matvec with whole tiles staged through shared memory by TMA bulk
+// copies (cp.async.bulk + mbarrier transaction counts): persistent CTAs,
+// one per SM, two tiles in flight per CTA (~150 KB per SM), so the copy
+// engine keeps HBM busy while the threads compute the previous tile.
+// Every mbarrier wait is bounded: on timeout the CTA records the fault in
+// *err, waits (bounded) for its own copies in flight, and returns.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false on timeout
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 24); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int M>
+struct BulkShape {
+  static constexpr int M3 = 3 * M;
+  static constexpr int NQ16 = M * M * 3;                       // words per pair
+  static constexpr uint32_t kTileBytes = 4u * 8 * NQ16 * 8 * 4;  // 4 sub-tiles x 8 j x NQ16 x 8 i words
+  static constexpr int XS = (M3 + 3) / 4 * 4 + 4;
+  static constexpr size_t kX = (size_t)2 * kStoreTile * XS * 4;
+  static constexpr size_t kWI = (size_t)kStoreTile * 4 * M3 * 4;
+  static constexpr size_t kWJ = (size_t)kStoreTile * 2 * M3 * 4;
+  static constexpr size_t kBytes = 2 * (size_t)kTileBytes + kX + kWI + kWJ + 16;
+};
+
+template <int M, int SMODE>
+__global__ void __launch_bounds__(256, 1)
+k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restrict__ x, float* __restrict__ zpart,
+                  const int* __restrict__ skip, int* __restrict__ err) {
+  constexpr int TI = 8, M3 = 3 * M;
+  using B = BulkShape<M>;
+  using RL = RowLoader<M, TI, SMODE>;
+  constexpr int XS = B::XS;
+  if (skip != nullptr && *skip) return;
+  extern __shared__ __align__(128) unsigned char bsm[];
+  uint32_t* stage[2] = {reinterpret_cast<uint32_t*>(bsm), reinterpret_cast<uint32_t*>(bsm + B::kTileBytes)};
+  float (*sx)[kStoreTile][XS] = reinterpret_cast<float (*)[kStoreTile][XS]>(bsm + 2 * B::kTileBytes);
+  float (*swi)[4][M3] = reinterpret_cast<float (*)[4][M3]>(bsm + 2 * B::kTileBytes + B::kX);
+  float (*swj)[2][M3] = reinterpret_cast<float (*)[2][M3]>(bsm + 2 * B::kTileBytes + B::kX + B::kWI);
+  __shared__ __align__(8) uint64_t bar[2];
+  const int64_t ntiles = struct_store_tiles_dev(N);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int64_t R = (int64_t)M3 * N;
+  const TileMap<TI> mp(t);
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int64_t L, int s) {
+    mbar_expect_tx(&bar[s], B::kTileBytes);
+    bulk_g2s(stage[s], S16 + L * (int64_t)(B::kTileBytes / 4), B::kTileBytes, &bar[s]);
+  };
+  if (t == 0) {
+    for (int s = 0; s < 2; ++s) {
+      const int64_t L = blockIdx.x + (int64_t)s * gridDim.x;
+      if (L < ntiles) issue(L, s);
+    }
+  }
+  bool failed = false;
+  int k = 0;
+  for (int64_t L = blockIdx.x; L < ntiles; L += gridDim.x, ++k) {
+    const int s = k & 1;
+    const uint32_t parity = (k >> 1) & 1;
+    int I16, J16;
+    tile_pair16(L, I16, J16);
+    const bool diag = I16 == J16;
+    for (int q = t; q < 2 * kStoreTile * M3; q += blockDim.x) {
+      const int side = q / (kStoreTile * M3), rem = q % (kStoreTile * M3);
+      const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3, v = rem % M3;
+      sx[side][rem / M3][v] = f < N ? x[(int64_t)f * M3 + v] : 0.f;
+    }
+    const bool ok_wait = mbar_wait_bounded(&bar[s], parity);
+    if (__syncthreads_or(!ok_wait)) {
+      failed = true;
+      break;
+    }
+    const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
+    const bool active = i < j && j < N;
+    const uint32_t* pw = stage[s] + ((mp.sub * TI + mp.jl) * B::NQ16) * TI + mp.tl;
+    float zj[M3];
+#pragma unroll
+    for (int q = 0; q < M3; ++q) zj[q] = 0.f;
+    constexpr int M3P = (M3 + 3) / 4 * 4;
+    float xjr[M3P];
+    load_xrow<float, M3P>(sx[1][mp.j16()], xjr);
+    const float* xi = sx[0][mp.i16()];
+#pragma unroll
+    for (int kI = 0; kI < M; ++kI) {
+      float ziv[3] = {0.f, 0.f, 0.f};
+      if (active) {
+        uint32_t w[3 * M];
+#pragma unroll
+        for (int q = 0; q < 3 * M; ++q) w[q] = pw[(kI * 3 * M + q) * TI];
+        const float xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
+#pragma unroll
+        for (int kJ = 0; kJ < M; ++kJ) {
+          float tv[6];
+          RL::values(w, kJ, tv);
+          sym_mv_acc(tv, xjr + 3 * kJ, ziv);
+          sym_mv_acc(tv, xik, zj + 3 * kJ);
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        float v = ziv[a];
+        v += shfl_xor(v, 8);
+        v += shfl_xor(v, 16);
+        if (lane < TI) swi[mp.i16()][warp & 3][3 * kI + a] = v;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < M3; ++q) {
+      float b = zj[q];
+      b += shfl_xor(b, 1);
+      b += shfl_xor(b, 2);
+      b += shfl_xor(b, 4);
+      zj[q] = b;
+    }
+    if ((lane & (TI - 1)) == 0) {
+#pragma unroll
+      for (int q = 0; q < M3; ++q) swj[mp.j16()][warp >> 2][q] = zj[q];
+    }
+    __syncthreads();
+    // stage s is free again: refill it with the tile two steps ahead
+    if (t == 0) {
+      const int64_t Ln = L + 2 * (int64_t)gridDim.x;
+      if (Ln < ntiles) issue(Ln, s);
+    }
+    for (int task = t; task < kStoreTile * M3; task += blockDim.x) {
+      const int rf = task / M3, rv = task % M3;
+      const float si = ((swi[rf][0][rv] + swi[rf][1][rv]) + swi[rf][2][rv]) + swi[rf][3][rv];
+      const float sj = swj[rf][0][rv] + swj[rf][1][rv];
+      const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
+      if (diag) {
+        if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si + sj;
+      } else {
+        if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si;
+        if (fj < N) zpart[(int64_t)I16 * R + (int64_t)fj * M3 + rv] = sj;
+      }
+    }
+  }
+  if (failed) {
+    if (t == 0) {
+      atomicExch(err, 1);
+      // drain: wait (bounded) for the copies this CTA still has in flight
+      for (int kk = k; kk < k + 2; ++kk) {
+        const int64_t L = blockIdx.x + (int64_t)kk * gridDim.x;
+        if (L < ntiles) (void)mbar_wait_bounded(&bar[kk & 1], (kk >> 1) & 1);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // y = x + C z (z = sum of partials), or r = b - (x + C z).  One thread per (fiber, k).
 template <typename XT, typename ACC, bool RESIDUAL>
 __global__ void k_struct_finalize(const Tables tab, int N, const float4* __restrict__ ori, const XT* __restrict__ x,
@@ -425,13 +613,44 @@ static int launch_z(int smode, bool fp64, int N, const float* S32, const uint32_
   return launch_z_one<M, TI, 2, float, float>(N, S32, S16, (const float*)x, (float*)zpart, skip, st);
 }
 
+template <int M, int SMODE>
+static int launch_z16_bulk(int N, const uint32_t* S16, const float* x, float* zpart, const int* skip, int* err,
+                           cudaStream_t st) {
+  using B = BulkShape<M>;
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    RF_CUDA_TRY(cudaGetDevice(&dev));
+    RF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z16_bulk<M, SMODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)B::kBytes));
+  }
+  const int64_t ntiles = struct_store_tiles(N);
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
+  k_struct_z16_bulk<M, SMODE><<<grid, 256, B::kBytes, st>>>(N, S16, x, zpart, skip, err);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
 int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
-                         const float4* ori, const float* x, float* zpart, float* y, const int* skip, cudaStream_t st) {
+                         const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
+                         cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
+  if (tab.Q == 24 && smode != 0 && err != nullptr && tab.M <= 5) {
+    // tiles staged by TMA bulk copies (two 3072*M-byte tiles per SM fit in shared memory for M <= 5)
+    switch (tab.M) {
+      case 1: rc = smode == 1 ? launch_z16_bulk<1, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<1, 2>(N, S16, x, zpart, skip, err, st); break;
+      case 2: rc = smode == 1 ? launch_z16_bulk<2, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<2, 2>(N, S16, x, zpart, skip, err, st); break;
+      case 3: rc = smode == 1 ? launch_z16_bulk<3, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<3, 2>(N, S16, x, zpart, skip, err, st); break;
+      case 4: rc = smode == 1 ? launch_z16_bulk<4, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<4, 2>(N, S16, x, zpart, skip, err, st); break;
+      case 5: rc = smode == 1 ? launch_z16_bulk<5, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<5, 2>(N, S16, x, zpart, skip, err, st); break;
+    }
+  } else {
 #define RF_Z_CASE(MM, QQ) \
   if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(smode, false, N, S32, S16, x, zpart, skip, st);
-  RF_FOR_EACH_MQ(RF_Z_CASE)
+    RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
+  }
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
   k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(
