@@ -310,17 +310,22 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 template <int M>
 struct BulkShape {
   static constexpr int M3 = 3 * M;
-  static constexpr int NQ16 = M * M * 3;                       // words per pair
+  static constexpr int NQ16 = M * M * 3;                         // words per pair
   static constexpr uint32_t kTileBytes = 4u * 8 * NQ16 * 8 * 4;  // 4 sub-tiles x 8 j x NQ16 x 8 i words
   static constexpr int XS = (M3 + 3) / 4 * 4 + 4;
-  static constexpr size_t kX = (size_t)2 * kStoreTile * XS * 4;
+  static constexpr size_t kX = (size_t)2 * 2 * kStoreTile * XS * 4;   // double-buffered x rows
   static constexpr size_t kWI = (size_t)kStoreTile * 4 * M3 * 4;
-  static constexpr size_t kWJ = (size_t)kStoreTile * 2 * M3 * 4;
-  static constexpr size_t kBytes = 2 * (size_t)kTileBytes + kX + kWI + kWJ + 16;
+  static constexpr size_t kWJ = (size_t)kStoreTile * 4 * M3 * 4;
+  static constexpr size_t kBytes = 2 * (size_t)kTileBytes + kX + kWI + kWJ;
+  static constexpr int kThreads = 512;                            // two threads per pair
+  static constexpr int KSPLIT = (M + 1) / 2;                       // block rows of the first half
 };
 
+// Thread t: half h = t / 256 takes block rows [h ? KSPLIT : 0, h ? M : KSPLIT)
+// of pair tt = t % 256 (TileMap).  z_i of a row comes from one half only;
+// z_j gets one partial per half (4 slots per row fiber).
 template <int M, int SMODE>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(512, 1)
 k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restrict__ x, float* __restrict__ zpart,
                   const int* __restrict__ skip, int* __restrict__ err) {
   constexpr int TI = 8, M3 = 3 * M;
@@ -330,24 +335,42 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
   if (skip != nullptr && *skip) return;
   extern __shared__ __align__(128) unsigned char bsm[];
   uint32_t* stage[2] = {reinterpret_cast<uint32_t*>(bsm), reinterpret_cast<uint32_t*>(bsm + B::kTileBytes)};
-  float (*sx)[kStoreTile][XS] = reinterpret_cast<float (*)[kStoreTile][XS]>(bsm + 2 * B::kTileBytes);
+  float (*sx)[2][kStoreTile][XS] = reinterpret_cast<float (*)[2][kStoreTile][XS]>(bsm + 2 * B::kTileBytes);
   float (*swi)[4][M3] = reinterpret_cast<float (*)[4][M3]>(bsm + 2 * B::kTileBytes + B::kX);
-  float (*swj)[2][M3] = reinterpret_cast<float (*)[2][M3]>(bsm + 2 * B::kTileBytes + B::kX + B::kWI);
+  float (*swj)[4][M3] = reinterpret_cast<float (*)[4][M3]>(bsm + 2 * B::kTileBytes + B::kX + B::kWI);
   __shared__ __align__(8) uint64_t bar[2];
   const int64_t ntiles = struct_store_tiles_dev(N);
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int t = threadIdx.x, lane = t & 31;
+  const int half = t >> 8, tt = t & 255, hw = tt >> 5;   // warp index within the half
+  const int kbeg = half ? B::KSPLIT : 0, kend = half ? M : B::KSPLIT;
   const int64_t R = (int64_t)M3 * N;
-  const TileMap<TI> mp(t);
+  const TileMap<TI> mp(tt);
   if (t == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncthreads();
   auto issue = [&](int64_t L, int s) {
     mbar_expect_tx(&bar[s], B::kTileBytes);
     bulk_g2s(stage[s], S16 + L * (int64_t)(B::kTileBytes / 4), B::kTileBytes, &bar[s]);
   };
+  // x rows of a tile: thread t < 2*16*M3 owns one value
+  auto xval = [&](int64_t L) -> float {
+    if (t >= 2 * kStoreTile * M3 || L >= ntiles) return 0.f;
+    int I16, J16;
+    tile_pair16(L, I16, J16);
+    const int side = t / (kStoreTile * M3), rem = t % (kStoreTile * M3);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
+    return f < N ? x[(int64_t)f * M3 + rem % M3] : 0.f;
+  };
+  auto xstore = [&](int buf, float v) {
+    if (t < 2 * kStoreTile * M3) {
+      const int side = t / (kStoreTile * M3), rem = t % (kStoreTile * M3);
+      sx[buf][side][rem / M3][rem % M3] = v;
+    }
+  };
+  xstore(0, xval(blockIdx.x));
+  __syncthreads();
   if (t == 0) {
     for (int s = 0; s < 2; ++s) {
       const int64_t L = blockIdx.x + (int64_t)s * gridDim.x;
@@ -357,16 +380,12 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
   bool failed = false;
   int k = 0;
   for (int64_t L = blockIdx.x; L < ntiles; L += gridDim.x, ++k) {
-    const int s = k & 1;
+    const int s = k & 1, xb = k & 1;
     const uint32_t parity = (k >> 1) & 1;
     int I16, J16;
     tile_pair16(L, I16, J16);
     const bool diag = I16 == J16;
-    for (int q = t; q < 2 * kStoreTile * M3; q += blockDim.x) {
-      const int side = q / (kStoreTile * M3), rem = q % (kStoreTile * M3);
-      const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3, v = rem % M3;
-      sx[side][rem / M3][v] = f < N ? x[(int64_t)f * M3 + v] : 0.f;
-    }
+    const float xnext = xval(L + gridDim.x);   // in flight while this tile is computed
     const bool ok_wait = mbar_wait_bounded(&bar[s], parity);
     if (__syncthreads_or(!ok_wait)) {
       failed = true;
@@ -380,10 +399,11 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     for (int q = 0; q < M3; ++q) zj[q] = 0.f;
     constexpr int M3P = (M3 + 3) / 4 * 4;
     float xjr[M3P];
-    load_xrow<float, M3P>(sx[1][mp.j16()], xjr);
-    const float* xi = sx[0][mp.i16()];
+    load_xrow<float, M3P>(sx[xb][1][mp.j16()], xjr);
+    const float* xi = sx[xb][0][mp.i16()];
 #pragma unroll
     for (int kI = 0; kI < M; ++kI) {
+      if (kI < kbeg || kI >= kend) continue;   // uniform per warp
       float ziv[3] = {0.f, 0.f, 0.f};
       if (active) {
         uint32_t w[3 * M];
@@ -403,7 +423,7 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
         float v = ziv[a];
         v += shfl_xor(v, 8);
         v += shfl_xor(v, 16);
-        if (lane < TI) swi[mp.i16()][warp & 3][3 * kI + a] = v;
+        if (lane < TI) swi[mp.i16()][hw & 3][3 * kI + a] = v;
       }
     }
 #pragma unroll
@@ -416,8 +436,9 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     }
     if ((lane & (TI - 1)) == 0) {
 #pragma unroll
-      for (int q = 0; q < M3; ++q) swj[mp.j16()][warp >> 2][q] = zj[q];
+      for (int q = 0; q < M3; ++q) swj[mp.j16()][2 * half + (hw >> 2)][q] = zj[q];
     }
+    xstore(xb ^ 1, xnext);
     __syncthreads();
     // stage s is free again: refill it with the tile two steps ahead
     if (t == 0) {
@@ -427,7 +448,7 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     for (int task = t; task < kStoreTile * M3; task += blockDim.x) {
       const int rf = task / M3, rv = task % M3;
       const float si = ((swi[rf][0][rv] + swi[rf][1][rv]) + swi[rf][2][rv]) + swi[rf][3][rv];
-      const float sj = swj[rf][0][rv] + swj[rf][1][rv];
+      const float sj = ((swj[rf][0][rv] + swj[rf][1][rv]) + swj[rf][2][rv]) + swj[rf][3][rv];
       const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
       if (diag) {
         if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si + sj;
@@ -627,7 +648,7 @@ static int launch_z16_bulk(int N, const uint32_t* S16, const float* x, float* zp
   }
   const int64_t ntiles = struct_store_tiles(N);
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
-  k_struct_z16_bulk<M, SMODE><<<grid, 256, B::kBytes, st>>>(N, S16, x, zpart, skip, err);
+  k_struct_z16_bulk<M, SMODE><<<grid, B::kThreads, B::kBytes, st>>>(N, S16, x, zpart, skip, err);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
