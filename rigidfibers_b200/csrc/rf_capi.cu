@@ -345,8 +345,9 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   } else {
     if (!rc) rc = h->alloc((void**)&h->S32, (size_t)struct_floats32(h->M, N) * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->S16, (size_t)struct_words16(h->M, N) * sizeof(uint32_t));
-    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)T16 * (size_t)R * sizeof(float));
-    if (!rc) rc = h->alloc((void**)&h->zpart64, (size_t)T16 * (size_t)R * sizeof(double));
+    // one extra row slot holds the summed partials
+    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)(T16 + 1) * (size_t)R * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&h->zpart64, (size_t)(T16 + 1) * (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&h->x64, (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&h->svpart, (size_t)T16 * N * 6 * sizeof(float));
   }
@@ -454,7 +455,7 @@ int rf_solve(rf_handle* h) {
       const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
       rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
                                 &h->ctl->timeout, st);
-      ++mv_launches;
+      mv_launches += 2;
     } else {
       rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
     }

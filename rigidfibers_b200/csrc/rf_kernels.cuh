@@ -28,13 +28,13 @@ int64_t struct_store_tiles(int N);
 int64_t struct_floats32(int M, int N);
 int64_t struct_words16(int M, int N);
 // y = A v on the structured operator (smode 0 FP32 / 1 FP16 / 2 BF16 storage, FP32 accumulation);
-// zpart: ceil(N/16) x R floats.
+// zpart: (ceil(N/16) + 1) x R floats.
 // err: device word set to 1 if a bounded wait inside the kernel gave up (may be null:
 // then the register-staged kernel is used)
 int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
                          cudaStream_t st);
-// r = b - A x with the FP32 blocks, x and accumulation in FP64; zpart64: ceil(N/16) x R doubles.
+// r = b - A x with the FP32 blocks, x and accumulation in FP64; zpart64: (ceil(N/16) + 1) x R doubles.
 int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
                              double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st);
 // y = A x with the FP32 blocks, x and accumulation in FP64.

@@ -471,6 +471,34 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
   }
 }
 
+// zsum[r] = sum_p zpart[p][r] (fixed order within each of 4 p-groups, then
+// the 4 groups in order).  256 threads = 64 consecutive rows x 4 groups, the
+// p loop unrolled so that 8 loads per thread are in flight.
+template <typename ACC>
+__global__ void __launch_bounds__(256)
+k_sum_parts(const ACC* __restrict__ part, int nparts, int64_t R, ACC* __restrict__ out,
+            const int* __restrict__ skip) {
+  if (skip != nullptr && *skip) return;
+  __shared__ ACC red[4][64];
+  const int rr = threadIdx.x & 63, g = threadIdx.x >> 6;
+  const int64_t r = (int64_t)blockIdx.x * 64 + rr;
+  ACC s = (ACC)0;
+  if (r < R) {
+    int p = g;
+    for (; p + 28 < nparts; p += 32) {
+      ACC v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = part[(int64_t)(p + 4 * u) * R + r];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += v[u];
+    }
+    for (; p < nparts; p += 4) s += part[(int64_t)p * R + r];
+  }
+  red[g][rr] = s;
+  __syncthreads();
+  if (g == 0 && r < R) out[r] = ((red[0][rr] + red[1][rr]) + red[2][rr]) + red[3][rr];
+}
+
 // y = x + C z (z = sum of partials), or r = b - (x + C z).  One thread per (fiber, k).
 template <typename XT, typename ACC, bool RESIDUAL>
 __global__ void k_struct_finalize(const Tables tab, int N, const float4* __restrict__ ori, const XT* __restrict__ x,
@@ -674,8 +702,13 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
   }
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
+  const int64_t R = 3 * n;
+  const int nparts = (int)ceil_div(N, kStoreTile);
+  // the summed rows go to partial slot 0 (read by nothing else afterwards)
+  k_sum_parts<float><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart, nparts, R, zpart + (int64_t)nparts * R, skip);
+  RF_LAUNCH_CHECK();
   k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(
-      tab, N, ori, x, zpart, (int)ceil_div(N, kStoreTile), nullptr, y, skip);
+      tab, N, ori, x, zpart + (int64_t)nparts * R, 1, nullptr, y, skip);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
@@ -689,8 +722,13 @@ int launch_struct_residual64(const Tables& tab, int N, const float* S32, const f
 #undef RF_Z_CASE
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
+  const int64_t R = 3 * n;
+  const int nparts = (int)ceil_div(N, kStoreTile);
+  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, nparts, R, zpart64 + (int64_t)nparts * R,
+                                                                 skip);
+  RF_LAUNCH_CHECK();
   k_struct_finalize<double, double, true><<<fin_blocks(n), 256, 0, st>>>(
-      tab, N, ori, x, zpart64, (int)ceil_div(N, kStoreTile), b, r, skip);
+      tab, N, ori, x, zpart64 + (int64_t)nparts * R, 1, b, r, skip);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
@@ -704,8 +742,13 @@ int launch_struct_apply64(const Tables& tab, int N, const float* S32, const floa
 #undef RF_Z_CASE
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
+  const int64_t R = 3 * n;
+  const int nparts = (int)ceil_div(N, kStoreTile);
+  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, nparts, R, zpart64 + (int64_t)nparts * R,
+                                                                 nullptr);
+  RF_LAUNCH_CHECK();
   k_struct_finalize<double, double, false><<<fin_blocks(n), 256, 0, st>>>(
-      tab, N, ori, x, zpart64, (int)ceil_div(N, kStoreTile), nullptr, y, nullptr);
+      tab, N, ori, x, zpart64 + (int64_t)nparts * R, 1, nullptr, y, nullptr);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
