@@ -622,45 +622,46 @@ static int gmres(int n, const T* A, const T* b, T* x, int restart, int maxit, do
   }
 }
 
-// BiCGSTAB (van der Vorst 1992), x0 = 0, restarted from the true residual
-// every `restart_every` iterations; stops when ||r||/||b|| <= tol.
+// BiCGSTAB (van der Vorst 1992) with the semantics of the reference's
+// ViennaCL 1.5.1 solver (lib/viennacl/linalg/bicgstab.hpp:80-166): x0 = 0,
+// convergence when ||r||/||b|| < tol on the recursive residual after a full
+// iteration, restart from the true residual when rho or omega vanish or more
+// than `restart_every` iterations passed since the last restart.
 template <typename T>
 static int bicgstab(int n, const T* A, const T* b, T* x, int maxit, double tol, int restart_every, double* relres) {
   std::vector<T> r(n), r0(n), p(n), v(n), s(n), t(n);
   std::fill(x, x + n, (T)0);
   const double bnorm = std::sqrt(dot(n, b, b));
   if (bnorm == 0) { *relres = 0; return 0; }
-  for (int i = 0; i < n; ++i) { r[i] = b[i]; r0[i] = b[i]; p[i] = b[i]; }
-  double rho = dot(n, r.data(), r0.data());
-  for (int it = 1; it <= maxit; ++it) {
+  bool restart = true;
+  int last_restart = 0;
+  double rho = 0;
+  for (int i = 0; i < maxit; ++i) {
+    if (restart) {
+      gemv_colmajor(n, n, A, x, t.data());
+      for (int k = 0; k < n; ++k) { r[k] = b[k] - t[k]; p[k] = r[k]; r0[k] = r[k]; }
+      rho = dot(n, r.data(), r.data());
+      restart = false;
+      last_restart = i;
+    }
     gemv_colmajor(n, n, A, p.data(), v.data());
     const double alpha = rho / dot(n, v.data(), r0.data());
-    for (int i = 0; i < n; ++i) s[i] = r[i] - (T)alpha * v[i];
-    if (std::sqrt(dot(n, s.data(), s.data())) / bnorm <= tol) {
-      for (int i = 0; i < n; ++i) x[i] += (T)alpha * p[i];
-      *relres = std::sqrt(dot(n, s.data(), s.data())) / bnorm;
-      return it;
-    }
+    for (int k = 0; k < n; ++k) s[k] = r[k] - (T)alpha * v[k];
     gemv_colmajor(n, n, A, s.data(), t.data());
     const double tt = dot(n, t.data(), t.data());
     const double omega = tt > 0 ? dot(n, t.data(), s.data()) / tt : 0.0;
-    for (int i = 0; i < n; ++i) {
-      x[i] += (T)alpha * p[i] + (T)omega * s[i];
-      r[i] = s[i] - (T)omega * t[i];
+    for (int k = 0; k < n; ++k) {
+      x[k] = x[k] + (T)alpha * p[k] + (T)omega * s[k];
+      r[k] = s[k] - (T)omega * t[k];
     }
-    const double rn = std::sqrt(dot(n, r.data(), r.data())) / bnorm;
-    *relres = rn;
-    if (rn <= tol) return it;
-    double rho_new = dot(n, r.data(), r0.data());
-    if (restart_every > 0 && it % restart_every == 0) {
-      gemv_colmajor(n, n, A, x, t.data());
-      for (int i = 0; i < n; ++i) { r[i] = b[i] - t[i]; r0[i] = r[i]; p[i] = r[i]; }
-      rho = dot(n, r.data(), r0.data());
-      continue;
-    }
+    const double rho_new = dot(n, r.data(), r0.data());
+    const double rn = std::sqrt(dot(n, r.data(), r.data()));
+    *relres = rn / bnorm;
+    if (rn / bnorm < tol) return i + 1;
     const double beta = (rho_new / rho) * (alpha / omega);
-    for (int i = 0; i < n; ++i) p[i] = r[i] + (T)beta * (p[i] - (T)omega * v[i]);
     rho = rho_new;
+    if (rho == 0 || omega == 0 || i - last_restart > restart_every) restart = true;
+    for (int k = 0; k < n; ++k) p[k] = r[k] + (T)beta * (p[k] - (T)omega * v[k]);
   }
   return -1;
 }

@@ -31,6 +31,7 @@
 //                whole 32-byte sectors (see rf_struct.cu).
 #include "rf_common.cuh"
 #include "rf_kernels.cuh"
+#include "rf_analytic.cuh"
 
 namespace rf {
 
@@ -44,6 +45,7 @@ __device__ __forceinline__ void tile_pair(int64_t L, int& I, int& J) {
 }
 
 enum AsmMode { kAsmDense = 0, kAsmStructF16 = 1, kAsmStructBF16 = 2 };
+enum AsmInteg { kNumerical = 0, kAnalytical = 1 };
 
 template <int M, int Q>
 struct AsmShape {
@@ -80,10 +82,10 @@ struct AsmOut {
   float* ffpart;
 };
 
-template <int M, int Q, int MODE>
-__global__ void __launch_bounds__(192, 4)
-k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
-                     AsmOut out) {
+template <int M, int Q, int MODE, int INTEG>
+__global__ void __launch_bounds__(192, INTEG == kNumerical ? 4 : 2)
+k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+                 AsmOut out) {
   using S = AsmShape<M, Q>;
   constexpr int TI = S::TI, K1 = S::K1, NC = S::NC, H = S::H;
   constexpr int M3 = 3 * M;
@@ -99,8 +101,18 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
   __shared__ float sfJ[TI][FF];
   __shared__ short sMap16[S::NQ16 * 2];   // 16-bit value q' -> offset of its T entry within a pair
 
+  // numerical: unordered tile pairs (I <= J), both blocks of a pair from one
+  // evaluation of K; analytical: ordered tile pairs, direct blocks only
+  constexpr bool SYM = INTEG == kNumerical;
+  static_assert(SYM || MODE == kAsmDense, "structured storage needs the symmetric numerical blocks");
   int I, J;
-  tile_pair(blockIdx.x, I, J);
+  if (SYM) {
+    tile_pair(blockIdx.x, I, J);
+  } else {
+    const int T = (N + TI - 1) / TI;
+    I = (int)(blockIdx.x / T);
+    J = (int)(blockIdx.x % T);
+  }
   const bool diag = (I == J);
   const int tid = threadIdx.x;
   const int i0 = I * TI, j0 = J * TI;
@@ -150,14 +162,25 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     // step jl still reads, so one barrier per step suffices after phase 2
     float* const sTflat = sTbase + (jl & 1) * (TI * S::TP);
     auto sT = [&](int tl, int k, int kj) -> float* { return sTflat + tl * S::TP + (k * K1 + kj) * 6; };
-    const bool pair_ok = unit_ok && (!diag || il < jl);
-    // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj], mirror-folded over qj
+    const bool pair_ok = unit_ok && (!diag || (SYM ? il < jl : il != jl));
+    // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj] (numerical, mirror-
+    // folded over qj) or the closed-form integral (analytical)
     float g[6][K1];
 #pragma unroll
     for (int c = 0; c < 6; ++c)
 #pragma unroll
       for (int k = 0; k < K1; ++k) g[c][k] = 0.f;
-    if (pair_ok) {
+    if (!SYM && pair_ok) {
+      const float4 xi4 = pos[i], ti4 = ori[i];
+      const float4 xj4 = pos[j0 + jl], tj4 = sTj[jl];
+      const double s = (double)tab.pts[qi];
+      const double R0[3] = {(double)xi4.x + s * (double)ti4.x - (double)xj4.x,
+                            (double)xi4.y + s * (double)ti4.y - (double)xj4.y,
+                            (double)xi4.z + s * (double)ti4.z - (double)xj4.z};
+      const double tj[3] = {(double)tj4.x, (double)tj4.y, (double)tj4.z};
+      analytic_G<M>(R0, tj, 2.0 * (double)tab.eps * (double)tab.eps, g);
+    }
+    if (SYM && pair_ok) {
 #pragma unroll
       for (int q = 0; q < H; ++q) {
         float Kp[6], Km[6];
@@ -224,7 +247,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
         const int kJp = task / (TI * M), rem = task % (TI * M);
         const int tl = rem / M, kIp = rem % M;
         const int ii = i0 + tl;
-        if (ii >= N || (diag && tl > jl)) continue;
+        if (ii >= N || (SYM && diag && tl > jl)) continue;
         float* dst = out.A + (int64_t)(i0 * M3 + 3 * rem) + (int64_t)(j * M3 + 3 * kJp) * out.lda;
         if (diag && tl == jl) {
 #pragma unroll
@@ -248,7 +271,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
             dst[a + b * out.lda] = kIp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
       }
       // ---- phase 3b: block (j, i) -- rows of fiber j, columns of fiber i
-      {
+      if (SYM) {
         const float4 tj = sTj[jl];
         const float t3[3] = {tj.x, tj.y, tj.z};
         for (int task = tid; task < TI * M * M; task += blockDim.x) {
@@ -305,14 +328,14 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     //      F_j[kj] += T^{ij}[P0][kj] F/2 (F/2 = (0, 0, fz): column z of the block)
     if (tid < TI * K1) {
       const int tl = tid / K1, k = tid % K1;
-      if (i0 + tl < N && (!diag || tl < jl)) {
+      if (i0 + tl < N && (!diag || (SYM ? tl < jl : tl != jl))) {
         const float* T6 = sT(tl, k, 0);
         facc[0] = fmaf(T6[4], fz, facc[0]);
         facc[1] = fmaf(T6[5], fz, facc[1]);
         facc[2] = fmaf(T6[2], fz, facc[2]);
       }
     }
-    if (tid < K1) {
+    if (SYM && tid < K1) {
       const int kj = tid;
       float s[3] = {0.f, 0.f, 0.f};
       for (int tl = 0; tl < TI; ++tl) {
@@ -334,7 +357,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     const int tl = tid / K1, k = tid % K1;
     if (i0 + tl < N) {
       float v[3] = {facc[0], facc[1], facc[2]};
-      if (diag) {
+      if (SYM && diag) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) v[a] += sfJ[tl][3 * k + a];
       }
@@ -343,7 +366,7 @@ k_assemble_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
       for (int a = 0; a < 3; ++a) dst[a] = v[a];
     }
   }
-  if (!diag) {
+  if (SYM && !diag) {
     for (int k = tid; k < TI * FF; k += blockDim.x) {
       const int jl = k / FF;
       if (j0 + jl < N) ffpart[((int64_t)I * N + j0) * FF + k] = (&sfJ[0][0])[k];
@@ -411,19 +434,19 @@ int64_t struct_words16(int M, int N) {
   return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * M * M * 3;
 }
 
-template <int M, int Q, int MODE>
+template <int M, int Q, int MODE, int INTEG>
 static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
                               float* F, float* b, cudaStream_t st) {
   using S = AsmShape<M, Q>;
   const int64_t T = ceil_div(N, S::TI);
-  const int64_t ntp = T * (T + 1) / 2;
+  const int64_t ntp = INTEG == kNumerical ? T * (T + 1) / 2 : T * T;
   static bool attr_set = false;  // per process; the attribute is per function
   if (!attr_set) {
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_numerical<M, Q, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)S::kSmem));
+    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_pairs<M, Q, MODE, INTEG>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem));
     attr_set = true;
   }
-  k_assemble_numerical<M, Q, MODE><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
+  k_assemble_pairs<M, Q, MODE, INTEG><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
   RF_LAUNCH_CHECK();
   const int64_t n = (int64_t)N * (M + 1);
   k_force_terms<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 8), 256, 0, st>>>(tab, N, ori, out.ffpart,
@@ -432,11 +455,11 @@ static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const
   return RF_OK;
 }
 
-template <int MODE>
+template <int MODE, int INTEG>
 static int dispatch_assemble(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
                              float* F, float* b, cudaStream_t st) {
 #define RF_ASM_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) return launch_assemble_mq<MM, QQ, MODE>(tab, N, pos, ori, out, F, b, st);
+  if (tab.M == MM && tab.Q == QQ) return launch_assemble_mq<MM, QQ, MODE, INTEG>(tab, N, pos, ori, out, F, b, st);
   RF_FOR_EACH_MQ(RF_ASM_CASE)
 #undef RF_ASM_CASE
   set_last_error_str("assemble: (M, Q) combination not instantiated");
@@ -449,7 +472,16 @@ int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const
   out.A = A;
   out.lda = lda;
   out.ffpart = ffpart;
-  return dispatch_assemble<kAsmDense>(tab, N, pos, ori, out, F, b, st);
+  return dispatch_assemble<kAsmDense, kNumerical>(tab, N, pos, ori, out, F, b, st);
+}
+
+int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
+                               int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
+  AsmOut out{};
+  out.A = A;
+  out.lda = lda;
+  out.ffpart = ffpart;
+  return dispatch_assemble<kAsmDense, kAnalytical>(tab, N, pos, ori, out, F, b, st);
 }
 
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
@@ -458,8 +490,8 @@ int launch_assemble_structured(const Tables& tab, int N, const float4* pos, cons
   out.S32 = S32;
   out.S16 = S16;
   out.ffpart = ffpart;
-  if (bf16) return dispatch_assemble<kAsmStructBF16>(tab, N, pos, ori, out, F, b, st);
-  return dispatch_assemble<kAsmStructF16>(tab, N, pos, ori, out, F, b, st);
+  if (bf16) return dispatch_assemble<kAsmStructBF16, kNumerical>(tab, N, pos, ori, out, F, b, st);
+  return dispatch_assemble<kAsmStructF16, kNumerical>(tab, N, pos, ori, out, F, b, st);
 }
 
 }  // namespace rf

@@ -91,6 +91,7 @@ static Tables make_tables(const rf_config& c) {
   const float df = -cf;
   t.d = df;
   t.e2 = 2.0f * epsf * epsf;
+  t.eps = epsf;
   t.fz_half = -0.5f;
   t.gamma[0] = 0.75f / (df - 2.0f * 1.0f);  // D1
   t.eigen[0] = (float)eig[0];
@@ -145,6 +146,9 @@ struct rf_handle {
   double* g = nullptr;
   GmresCtl* ctl = nullptr;
   GmresCtl* host_ctl = nullptr;
+  float* bicg_work = nullptr;     // BiCGSTAB vectors r, r0, p, v, s, t
+  BicgCtl* bctl = nullptr;
+  BicgCtl* host_bctl = nullptr;
   DenseGemvPlan gemv_plan;
   int coop_blocks = 1;
   // velocity scratch
@@ -179,6 +183,7 @@ struct rf_handle {
     for (auto e : mv_events) cudaEventDestroy(e);
     for (void* p : allocations) cudaFree(p);
     if (host_ctl) cudaFreeHost(host_ctl);
+    if (host_bctl) cudaFreeHost(host_bctl);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -222,8 +227,13 @@ static int validate_config(const rf_config* c, int N) {
   if (c->precision != RF_PREC_FP32 && !(c->refinement_tolerance > 0.0)) {
     set_last_error_str("refinement_tolerance must be positive"); return RF_E_INPUT;
   }
-  if (c->integration == RF_ANALYTICAL) { set_last_error_str("analytical integration not built yet"); return RF_E_UNSUPPORTED; }
-  if (c->solver != RF_SOLVER_GMRES) { set_last_error_str("solver not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->velocity_integration < -1 || c->velocity_integration > 1) {
+    set_last_error_str("velocity_integration must be -1, 0 or 1"); return RF_E_INPUT;
+  }
+  if (c->solver == RF_SOLVER_DIRECT) { set_last_error_str("direct solver not built yet"); return RF_E_UNSUPPORTED; }
+  if (c->solver == RF_SOLVER_BICGSTAB && (c->bicgstab_max_iterations < 1 || !(c->bicgstab_tolerance > 0.0))) {
+    set_last_error_str("bicgstab_max_iterations / bicgstab_tolerance"); return RF_E_INPUT;
+  }
   if (c->gmres_restart < 1 || c->gmres_restart > kMaxRestart) { set_last_error_str("gmres restart in [1, 64]"); return RF_E_INPUT; }
   if (c->refinement_restart < 0 || c->refinement_restart > kMaxRestart) {
     set_last_error_str("refinement_restart in [0, 64]"); return RF_E_INPUT;
@@ -374,6 +384,11 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (!rc) rc = h->alloc((void**)&h->g, (size_t)(m + 1) * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->ctl, sizeof(GmresCtl));
   if (!rc && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
+  if (cfg->solver == RF_SOLVER_BICGSTAB) {
+    if (!rc) rc = h->alloc((void**)&h->bicg_work, (size_t)6 * (size_t)ldv * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&h->bctl, sizeof(BicgCtl));
+    if (!rc && cudaMallocHost((void**)&h->host_bctl, sizeof(BicgCtl)) != cudaSuccess) rc = RF_E_OOM;
+  }
   // velocities
   if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
   if (!rc) rc = h->alloc((void**)&h->vpart, (size_t)velocity_chunks(N) * N * 6 * sizeof(float));
@@ -404,6 +419,8 @@ int rf_assemble(rf_handle* h) {
   if (h->mixed)
     RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->S32, h->S16,
                                       h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st));
+  else if (h->cfg.integration == RF_ANALYTICAL)
+    RF_TRY(launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
   else
     RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
   h->launches += 2;
@@ -462,6 +479,33 @@ int rf_solve(rf_handle* h) {
     if (h->profile) RF_CUDA_TRY(cudaEventRecord(e1, st));
     return rc;
   };
+  if (h->cfg.solver == RF_SOLVER_BICGSTAB) {
+    BicgSetup bs;
+    bs.R = h->R;
+    bs.maxit = h->cfg.bicgstab_max_iterations;
+    bs.restart_every = 200;   // ViennaCL's max_iterations_before_restart default (bicgstab.hpp:51)
+    bs.tol = h->cfg.bicgstab_tolerance;
+    bs.work = h->bicg_work;
+    bs.ldv = ceil_div(h->R, 32) * 32;
+    bs.ypart = h->ypart;
+    bs.nsplit = h->gemv_plan.splits;
+    bs.part = h->part;
+    bs.ctl = h->bctl;
+    bs.host_ctl = h->host_bctl;
+    bs.coop_blocks = h->coop_blocks;
+    BicgResult br;
+    int brc = bicgstab_solve(bs, mv, h->b, h->x, h->st, &br);
+    RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
+    h->launches += br.launches + mv_launches;
+    h->matvecs_done = br.matvecs;
+    h->stats.iterations = br.iterations;
+    h->stats.restarts = br.restarts;
+    h->stats.refinement_steps = 0;
+    h->stats.relative_residual = br.relative_residual;
+    if (brc != RF_OK && brc != RF_E_NOCONV) return brc;
+    h->solved = true;
+    return brc;
+  }
   GmresResult res;
   int rc;
   if (h->mixed) {
@@ -497,7 +541,12 @@ int rf_update_velocities(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   if (!h->solved) { set_last_error_str("rf_update_velocities before rf_solve"); return RF_E_STATE; }
   RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
-  if (h->mixed) {
+  const int vint = h->cfg.velocity_integration < 0 ? h->cfg.integration : h->cfg.velocity_integration;
+  if (vint == RF_ANALYTICAL) {
+    RF_TRY(launch_velocity_analytical(h->tab, h->N, h->pos32, h->ori32, h->x, h->vpart, h->tv[h->vcur],
+                                      h->rv[h->vcur], h->st));
+    h->launches += 2;
+  } else if (h->mixed) {
     RF_TRY(launch_struct_velocity(h->tab, h->N, h->S32, h->ori32, h->F, h->x, h->svpart, h->tv[h->vcur],
                                   h->rv[h->vcur], h->st));
     h->launches += 2;

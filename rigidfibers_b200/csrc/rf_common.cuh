@@ -26,6 +26,7 @@ struct Tables {
   float e2;                 // 2 * eps^2
   float fz_half;            // external force z / 2 = -0.5 (fortran/fibers.f95:149)
   float d;                  // -log(eps^2 e)
+  float eps;                // slenderness
   int M, Q;
 };
 

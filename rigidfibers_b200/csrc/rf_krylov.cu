@@ -483,4 +483,239 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   return RF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// BiCGSTAB (van der Vorst 1992) with the semantics of the reference's
+// ViennaCL 1.5.1 solver (lib/viennacl/linalg/bicgstab.hpp:80-166): x0 = 0,
+// two matvecs per iteration, convergence when ||r||/||b|| < tol on the
+// recursive residual, restart from the true residual when rho or omega
+// vanish or every `restart_every` iterations.  FP64 dots and scalars.
+// ---------------------------------------------------------------------------
+struct BicgArgs {
+  const float* ypart;
+  int nsplit;
+  const float* b;
+  float* x;
+  float* r;
+  float* r0;
+  float* p;
+  float* v;
+  float* sv;
+  float* t;
+  int64_t R;
+  double* part;
+  int stride;
+  BicgCtl* ctl;
+};
+
+// a.b and c.d partial dots of this block into part[blk*stride + slot], slot+1
+__device__ void grid_partial_dot2(const float* __restrict__ a, const float* __restrict__ b,
+                                  const float* __restrict__ c, const float* __restrict__ d, int64_t R,
+                                  double* __restrict__ part, int stride, int slot) {
+  double acc[2] = {0.0, 0.0};
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
+    acc[0] = fma((double)a[r], (double)b[r], acc[0]);
+    acc[1] = fma((double)c[r], (double)d[r], acc[1]);
+  }
+  __shared__ double tmp[2];
+  block_reduce_store<2>(acc, tmp);
+  if (threadIdx.x < 2) part[(int64_t)blockIdx.x * stride + slot + threadIdx.x] = tmp[threadIdx.x];
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool bicg_stopped(const BicgCtl* c) {
+  return c->converged || c->nan || c->need_restart || c->iters >= c->maxit;
+}
+
+// ||b||, x = 0, r = r0 = p = b, rho = ||b||^2
+__global__ void k_bicg_init(BicgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
+    const float bv = a.b[r];
+    a.x[r] = 0.f;
+    a.r[r] = bv;
+    a.r0[r] = bv;
+    a.p[r] = bv;
+  }
+  grid_partial_norm(a.b, a.R, a.part, a.stride, 0);
+  grid.sync();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double bb = sum_parts(a.part, gridDim.x, a.stride, 0);
+    BicgCtl* c = a.ctl;
+    c->bnorm = sqrt(bb);
+    c->rho = bb;
+    c->rnorm = sqrt(bb);
+    c->iters = 0;
+    c->last_restart = 0;
+    c->converged = bb == 0.0 ? 1 : 0;
+    c->nan = isfinite(bb) ? 0 : 1;
+    c->need_restart = 0;
+    c->restarts = 0;
+  }
+}
+
+// after the matvec of x: r = b - A x, r0 = p = r, rho = ||r||^2
+__global__ void k_bicg_restart(BicgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  if (a.ctl->converged || a.ctl->nan || !a.ctl->need_restart) return;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
+    const float rv = a.b[r] - sum_splits(a.ypart, a.nsplit, a.R, r);
+    a.r[r] = rv;
+    a.r0[r] = rv;
+    a.p[r] = rv;
+  }
+  grid_partial_norm(a.r, a.R, a.part, a.stride, 0);
+  grid.sync();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double rr = sum_parts(a.part, gridDim.x, a.stride, 0);
+    a.ctl->rho = rr;
+    a.ctl->need_restart = 0;
+    a.ctl->last_restart = a.ctl->iters;
+    a.ctl->restarts += 1;
+    if (!isfinite(rr)) a.ctl->nan = 1;
+  }
+}
+
+// after v = A p: alpha = rho / (v . r0), s = r - alpha v
+__global__ void k_bicg_step1(BicgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  if (bicg_stopped(a.ctl)) return;
+  const double rho = a.ctl->rho;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
+    a.v[r] = sum_splits(a.ypart, a.nsplit, a.R, r);
+  grid_partial_dot2(a.v, a.r0, a.v, a.v, a.R, a.part, a.stride, 0);
+  grid.sync();
+  const double vr0 = sum_parts(a.part, gridDim.x, a.stride, 0);
+  const double alpha = rho / vr0;
+  const float af = (float)alpha;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
+    a.sv[r] = a.r[r] - af * a.v[r];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ctl->alpha = alpha;
+    if (!isfinite(alpha)) a.ctl->nan = 1;
+  }
+}
+
+// after t = A s: omega = (t.s)/(t.t), x += alpha p + omega s, r = s - omega t,
+// rho' = r.r0, ||r||; convergence; beta; p = r + beta (p - omega v)
+__global__ void k_bicg_step2(BicgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  if (bicg_stopped(a.ctl)) return;
+  // every block reads the control block before the first grid sync; block 0
+  // updates it only after the last one
+  BicgCtl* c = a.ctl;
+  const double rho = c->rho, alpha = c->alpha, bnorm = c->bnorm, tol = c->tol;
+  const int it = c->iters + 1, last_restart = c->last_restart, restart_every = c->restart_every;
+  double* p0 = a.part;
+  double* p1 = a.part + (int64_t)gridDim.x * a.stride;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
+    a.t[r] = sum_splits(a.ypart, a.nsplit, a.R, r);
+  grid_partial_dot2(a.t, a.sv, a.t, a.t, a.R, p0, a.stride, 0);
+  grid.sync();
+  const double ts = sum_parts(p0, gridDim.x, a.stride, 0);
+  const double tt = sum_parts(p0, gridDim.x, a.stride, 1);
+  const double omega = tt > 0.0 ? ts / tt : 0.0;
+  const float af = (float)alpha, of = (float)omega;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
+    a.x[r] = a.x[r] + af * a.p[r] + of * a.sv[r];
+    a.r[r] = a.sv[r] - of * a.t[r];
+  }
+  grid_partial_dot2(a.r, a.r0, a.r, a.r, a.R, p1, a.stride, 0);
+  grid.sync();
+  const double rho_new = sum_parts(p1, gridDim.x, a.stride, 0);
+  const double rnorm = sqrt(sum_parts(p1, gridDim.x, a.stride, 1));
+  const bool conv = rnorm / bnorm < tol;
+  const double beta = (rho_new / rho) * (alpha / omega);
+  const bool restart = !conv && (rho_new == 0.0 || omega == 0.0 || (it - 1) - last_restart > restart_every);
+  if (!conv && !restart) {
+    const float bf = (float)beta;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x)
+      a.p[r] = a.r[r] + bf * (a.p[r] - of * a.v[r]);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->iters = it;
+    c->rnorm = rnorm;
+    c->rho = rho_new;
+    if (conv) c->converged = 1;
+    if (restart) c->need_restart = 1;
+    if (!isfinite(rnorm)) c->nan = 1;
+  }
+}
+
+__global__ void k_bicg_stopword(BicgCtl* c) {
+  c->stop_word = (c->converged || c->nan || c->need_restart || c->iters >= c->maxit) ? 1 : 0;
+}
+
+int bicgstab_solve(const BicgSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
+                   BicgResult* res) {
+  BicgArgs a;
+  a.ypart = s.ypart;
+  a.nsplit = s.nsplit;
+  a.b = b;
+  a.x = x;
+  a.r = s.work;
+  a.r0 = s.work + s.ldv;
+  a.p = s.work + 2 * s.ldv;
+  a.v = s.work + 3 * s.ldv;
+  a.sv = s.work + 4 * s.ldv;
+  a.t = s.work + 5 * s.ldv;
+  a.R = s.R;
+  a.part = s.part;
+  a.stride = kMaxRestart + 2;
+  a.ctl = s.ctl;
+  const int nblk = s.coop_blocks;
+  BicgCtl init{};
+  init.tol = s.tol;
+  init.maxit = s.maxit;
+  init.restart_every = s.restart_every;
+  RF_CUDA_TRY(cudaMemcpyAsync(s.ctl, &init, sizeof(BicgCtl), cudaMemcpyHostToDevice, st));
+  {
+    void* args[] = {&a};
+    int rc = coop_launch((const void*)k_bicg_init, nblk, 256, args, st);
+    if (rc) return rc;
+  }
+  res->launches = 1;
+  res->matvecs = 0;
+  BicgCtl h{};
+  const int chunk = 10;   // iterations between host checks
+  for (int guard = 0; guard < s.maxit + 4 * (s.maxit / std::max(1, s.restart_every) + 2); ++guard) {
+    for (int k = 0; k < chunk; ++k) {
+      int rc = matvec(a.p, (const int*)&s.ctl->stop_word, st);
+      if (rc) return rc;
+      void* args[] = {&a};
+      rc = coop_launch((const void*)k_bicg_step1, nblk, 256, args, st);
+      if (rc) return rc;
+      rc = matvec(a.sv, (const int*)&s.ctl->stop_word, st);
+      if (rc) return rc;
+      rc = coop_launch((const void*)k_bicg_step2, nblk, 256, args, st);
+      if (rc) return rc;
+      // the matvec kernels read one word: fold the stop conditions into it
+      k_bicg_stopword<<<1, 1, 0, st>>>(s.ctl);
+      RF_LAUNCH_CHECK();
+      res->launches += 5;
+    }
+    RF_CUDA_TRY(cudaMemcpyAsync(s.host_ctl, s.ctl, sizeof(BicgCtl), cudaMemcpyDeviceToHost, st));
+    RF_CUDA_TRY(cudaStreamSynchronize(st));
+    h = *s.host_ctl;
+    if (h.converged || h.nan || h.iters >= s.maxit) break;
+    if (h.need_restart) {
+      int rc = matvec(x, nullptr, st);
+      if (rc) return rc;
+      void* args[] = {&a};
+      rc = coop_launch((const void*)k_bicg_restart, nblk, 256, args, st);
+      if (rc) return rc;
+      k_bicg_stopword<<<1, 1, 0, st>>>(s.ctl);
+      RF_LAUNCH_CHECK();
+      res->launches += 2;
+      ++res->matvecs;
+    }
+  }
+  res->iterations = h.iters;
+  res->restarts = h.restarts;
+  res->matvecs += 2 * h.iters;
+  res->relative_residual = h.bnorm > 0 ? h.rnorm / h.bnorm : 0.0;
+  if (h.nan) return RF_E_NAN;
+  if (!h.converged) return RF_E_NOCONV;
+  return RF_OK;
+}
+
 }  // namespace rf

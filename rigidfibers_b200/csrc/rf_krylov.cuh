@@ -67,6 +67,51 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
 int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b, void* x,
                    bool x_double, cudaStream_t st, GmresResult* res);
 
+// BiCGSTAB control block (device); stop_word is what the matvec kernels read.
+struct BicgCtl {
+  int stop_word;
+  int converged;
+  int nan;
+  int need_restart;
+  int iters;
+  int maxit;
+  int last_restart;
+  int restart_every;
+  int restarts;
+  int pad;
+  double tol;
+  double bnorm;
+  double rho;
+  double alpha;
+  double rnorm;
+};
+
+struct BicgSetup {
+  int64_t R;
+  int maxit;
+  int restart_every;   // iterations before a restart from the true residual (ViennaCL: 200)
+  double tol;
+  float* work;         // 6 x ldv floats: r, r0, p, v, s, t
+  int64_t ldv;
+  const float* ypart;
+  int nsplit;
+  double* part;        // 2 * coop_blocks * (kMaxRestart + 2)
+  BicgCtl* ctl;
+  BicgCtl* host_ctl;
+  int coop_blocks;
+};
+
+struct BicgResult {
+  int iterations = 0;
+  int restarts = 0;
+  int matvecs = 0;
+  int launches = 0;
+  double relative_residual = 0.0;
+};
+
+int bicgstab_solve(const BicgSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
+                   BicgResult* res);
+
 struct DenseGemvPlan {
   int row_blocks;
   int splits;

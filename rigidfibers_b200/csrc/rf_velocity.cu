@@ -11,8 +11,11 @@
 // fixed-order sum; no atomics.
 #include "rf_common.cuh"
 #include "rf_kernels.cuh"
+#include "rf_analytic.cuh"
 
 namespace rf {
+
+int velocity_chunks(int N);
 
 // fw[j*Q + q] = w_q f_j(s_q) = W[0][q] F/2 + sum_k a_{j,k} W[k+1][q]
 __global__ void k_source_density(const Tables tab, int N, const float* __restrict__ x, float4* __restrict__ fw) {
@@ -127,6 +130,90 @@ __global__ void k_velocity_finalize(const Tables tab, int N, const float4* __res
   const float su = 0.5f / d, sr = 1.5f / d;
   tvel[i] = make_float4(U[0] * su, U[1] * su, U[2] * su, 0.f);
   rvel[i] = make_float4((W[0] - t.x * tW) * sr, (W[1] - t.y * tW) * sr, (W[2] - t.z * tW) * sr, 0.f);
+}
+
+// Analytical variant: the inner integral over fiber j in closed form (FP64),
+// GF_ij(qi) = G_0(qi) F/2 + sum_k G_{k+1}(qi) a_{j,k}; the outer quadrature
+// over fiber i as in the numerical kernel.  This is how the reference's
+// 100_analytic_* golden files were produced (its committed
+// fortran/update_velocities.incl integrates numerically in both modes).
+template <int M, int Q>
+__global__ void __launch_bounds__(192, 2)
+k_velocity_analytical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+                      const float* __restrict__ coeff, int jchunk, float* __restrict__ vpart) {
+  constexpr int TI = 192 / Q;
+  constexpr int U = TI * Q;
+  constexpr int M3 = 3 * M;
+  __shared__ float sGs[3][U];
+  const int tid = threadIdx.x;
+  const int il = tid / Q, qi = tid % Q;
+  const int i0 = blockIdx.x * TI;
+  const int i = i0 + il;
+  const bool unit_ok = tid < U && i < N;
+  const double e2 = 2.0 * (double)tab.eps * (double)tab.eps;
+  const float fz = tab.fz_half;
+  float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+  const int jbeg = blockIdx.y * jchunk, jend = min(N, jbeg + jchunk);
+  if (unit_ok) {
+    const float4 xi4 = pos[i], ti4 = ori[i];
+    const double s = (double)tab.pts[qi];
+    for (int j = jbeg; j < jend; ++j) {
+      if (j == i) continue;
+      const float4 xj4 = pos[j], tj4 = ori[j];
+      const double R0[3] = {(double)xi4.x + s * (double)ti4.x - (double)xj4.x,
+                            (double)xi4.y + s * (double)ti4.y - (double)xj4.y,
+                            (double)xi4.z + s * (double)ti4.z - (double)xj4.z};
+      const double tj[3] = {(double)tj4.x, (double)tj4.y, (double)tj4.z};
+      float G[6][M + 1];
+      analytic_G<M>(R0, tj, e2, G);
+      // F/2 = (0, 0, fz): column z of G_0
+      float f0 = G[4][0] * fz, f1 = G[5][0] * fz, f2 = G[2][0] * fz;
+      const float* a = coeff + (int64_t)j * M3;
+#pragma unroll
+      for (int k = 0; k < M; ++k) {
+        const float a0 = a[3 * k], a1 = a[3 * k + 1], a2 = a[3 * k + 2];
+        f0 += G[0][k + 1] * a0 + G[3][k + 1] * a1 + G[4][k + 1] * a2;
+        f1 += G[3][k + 1] * a0 + G[1][k + 1] * a1 + G[5][k + 1] * a2;
+        f2 += G[4][k + 1] * a0 + G[5][k + 1] * a1 + G[2][k + 1] * a2;
+      }
+      g0 += f0; g1 += f1; g2 += f2;
+    }
+  }
+  if (tid < U) { sGs[0][tid] = g0; sGs[1][tid] = g1; sGs[2][tid] = g2; }
+  __syncthreads();
+  if (tid < TI * 6) {
+    const int fl = tid / 6, comp = tid % 6;
+    const int a = comp % 3;
+    const bool rot = comp >= 3;
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) acc = fmaf(rot ? tab.W[1][q] : tab.W[0][q], sGs[a][fl * Q + q], acc);
+    if (i0 + fl < N) vpart[((int64_t)blockIdx.y * N + i0 + fl) * 6 + comp] = acc;
+  }
+}
+
+int launch_velocity_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
+                               float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
+  const int chunks = velocity_chunks(N);
+  const int jchunk = (int)ceil_div(N, chunks);
+  const int TI = 192 / tab.Q;
+  dim3 grid((unsigned)ceil_div(N, TI), (unsigned)chunks);
+  bool done = false;
+#define RF_VA_CASE(MM, QQ)                                                                   \
+  if (!done && tab.M == MM && tab.Q == QQ) {                                                 \
+    k_velocity_analytical<MM, QQ><<<grid, 192, 0, st>>>(tab, N, pos, ori, x, jchunk, vpart); \
+    done = true;                                                                             \
+  }
+  RF_FOR_EACH_MQ(RF_VA_CASE)
+#undef RF_VA_CASE
+  if (!done) {
+    set_last_error_str("velocity: (M, Q) combination not instantiated");
+    return RF_E_UNSUPPORTED;
+  }
+  RF_LAUNCH_CHECK();
+  k_velocity_finalize<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(tab, N, ori, vpart, chunks, tvel, rvel);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
 }
 
 int velocity_chunks(int N) {
