@@ -80,6 +80,10 @@ struct AsmOut {
   uint32_t* S16;
   // both: partial force terms ffpart[X][i][k][3]
   float* ffpart;
+  // analytical: the FP64 fiber state (the closed-form integral is ~7x more
+  // sensitive to the rounding of its inputs than the quadrature)
+  const double4* pos64;
+  const double4* ori64;
 };
 
 template <int M, int Q, int MODE, int INTEG>
@@ -171,13 +175,11 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
 #pragma unroll
       for (int k = 0; k < K1; ++k) g[c][k] = 0.f;
     if (!SYM && pair_ok) {
-      const float4 xi4 = pos[i], ti4 = ori[i];
-      const float4 xj4 = pos[j0 + jl], tj4 = sTj[jl];
+      const double4 xi4 = out.pos64[i], ti4 = out.ori64[i];
+      const double4 xj4 = out.pos64[j0 + jl], tj4 = out.ori64[j0 + jl];
       const double s = (double)tab.pts[qi];
-      const double R0[3] = {(double)xi4.x + s * (double)ti4.x - (double)xj4.x,
-                            (double)xi4.y + s * (double)ti4.y - (double)xj4.y,
-                            (double)xi4.z + s * (double)ti4.z - (double)xj4.z};
-      const double tj[3] = {(double)tj4.x, (double)tj4.y, (double)tj4.z};
+      const double R0[3] = {xi4.x + s * ti4.x - xj4.x, xi4.y + s * ti4.y - xj4.y, xi4.z + s * ti4.z - xj4.z};
+      const double tj[3] = {tj4.x, tj4.y, tj4.z};
       analytic_G<M>(R0, tj, 2.0 * (double)tab.eps * (double)tab.eps, g);
     }
     if (SYM && pair_ok) {
@@ -475,9 +477,12 @@ int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const
   return dispatch_assemble<kAsmDense, kNumerical>(tab, N, pos, ori, out, F, b, st);
 }
 
-int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                               int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
+int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
+                               const double4* pos64, const double4* ori64, float* A, int64_t lda, float* ffpart,
+                               float* F, float* b, cudaStream_t st) {
   AsmOut out{};
+  out.pos64 = pos64;
+  out.ori64 = ori64;
   out.A = A;
   out.lda = lda;
   out.ffpart = ffpart;

@@ -420,7 +420,8 @@ int rf_assemble(rf_handle* h) {
     RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->S32, h->S16,
                                       h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st));
   else if (h->cfg.integration == RF_ANALYTICAL)
-    RF_TRY(launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
+    RF_TRY(launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
+                                      h->lda, h->ffpart, h->F, h->b, h->st));
   else
     RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
   h->launches += 2;
@@ -543,8 +544,8 @@ int rf_update_velocities(rf_handle* h) {
   RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
   const int vint = h->cfg.velocity_integration < 0 ? h->cfg.integration : h->cfg.velocity_integration;
   if (vint == RF_ANALYTICAL) {
-    RF_TRY(launch_velocity_analytical(h->tab, h->N, h->pos32, h->ori32, h->x, h->vpart, h->tv[h->vcur],
-                                      h->rv[h->vcur], h->st));
+    RF_TRY(launch_velocity_analytical(h->tab, h->N, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->x,
+                                      h->vpart, h->tv[h->vcur], h->rv[h->vcur], h->st));
     h->launches += 2;
   } else if (h->mixed) {
     RF_TRY(launch_struct_velocity(h->tab, h->N, h->S32, h->ori32, h->F, h->x, h->svpart, h->tv[h->vcur],

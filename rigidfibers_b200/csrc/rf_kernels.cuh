@@ -22,8 +22,9 @@ int assemble_tiles(int M, int Q, int N);
 int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
                               int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
 // Analytical integration (closed-form inner integral in FP64), dense A.
-int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                               int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
+int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
+                               const double4* pos64, const double4* ori64, float* A, int64_t lda, float* ffpart,
+                               float* F, float* b, cudaStream_t st);
 // Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
                                uint32_t* S16, bool bf16, float* ffpart, float* F, float* b, cudaStream_t st);
@@ -56,8 +57,9 @@ int velocity_chunks(int N);
 int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
                               float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 // analytical inner integrals (FP64 moments); vpart as for the numerical kernel
-int launch_velocity_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
-                               float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
+int launch_velocity_analytical(const Tables& tab, int N, const float4* ori, const double4* pos64,
+                               const double4* ori64, const float* x, float* vpart, float4* tvel, float4* rvel,
+                               cudaStream_t st);
 int launch_update_fibers(int N, int first, double dt, const double4* pp, const double4* cp, const double4* po,
                          const double4* co, const float4* ptv, const float4* ctv, const float4* prv,
                          const float4* crv, double4* np, double4* no, float4* pos32, float4* ori32,

@@ -139,7 +139,7 @@ __global__ void k_velocity_finalize(const Tables tab, int N, const float4* __res
 // fortran/update_velocities.incl integrates numerically in both modes).
 template <int M, int Q>
 __global__ void __launch_bounds__(192, 2)
-k_velocity_analytical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+k_velocity_analytical(const Tables tab, int N, const double4* __restrict__ pos, const double4* __restrict__ ori,
                       const float* __restrict__ coeff, int jchunk, float* __restrict__ vpart) {
   constexpr int TI = 192 / Q;
   constexpr int U = TI * Q;
@@ -155,15 +155,13 @@ k_velocity_analytical(const Tables tab, int N, const float4* __restrict__ pos, c
   float g0 = 0.f, g1 = 0.f, g2 = 0.f;
   const int jbeg = blockIdx.y * jchunk, jend = min(N, jbeg + jchunk);
   if (unit_ok) {
-    const float4 xi4 = pos[i], ti4 = ori[i];
+    const double4 xi4 = pos[i], ti4 = ori[i];
     const double s = (double)tab.pts[qi];
     for (int j = jbeg; j < jend; ++j) {
       if (j == i) continue;
-      const float4 xj4 = pos[j], tj4 = ori[j];
-      const double R0[3] = {(double)xi4.x + s * (double)ti4.x - (double)xj4.x,
-                            (double)xi4.y + s * (double)ti4.y - (double)xj4.y,
-                            (double)xi4.z + s * (double)ti4.z - (double)xj4.z};
-      const double tj[3] = {(double)tj4.x, (double)tj4.y, (double)tj4.z};
+      const double4 xj4 = pos[j], tj4 = ori[j];
+      const double R0[3] = {xi4.x + s * ti4.x - xj4.x, xi4.y + s * ti4.y - xj4.y, xi4.z + s * ti4.z - xj4.z};
+      const double tj[3] = {tj4.x, tj4.y, tj4.z};
       float G[6][M + 1];
       analytic_G<M>(R0, tj, e2, G);
       // F/2 = (0, 0, fz): column z of G_0
@@ -192,8 +190,9 @@ k_velocity_analytical(const Tables tab, int N, const float4* __restrict__ pos, c
   }
 }
 
-int launch_velocity_analytical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
-                               float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
+int launch_velocity_analytical(const Tables& tab, int N, const float4* ori, const double4* pos64,
+                               const double4* ori64, const float* x, float* vpart, float4* tvel, float4* rvel,
+                               cudaStream_t st) {
   const int chunks = velocity_chunks(N);
   const int jchunk = (int)ceil_div(N, chunks);
   const int TI = 192 / tab.Q;
@@ -201,7 +200,7 @@ int launch_velocity_analytical(const Tables& tab, int N, const float4* pos, cons
   bool done = false;
 #define RF_VA_CASE(MM, QQ)                                                                   \
   if (!done && tab.M == MM && tab.Q == QQ) {                                                 \
-    k_velocity_analytical<MM, QQ><<<grid, 192, 0, st>>>(tab, N, pos, ori, x, jchunk, vpart); \
+    k_velocity_analytical<MM, QQ><<<grid, 192, 0, st>>>(tab, N, pos64, ori64, x, jchunk, vpart); \
     done = true;                                                                             \
   }
   RF_FOR_EACH_MQ(RF_VA_CASE)
