@@ -1,5 +1,15 @@
 """Seeded synthetic fiber layouts.
 
+`grown_sphere_layout`: the concentration-controlled scenes of the reference's
+benchmark mode (tools/gen2.f95, called by runner/cuda_runner.py:253): fibers
+(segments of length 2) are placed one by one in the outer shell
+[r - 4 d, r] of a sphere whose radius r starts at d and grows by d whenever
+1000 consecutive candidates are rejected; a candidate is rejected when its
+segment-segment distance to any placed fiber is below d.  Orientations are a
+uniform sample of the cube [-1,1]^3, normalised.  Written from the published
+closest-point-between-segments construction (D. Sunday), vectorised over the
+placed fibers.
+
 `sphere_layout`: centres uniform in a ball of radius `radius` (cube rejection),
 rejecting any centre closer than `min_distance` to an accepted one;
 orientations uniform on the unit sphere (normalised standard normal).  This
@@ -59,3 +69,125 @@ def sphere_layout(n, radius, min_distance=0.2, seed=0, max_tries=200):
 
 def serving_radius(n, phi=0.01):
     return (n / phi) ** (1.0 / 3.0)
+
+
+def segment_distances2(p, o, P, O):
+    """Squared distances between segments [p_b - o_b, p_b + o_b] (B of them,
+    or one) and [P_k - O_k, P_k + O_k] (K of them): a (B, K) array (or (K,))."""
+    single = np.ndim(p) == 1
+    p = np.atleast_2d(p)[:, None, :]
+    o = np.atleast_2d(o)[:, None, :]
+    P = np.asarray(P)[None, :, :]
+    O = np.asarray(O)[None, :, :]
+    u = 2.0 * o
+    v = 2.0 * O
+    w = (p - o) - (P - O)
+    a = np.sum(u * u, -1)
+    b = np.sum(u * v, -1)
+    c = np.sum(v * v, -1)
+    d = np.sum(u * w, -1)
+    e = np.sum(v * w, -1)
+    a = np.broadcast_to(a, b.shape)
+    den = a * c - b * b
+    small = den < 1e-5
+    sN = np.where(small, 0.0, b * e - c * d)
+    sD = np.where(small, 1.0, den)
+    tN = np.where(small, e, a * e - b * d)
+    tD = np.where(small, c, den)
+    lo = (~small) & (sN < 0.0)
+    hi = (~small) & (sN > sD)
+    sN = np.where(lo, 0.0, np.where(hi, sD, sN))
+    tN = np.where(lo, e, np.where(hi, e + b, tN))
+    tD = np.where(lo | hi, c, tD)
+    tlo = tN < 0.0
+    thi = tN > tD
+    tN = np.where(tlo, 0.0, np.where(thi, tD, tN))
+    s_lo_val = -d
+    s_hi_val = -d + b
+    sN = np.where(tlo, np.where(s_lo_val < 0.0, 0.0, np.where(s_lo_val > a, sD, s_lo_val)), sN)
+    sD = np.where(tlo & (s_lo_val >= 0.0) & (s_lo_val <= a), a, sD)
+    sN = np.where(thi, np.where(s_hi_val < 0.0, 0.0, np.where(s_hi_val > a, sD, s_hi_val)), sN)
+    sD = np.where(thi & (s_hi_val >= 0.0) & (s_hi_val <= a), a, sD)
+    sc = np.where(np.abs(sN) < 1e-5, 0.0, sN / sD)
+    tc = np.where(np.abs(tN) < 1e-5, 0.0, tN / tD)
+    dP = w + sc[..., None] * u - tc[..., None] * v
+    out = np.sum(dP * dP, -1)
+    return out[0] if single else out
+
+
+def segment_distances2_pairs(p, o, P, O):
+    """Squared distances between segments p_k +- o_k and P_k +- O_k, pairwise (K,)."""
+    u = 2.0 * o
+    v = 2.0 * O
+    w = (p - o) - (P - O)
+    a = np.sum(u * u, -1)
+    b = np.sum(u * v, -1)
+    c = np.sum(v * v, -1)
+    d = np.sum(u * w, -1)
+    e = np.sum(v * w, -1)
+    den = a * c - b * b
+    small = den < 1e-5
+    sN = np.where(small, 0.0, b * e - c * d)
+    sD = np.where(small, 1.0, den)
+    tN = np.where(small, e, a * e - b * d)
+    tD = np.where(small, c, den)
+    lo = (~small) & (sN < 0.0)
+    hi = (~small) & (sN > sD)
+    sN = np.where(lo, 0.0, np.where(hi, sD, sN))
+    tN = np.where(lo, e, np.where(hi, e + b, tN))
+    tD = np.where(lo | hi, c, tD)
+    tlo = tN < 0.0
+    thi = tN > tD
+    tN = np.where(tlo, 0.0, np.where(thi, tD, tN))
+    s_lo_val = -d
+    s_hi_val = -d + b
+    sN = np.where(tlo, np.where(s_lo_val < 0.0, 0.0, np.where(s_lo_val > a, sD, s_lo_val)), sN)
+    sD = np.where(tlo & (s_lo_val >= 0.0) & (s_lo_val <= a), a, sD)
+    sN = np.where(thi, np.where(s_hi_val < 0.0, 0.0, np.where(s_hi_val > a, sD, s_hi_val)), sN)
+    sD = np.where(thi & (s_hi_val >= 0.0) & (s_hi_val <= a), a, sD)
+    sc = np.where(np.abs(sN) < 1e-5, 0.0, sN / sD)
+    tc = np.where(np.abs(tN) < 1e-5, 0.0, tN / tD)
+    dP = w + sc[:, None] * u - tc[:, None] * v
+    return np.sum(dP * dP, -1)
+
+
+def grown_sphere_layout(n, min_distance=0.2, seed=0, max_retries=1000, batch=64):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pos = np.empty((n, 3))
+    ori = np.empty((n, 3))
+    radius = min_distance
+    d2 = min_distance * min_distance
+    for i in range(n):
+        while True:
+            placed = False
+            tries = 0
+            while tries < max_retries:
+                rmin = max(0.0, radius - 4.0 * min_distance)
+                c = rng.uniform(-radius, radius, (4 * batch, 3))
+                r2 = np.einsum("ij,ij->i", c, c)
+                c = c[(r2 > rmin * rmin) & (r2 < radius * radius)][:batch]
+                if len(c) == 0:
+                    continue
+                t = rng.uniform(-1.0, 1.0, (len(c), 3))
+                t /= np.linalg.norm(t, axis=1, keepdims=True)
+                ok = np.ones(len(c), bool)
+                if i > 0:
+                    # only fibers whose centres are closer than 2 + d can come
+                    # within d of the candidate (segments of half-length 1)
+                    dc = c[:, None, :] - pos[None, :i, :]
+                    bi, kj = np.nonzero(np.einsum("bkj,bkj->bk", dc, dc) < (2.0 + min_distance) ** 2)
+                    if len(bi):
+                        dd = segment_distances2_pairs(c[bi], t[bi], pos[kj], ori[kj])
+                        bad = bi[dd < d2]
+                        ok[bad] = False
+                k = np.flatnonzero(ok)
+                take = min(len(c), max_retries - tries)
+                if len(k) and k[0] < take:
+                    pos[i], ori[i] = c[k[0]], t[k[0]]
+                    placed = True
+                    break
+                tries += take
+            if placed:
+                break
+            radius += min_distance
+    return pos, ori
