@@ -171,6 +171,12 @@ int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
  * ViennaCL prod(A, x) behind the reference's GMRES
  * (lib/viennacl/linalg/cuda/matrix_operations_col.hpp:1251-1278). */
 int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream);
+/* rf_dense_lu_solve: x = A^{-1} b for column-major FP32 A (R x R) by LU with
+ * partial pivoting and FP64-residual refinement until ||b - A x|| / ||b|| <=
+ * tol (RF_E_NOCONV after 20 steps, RF_E_SINGULAR on a zero pivot); A and b
+ * are not modified.  Replaces MAGMA's magma_sgesv_gpu behind the reference's
+ * --magma path (src/simulation.cu:403-418). */
+int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, double tol, void* stream);
 /* rf_dense_matvec_noalloc: the same y = A x, for callers that cannot let a
  * library allocate device memory (a host program whose pool allocator owns all
  * of HBM, or a loop that cannot afford cudaMalloc's latency).  It has no

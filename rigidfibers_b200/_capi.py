@@ -80,6 +80,7 @@ SIGNATURES = {
     "rf_get_config": (ctypes.c_int, [_H, ctypes.POINTER(rf_config)]),
     "rf_number_of_fibers": (ctypes.c_int, [_H]),
     "rf_dense_matvec": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
+    "rf_dense_lu_solve": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_double, _P]),
     "rf_dense_matvec_noalloc": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "rf_operator_apply": (ctypes.c_int, [_H, _P, _P, ctypes.c_int]),
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),

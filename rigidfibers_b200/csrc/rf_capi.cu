@@ -12,6 +12,7 @@
 #include "rf_common.cuh"
 #include "rf_kernels.cuh"
 #include "rf_krylov.cuh"
+#include "rf_lu.cuh"
 
 namespace rf {
 
@@ -146,6 +147,7 @@ struct rf_handle {
   double* g = nullptr;
   GmresCtl* ctl = nullptr;
   GmresCtl* host_ctl = nullptr;
+  LuSetup lu{};                   // direct solver workspace
   float* bicg_work = nullptr;     // BiCGSTAB vectors r, r0, p, v, s, t
   BicgCtl* bctl = nullptr;
   BicgCtl* host_bctl = nullptr;
@@ -184,6 +186,8 @@ struct rf_handle {
     for (void* p : allocations) cudaFree(p);
     if (host_ctl) cudaFreeHost(host_ctl);
     if (host_bctl) cudaFreeHost(host_bctl);
+    if (lu.host_ipiv) cudaFreeHost(lu.host_ipiv);
+    if (lu.host_perm) cudaFreeHost(lu.host_perm);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -230,7 +234,6 @@ static int validate_config(const rf_config* c, int N) {
   if (c->velocity_integration < -1 || c->velocity_integration > 1) {
     set_last_error_str("velocity_integration must be -1, 0 or 1"); return RF_E_INPUT;
   }
-  if (c->solver == RF_SOLVER_DIRECT) { set_last_error_str("direct solver not built yet"); return RF_E_UNSUPPORTED; }
   if (c->solver == RF_SOLVER_BICGSTAB && (c->bicgstab_max_iterations < 1 || !(c->bicgstab_tolerance > 0.0))) {
     set_last_error_str("bicgstab_max_iterations / bicgstab_tolerance"); return RF_E_INPUT;
   }
@@ -384,6 +387,26 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (!rc) rc = h->alloc((void**)&h->g, (size_t)(m + 1) * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->ctl, sizeof(GmresCtl));
   if (!rc && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
+  if (cfg->solver == RF_SOLVER_DIRECT) {
+    LuSetup& L = h->lu;
+    L.R = R;
+    L.lda = h->lda;
+    L.tol = cfg->refinement_tolerance;
+    L.max_refine = cfg->refinement_max_iterations;
+    L.coop_blocks = h->coop_blocks;
+    if (!rc) rc = h->alloc((void**)&L.LU, (size_t)h->lda * (size_t)R * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.ipiv, (size_t)R * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.perm, (size_t)R * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.pmax, (size_t)h->coop_blocks * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.pidx, (size_t)h->coop_blocks * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.info, sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.d, (size_t)R * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.x64, (size_t)R * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&L.r64, (size_t)R * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&L.norms, 2 * sizeof(double));
+    if (!rc && cudaMallocHost((void**)&L.host_ipiv, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && cudaMallocHost((void**)&L.host_perm, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
+  }
   if (cfg->solver == RF_SOLVER_BICGSTAB) {
     if (!rc) rc = h->alloc((void**)&h->bicg_work, (size_t)6 * (size_t)ldv * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->bctl, sizeof(BicgCtl));
@@ -480,6 +503,20 @@ int rf_solve(rf_handle* h) {
     if (h->profile) RF_CUDA_TRY(cudaEventRecord(e1, st));
     return rc;
   };
+  if (h->cfg.solver == RF_SOLVER_DIRECT) {
+    LuResult lr;
+    const int lrc = lu_factor_solve(h->lu, h->A, h->b, h->x, h->st, &lr);
+    RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
+    h->launches += lr.launches;
+    h->matvecs_done = 0;
+    h->stats.iterations = 0;
+    h->stats.restarts = 0;
+    h->stats.refinement_steps = lr.refinement_steps;
+    h->stats.relative_residual = lr.relative_residual;
+    if (lrc != RF_OK && lrc != RF_E_NOCONV) return lrc;
+    h->solved = true;
+    return lrc;
+  }
   if (h->cfg.solver == RF_SOLVER_BICGSTAB) {
     BicgSetup bs;
     bs.R = h->R;
@@ -730,6 +767,45 @@ int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms) {
   *launches = h->matvecs_done;
   *total_ms = t;
   return RF_OK;
+}
+
+int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, double tol, void* stream) {
+  if (!A || !b || !x || R < 1 || !(tol > 0.0)) { set_last_error_str("rf_dense_lu_solve: bad arguments"); return RF_E_INPUT; }
+  int dev = 0, sms = 148;
+  RF_CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaStream_t st = (cudaStream_t)stream;
+  LuSetup L{};
+  L.R = R;
+  L.lda = R;
+  L.tol = tol;
+  L.max_refine = 20;
+  L.coop_blocks = krylov_coop_blocks(R, sms);
+  std::vector<void*> mem;
+  auto get = [&](void** p, size_t bytes) -> int {
+    cudaError_t e = cudaMallocAsync(p, bytes, st);
+    if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return RF_E_OOM; }
+    mem.push_back(*p);
+    return RF_OK;
+  };
+  int rc = get((void**)&L.LU, (size_t)R * R * sizeof(float));
+  if (!rc) rc = get((void**)&L.ipiv, R * sizeof(int));
+  if (!rc) rc = get((void**)&L.perm, R * sizeof(int));
+  if (!rc) rc = get((void**)&L.pmax, L.coop_blocks * sizeof(float));
+  if (!rc) rc = get((void**)&L.pidx, L.coop_blocks * sizeof(int));
+  if (!rc) rc = get((void**)&L.info, sizeof(int));
+  if (!rc) rc = get((void**)&L.d, R * sizeof(float));
+  if (!rc) rc = get((void**)&L.x64, R * sizeof(double));
+  if (!rc) rc = get((void**)&L.r64, R * sizeof(double));
+  if (!rc) rc = get((void**)&L.norms, 2 * sizeof(double));
+  std::vector<int> hi(R), hp(R);
+  L.host_ipiv = hi.data();
+  L.host_perm = hp.data();
+  LuResult lr;
+  if (!rc) rc = lu_factor_solve(L, A, b, x, st, &lr);
+  for (void* p : mem) cudaFreeAsync(p, st);
+  cudaStreamSynchronize(st);
+  return rc;
 }
 
 int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream) {

@@ -43,6 +43,13 @@ struct Tables {
 
 #define RF_LAUNCH_CHECK() RF_CUDA_TRY(cudaGetLastError())
 
+// propagate a non-zero rf_status
+#define RF_TRY_RF(expr)             \
+  do {                              \
+    int _rc = (expr);               \
+    if (_rc != RF_OK) return _rc;   \
+  } while (0)
+
 void set_last_error(const char* msg, const char* file, int line);
 void set_last_error_str(const char* msg);
 

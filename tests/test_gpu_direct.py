@@ -1,0 +1,87 @@
+"""Direct solver (--magma): blocked LU with partial pivoting + FP64-residual
+refinement, against the reference's direct-solve golden files and LAPACK.
+
+Bounds: golden fields within 1e-5 relative (the golden files are FP64 runs of
+the reference's sgesv path); general matrices within 1e-5 of an FP64 LAPACK
+solve after refinement to ||b - A x|| / ||b|| <= 1e-7.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = [("BVec", "b"), ("XVec", "x"), ("TRANSVel", "tvel"), ("ROTVel", "rvel"), ("POS", "pos"), ("ORIENT", "ori")]
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("integ", ["numeric", "analytic"])
+def test_golden_direct(golden, integ):
+    from rigidfibers_b200 import Config, Simulation
+    sim = Simulation(Config(solver="direct", integration="numerical" if integ == "numeric" else "analytical"),
+                     golden["positions"], golden["orientations"])
+    for t in range(2):
+        sim.assembleSystem()
+        _, b = sim.system(with_matrix=False)
+        sim.solveSystem()
+        x = sim.solution()
+        sim.updateVelocities()
+        tv, rv = sim.velocities()
+        sim.updateFibers(t == 0)
+        p, o = sim.state()
+        got = dict(b=b, x=x, tvel=tv, rvel=rv, pos=p, ori=o)
+        for f, k in FIELDS:
+            ref = golden["%s_direct/%d_%s" % (integ, t, f)]
+            assert _rel(got[k], ref) <= 1e-5, (t, f, _rel(got[k], ref))
+        assert sim.stats()["relative_residual"] <= 1e-6
+
+
+def _lu_solve(A, b, tol=1e-7):
+    import torch
+    from rigidfibers_b200 import _capi as C
+    R = A.shape[0]
+    Ad = torch.from_numpy(np.asfortranarray(A, np.float32).reshape(-1, order="F").copy()).cuda()
+    bd = torch.from_numpy(np.asarray(b, np.float32)).cuda()
+    xd = torch.zeros(R, device="cuda")
+    rc = C.load().rf_dense_lu_solve(ctypes.c_void_p(Ad.data_ptr()), ctypes.c_void_p(bd.data_ptr()),
+                                    ctypes.c_void_p(xd.data_ptr()), R, tol,
+                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return rc, xd.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("R", [1, 5, 64, 100, 131, 300])
+def test_lu_random_matrix_needs_pivoting(R):
+    rng = np.random.default_rng(R)
+    A = rng.standard_normal((R, R)).astype(np.float32)
+    b = rng.standard_normal(R).astype(np.float32)
+    rc, x = _lu_solve(A, b)
+    assert rc == 0
+    ref = np.linalg.solve(A.astype(np.float64), b.astype(np.float64))
+    assert _rel(x, ref) <= 1e-5
+
+
+def test_lu_permutation_matrix():
+    R = 130
+    rng = np.random.default_rng(1)
+    P = np.eye(R, dtype=np.float32)[rng.permutation(R)]
+    b = rng.standard_normal(R).astype(np.float32)
+    rc, x = _lu_solve(P, b)
+    assert rc == 0
+    assert np.abs(x - np.linalg.solve(P.astype(np.float64), b)).max() < 1e-6
+
+
+def test_lu_singular_matrix_reports_error():
+    from rigidfibers_b200 import _capi as C
+    R = 70
+    rng = np.random.default_rng(2)
+    A = rng.standard_normal((R, R)).astype(np.float32)
+    A[:, 33] = 0.0
+    rc, _ = _lu_solve(A, np.ones(R, np.float32))
+    assert rc == C.RF_E_SINGULAR
