@@ -76,6 +76,7 @@ __device__ void block_argmax(float v, int i, float* pmax, int* pidx) {
 __global__ void __launch_bounds__(256) k_lu_panel(PanelArgs a) {
   cg::grid_group grid = cg::this_grid();
   __shared__ int s_piv;
+  __shared__ float s_pabs;
   const int64_t R = a.R, lda = a.lda, k = a.k;
   const int nb = a.nb;
   float* A = a.A;
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(256) k_lu_panel(PanelArgs a) {
       int bi = INT_MAX;
       for (int b = 0; b < (int)gridDim.x; ++b) better(bv, bi, a.pmax[b], a.pidx[b]);
       s_piv = bi;
+      s_pabs = bv;
     }
     __syncthreads();
     const int64_t p = s_piv;
@@ -110,7 +112,8 @@ __global__ void __launch_bounds__(256) k_lu_panel(PanelArgs a) {
       }
       if (threadIdx.x == 0) {
         a.ipiv[j] = (int)p;
-        if (A[p + j * lda] == 0.f && *a.info == 0) *a.info = (int)(j + 1);
+        // the largest |a_ij| of the column is the pivot's magnitude
+        if (!(s_pabs > 0.f) && *a.info == 0) *a.info = (int)(j + 1);
       }
     }
     grid.sync();
