@@ -189,6 +189,60 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
  * threads on the same device) race and must be serialised by the caller. */
 int rf_dense_matvec_noalloc(const float* A, const float* x, float* y, int64_t R, void* stream);
 
+/* ---- Serving: an ensemble of independent suspensions ------------------------
+ * The reference runs one suspension per process (fibers_runner.py:17-162 starts
+ * one `fibers` binary per configuration).  The server below runs many at once
+ * on one GPU: requests are admitted in arrival order while a slot is free and
+ * their device memory (rf_device_bytes_estimate) fits hbm_budget_bytes; each
+ * runs on its own handle and stream, so requests overlap on the device, and its
+ * result equals that of a lone rf_create + rf_step loop on the same inputs. */
+enum rf_request_status { RF_REQ_QUEUED = 0, RF_REQ_RUNNING = 1, RF_REQ_DONE = 2, RF_REQ_FAILED = 3, RF_REQ_CANCELLED = 4 };
+
+typedef struct rf_server rf_server;
+
+typedef struct rf_server_config {
+  int max_active;            /* requests running at once */
+  int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
+} rf_server_config;
+
+typedef struct rf_request_stats {
+  int steps_done;
+  double queue_ms;      /* submit -> admission */
+  double run_ms;        /* admission -> last step done */
+  double mean_step_ms;  /* host wall time of rf_step, mean */
+  int64_t device_bytes; /* admission estimate */
+} rf_request_stats;
+
+typedef struct rf_server_stats {
+  int64_t steps;        /* completed steps of completed requests */
+  double p50_step_ms;   /* step latency percentiles over those steps */
+  double p99_step_ms;
+  int64_t fiber_steps;  /* sum of fibers x steps */
+  double elapsed_s;     /* server creation -> last completion */
+  int peak_active;
+  int64_t peak_bytes;
+  int completed, failed, queued, active;
+} rf_server_stats;
+
+/* Device bytes a handle of this configuration and size allocates (an upper
+ * estimate used for admission). */
+int64_t rf_device_bytes_estimate(const rf_config* cfg, int number_of_fibers);
+int rf_server_config_default(rf_server_config* cfg);
+int rf_server_create(const rf_server_config* cfg, rf_server** server);
+/* Queue `nsteps` time steps of a suspension; pos/ori are copied. */
+int rf_server_submit(rf_server* s, const rf_config* cfg, int number_of_fibers, const double* pos,
+                     const double* ori, int nsteps, int64_t* request_id);
+int rf_server_poll(rf_server* s, int64_t request_id, int* status, int* steps_done);
+int rf_server_cancel(rf_server* s, int64_t request_id);
+int rf_server_wait(rf_server* s, int64_t request_id, double timeout_seconds);
+int rf_server_drain(rf_server* s, double timeout_seconds);
+/* Final state and last velocities (any pointer may be NULL). */
+int rf_server_result(rf_server* s, int64_t request_id, double* pos, double* ori, double* tvel, double* rvel,
+                     rf_request_stats* stats);
+int rf_server_get_stats(rf_server* s, rf_server_stats* stats);
+/* Cancels what has not finished, waits for running steps, frees everything. */
+int rf_server_destroy(rf_server* s);
+
 const char* rf_status_string(int status);
 const char* rf_last_error(void);
 

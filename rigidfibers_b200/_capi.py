@@ -58,9 +58,43 @@ class rf_stats(ctypes.Structure):
     ]
 
 
+RF_REQ_QUEUED, RF_REQ_RUNNING, RF_REQ_DONE, RF_REQ_FAILED, RF_REQ_CANCELLED = range(5)
+
+
+class rf_server_config(ctypes.Structure):
+    _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64)]
+
+
+class rf_request_stats(ctypes.Structure):
+    _fields_ = [
+        ("steps_done", ctypes.c_int),
+        ("queue_ms", ctypes.c_double),
+        ("run_ms", ctypes.c_double),
+        ("mean_step_ms", ctypes.c_double),
+        ("device_bytes", ctypes.c_int64),
+    ]
+
+
+class rf_server_stats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64),
+        ("p50_step_ms", ctypes.c_double),
+        ("p99_step_ms", ctypes.c_double),
+        ("fiber_steps", ctypes.c_int64),
+        ("elapsed_s", ctypes.c_double),
+        ("peak_active", ctypes.c_int),
+        ("peak_bytes", ctypes.c_int64),
+        ("completed", ctypes.c_int),
+        ("failed", ctypes.c_int),
+        ("queued", ctypes.c_int),
+        ("active", ctypes.c_int),
+    ]
+
+
 # name -> (restype, argtypes); every entry point declared in include/rigidfibers.h
 _P = ctypes.c_void_p
 _H = ctypes.c_void_p
+_S = ctypes.c_void_p
 SIGNATURES = {
     "rf_config_default": (ctypes.c_int, [ctypes.POINTER(rf_config)]),
     "rf_create": (ctypes.c_int, [ctypes.POINTER(rf_config), ctypes.c_int, _P, _P, ctypes.POINTER(_H)]),
@@ -86,6 +120,18 @@ SIGNATURES = {
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "rf_device_bytes_estimate": (ctypes.c_int64, [ctypes.POINTER(rf_config), ctypes.c_int]),
+    "rf_server_config_default": (ctypes.c_int, [ctypes.POINTER(rf_server_config)]),
+    "rf_server_create": (ctypes.c_int, [ctypes.POINTER(rf_server_config), ctypes.POINTER(_S)]),
+    "rf_server_submit": (ctypes.c_int, [_S, ctypes.POINTER(rf_config), ctypes.c_int, _P, _P, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int64)]),
+    "rf_server_poll": (ctypes.c_int, [_S, ctypes.c_int64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "rf_server_cancel": (ctypes.c_int, [_S, ctypes.c_int64]),
+    "rf_server_wait": (ctypes.c_int, [_S, ctypes.c_int64, ctypes.c_double]),
+    "rf_server_drain": (ctypes.c_int, [_S, ctypes.c_double]),
+    "rf_server_result": (ctypes.c_int, [_S, ctypes.c_int64, _P, _P, _P, _P, ctypes.POINTER(rf_request_stats)]),
+    "rf_server_get_stats": (ctypes.c_int, [_S, ctypes.POINTER(rf_server_stats)]),
+    "rf_server_destroy": (ctypes.c_int, [_S]),
     "rf_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "rf_last_error": (ctypes.c_char_p, []),
 }

@@ -442,12 +442,11 @@ static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const
   using S = AsmShape<M, Q>;
   const int64_t T = ceil_div(N, S::TI);
   const int64_t ntp = INTEG == kNumerical ? T * (T + 1) / 2 : T * T;
-  static bool attr_set = false;  // per process; the attribute is per function
-  if (!attr_set) {
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_assemble_pairs<M, Q, MODE, INTEG>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem));
-    attr_set = true;
-  }
+  // once per process (thread-safe static initialisation; handles of a serving
+  // loop launch from several threads)
+  static const cudaError_t attr = cudaFuncSetAttribute(k_assemble_pairs<M, Q, MODE, INTEG>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
+  RF_CUDA_TRY(attr);
   k_assemble_pairs<M, Q, MODE, INTEG><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
   RF_LAUNCH_CHECK();
   const int64_t n = (int64_t)N * (M + 1);

@@ -170,8 +170,17 @@ struct rf_handle {
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
 
+  bool dry = false;          // count bytes only (rf_device_bytes_estimate)
+  // Stream-ordered allocations: creating or destroying a handle does not
+  // synchronise the device, so handles of a serving loop come and go without
+  // stalling the others.
   int alloc(void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes);
+    if (dry) {
+      *p = nullptr;
+      device_bytes += (int64_t)bytes;
+      return RF_OK;
+    }
+    cudaError_t e = cudaMallocAsync(p, bytes, st);
     if (e != cudaSuccess) {
       *p = nullptr;
       set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -183,7 +192,8 @@ struct rf_handle {
   }
   ~rf_handle() {
     for (auto e : mv_events) cudaEventDestroy(e);
-    for (void* p : allocations) cudaFree(p);
+    for (void* p : allocations) cudaFreeAsync(p, st);
+    if (st) cudaStreamSynchronize(st);
     if (host_ctl) cudaFreeHost(host_ctl);
     if (host_bctl) cudaFreeHost(host_bctl);
     if (lu.host_ipiv) cudaFreeHost(lu.host_ipiv);
@@ -316,29 +326,11 @@ int rf_set_state(rf_handle* h, const double* pos, const double* ori) {
   return RF_OK;
 }
 
-int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori, rf_handle** out) {
-  if (!out) return RF_E_INPUT;
-  *out = nullptr;
-  RF_TRY(validate_config(cfg, N));
-  if (!pos || !ori) { set_last_error_str("rf_create: null fiber arrays"); return RF_E_INPUT; }
-  rf_handle* h = new rf_handle();
-  h->cfg = *cfg;
-  h->N = N;
-  h->M = cfg->number_of_terms_in_force_expansion;
-  h->Q = 3 * cfg->number_of_quadrature_intervals;
-  h->R = (int64_t)3 * h->M * N;
-  h->lda = ceil_div(h->R, 32) * 32;
-  h->tab = make_tables(*cfg);
-  std::memset(&h->stats, 0, sizeof(h->stats));
-  for (auto& e : h->ev) e = nullptr;
-  auto fail = [&](int rc) { delete h; return rc; };
-  cudaError_t e = cudaGetDevice(&h->dev);
-  if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return fail(RF_E_CUDA); }
-  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev);
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(RF_E_CUDA);
-  for (auto& ev : h->ev)
-    if (cudaEventCreate(&ev) != cudaSuccess) return fail(RF_E_CUDA);
+// Every device buffer of a handle.  With h->dry set nothing is allocated and
+// h->device_bytes is the exact footprint (admission control of the server).
+static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   const int64_t R = h->R;
+  const int N = h->N;
   const size_t b64 = (size_t)N * sizeof(double4), b32 = (size_t)N * sizeof(float4);
   int rc = RF_OK;
   for (int s = 0; s < 3 && !rc; ++s) {
@@ -386,7 +378,7 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (!rc) rc = h->alloc((void**)&h->sn, (size_t)m * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->g, (size_t)(m + 1) * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->ctl, sizeof(GmresCtl));
-  if (!rc && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
+  if (!rc && !h->dry && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
   if (cfg->solver == RF_SOLVER_DIRECT) {
     LuSetup& L = h->lu;
     L.R = R;
@@ -404,17 +396,61 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
     if (!rc) rc = h->alloc((void**)&L.x64, (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&L.r64, (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&L.norms, 2 * sizeof(double));
-    if (!rc && cudaMallocHost((void**)&L.host_ipiv, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
-    if (!rc && cudaMallocHost((void**)&L.host_perm, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && !h->dry && cudaMallocHost((void**)&L.host_ipiv, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && !h->dry && cudaMallocHost((void**)&L.host_perm, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
   }
   if (cfg->solver == RF_SOLVER_BICGSTAB) {
     if (!rc) rc = h->alloc((void**)&h->bicg_work, (size_t)6 * (size_t)ldv * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->bctl, sizeof(BicgCtl));
-    if (!rc && cudaMallocHost((void**)&h->host_bctl, sizeof(BicgCtl)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && !h->dry && cudaMallocHost((void**)&h->host_bctl, sizeof(BicgCtl)) != cudaSuccess) rc = RF_E_OOM;
   }
   // velocities
   if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
   if (!rc) rc = h->alloc((void**)&h->vpart, (size_t)velocity_chunks(N) * N * 6 * sizeof(float));
+  return rc;
+}
+
+static void init_dims(rf_handle* h, const rf_config* cfg, int N) {
+  h->cfg = *cfg;
+  h->N = N;
+  h->M = cfg->number_of_terms_in_force_expansion;
+  h->Q = 3 * cfg->number_of_quadrature_intervals;
+  h->R = (int64_t)3 * h->M * N;
+  h->lda = ceil_div(h->R, 32) * 32;
+  h->tab = make_tables(*cfg);
+  std::memset(&h->stats, 0, sizeof(h->stats));
+  for (auto& e : h->ev) e = nullptr;
+}
+
+int64_t rf_device_bytes_estimate(const rf_config* cfg, int N) {
+  if (validate_config(cfg, N) != RF_OK) return -1;
+  rf_handle h;
+  init_dims(&h, cfg, N);
+  h.dry = true;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    h.num_sms = 148;
+  cudaGetLastError();
+  if (allocate_buffers(&h, cfg) != RF_OK) return -1;
+  return h.device_bytes;
+}
+
+int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori, rf_handle** out) {
+  if (!out) return RF_E_INPUT;
+  *out = nullptr;
+  RF_TRY(validate_config(cfg, N));
+  if (!pos || !ori) { set_last_error_str("rf_create: null fiber arrays"); return RF_E_INPUT; }
+  rf_handle* h = new rf_handle();
+  init_dims(h, cfg, N);
+  auto fail = [&](int rc) { delete h; return rc; };
+  cudaError_t e = cudaGetDevice(&h->dev);
+  if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return fail(RF_E_CUDA); }
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev);
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(RF_E_CUDA);
+  for (auto& ev : h->ev)
+    if (cudaEventCreate(&ev) != cudaSuccess) return fail(RF_E_CUDA);
+  int rc = allocate_buffers(h, cfg);
   if (rc) return fail(rc);
   h->stats.device_bytes = h->device_bytes;
   rc = rf_set_state(h, pos, ori);

@@ -379,10 +379,19 @@ static int coop_launch(const void* fn, int nblk, int threads, void** args, cudaS
   return RF_OK;
 }
 
+static thread_local int t_coop_cap = 0;
+
+void set_coop_block_cap(int cap) { t_coop_cap = cap; }
+
 int krylov_coop_blocks(int64_t R, int num_sms) {
   // 256-thread blocks; at most 2 per SM (always co-resident), fewer for small systems
   int want = (int)ceil_div(R, 256 * 4);
-  return std::max(1, std::min(want, 2 * num_sms));
+  int n = std::max(1, std::min(want, 2 * num_sms));
+  // Handles that share the device with other handles' cooperative grids keep
+  // the sum of all grids within one block per SM, so every grid can become
+  // fully resident once the non-cooperative kernels beside it drain.
+  if (t_coop_cap > 0) n = std::min(n, t_coop_cap);
+  return n;
 }
 
 int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,

@@ -1,0 +1,330 @@
+// Serving loop for ensembles of independent suspensions (continuous batching).
+//
+// Requests (a configuration, a fiber layout, a step budget) are queued as they
+// arrive; a dispatcher admits them in arrival order while a slot is free and
+// the device memory their system needs (rf_device_bytes_estimate) fits the
+// budget, so requests that arrive while others run start as soon as a slot
+// and memory free up.  Each admitted request gets its own handle (device-
+// resident fibers, Krylov state, previous-step velocities) and stream, driven
+// by a worker thread; the streams of all running requests overlap on the
+// device.  Every kernel is deterministic (fixed-order reductions, no
+// atomics), so a request's result does not depend on what runs beside it.
+// The reference has no serving layer; this is the ensemble workload of the
+// thesis' parameter studies run as a service.
+#include <algorithm>
+#include <cmath>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "rf_common.cuh"
+#include "rf_kernels.cuh"
+#include "rf_krylov.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  int64_t id = 0;
+  rf_config cfg;
+  int N = 0;
+  int nsteps = 0;
+  std::vector<double> pos, ori;       // inputs, then the final state
+  std::vector<double> tvel, rvel;     // last velocities
+  int64_t bytes = 0;                  // admission estimate
+  int status = RF_REQ_QUEUED;
+  int error = RF_OK;
+  int steps_done = 0;
+  bool cancel = false;
+  double t_submit = 0, t_start = 0, t_end = 0;
+  std::vector<double> step_ms;
+  std::thread worker;
+};
+
+}  // namespace
+
+struct rf_server {
+  rf_server_config cfg;
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv;        // dispatcher wake-up
+  std::condition_variable done_cv;   // waiters
+  std::deque<int64_t> queue;
+  std::map<int64_t, std::unique_ptr<Request>> reqs;
+  std::vector<std::thread> finished_workers;
+  int64_t next_id = 1;
+  int active = 0;
+  int64_t bytes_in_use = 0;
+  int64_t peak_bytes = 0;
+  int peak_active = 0;
+  bool stopping = false;
+  std::thread dispatcher;
+  std::vector<double> all_step_ms;
+  int64_t fiber_steps = 0;
+  double t0 = 0, t_last = 0;
+};
+
+static double now_s() {
+  return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+static void run_request(rf_server* s, Request* r) {
+  cudaSetDevice(s->device);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  rf::set_coop_block_cap(std::max(1, sms / s->cfg.max_active));
+  rf_handle* h = nullptr;
+  int rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
+  std::vector<double> lat;
+  if (rc == RF_OK) {
+    for (int t = 0; t < r->nsteps; ++t) {
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (r->cancel) break;
+      }
+      const auto a = Clock::now();
+      rc = rf_step(h, t);
+      const auto b = Clock::now();
+      if (rc != RF_OK && rc != RF_E_NOCONV) break;
+      rc = RF_OK;
+      lat.push_back(std::chrono::duration<double, std::milli>(b - a).count());
+      std::lock_guard<std::mutex> lk(s->mu);
+      r->steps_done = t + 1;
+    }
+    if (rc == RF_OK) {
+      rf_get_state(h, r->pos.data(), r->ori.data());
+      if (r->steps_done > 0) rf_get_velocities(h, r->tvel.data(), r->rvel.data());
+    }
+    rf_destroy(h);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->t_end = now_s();
+  r->step_ms = lat;
+  r->error = rc;
+  r->status = rc != RF_OK ? RF_REQ_FAILED : (r->cancel ? RF_REQ_CANCELLED : RF_REQ_DONE);
+  if (rc == RF_OK) {
+    s->all_step_ms.insert(s->all_step_ms.end(), lat.begin(), lat.end());
+    s->fiber_steps += (int64_t)r->N * (int64_t)lat.size();
+  }
+  s->t_last = r->t_end;
+  s->active -= 1;
+  s->bytes_in_use -= r->bytes;
+  s->finished_workers.push_back(std::move(r->worker));
+  s->cv.notify_all();
+  s->done_cv.notify_all();
+}
+
+static void dispatch_loop(rf_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    // join workers that finished (their threads were moved here)
+    while (!s->finished_workers.empty()) {
+      std::thread t = std::move(s->finished_workers.back());
+      s->finished_workers.pop_back();
+      lk.unlock();
+      if (t.joinable()) t.join();
+      lk.lock();
+    }
+    if (s->stopping && s->active == 0) return;
+    bool admitted = false;
+    while (!s->stopping && !s->queue.empty()) {
+      Request* r = s->reqs[s->queue.front()].get();
+      if (r->cancel) {
+        r->status = RF_REQ_CANCELLED;
+        s->queue.pop_front();
+        s->done_cv.notify_all();
+        continue;
+      }
+      if (s->active >= s->cfg.max_active) break;
+      if (s->active > 0 && s->bytes_in_use + r->bytes > s->cfg.hbm_budget_bytes) break;   // wait for memory
+      s->queue.pop_front();
+      r->status = RF_REQ_RUNNING;
+      r->t_start = now_s();
+      s->active += 1;
+      s->bytes_in_use += r->bytes;
+      s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
+      s->peak_active = std::max(s->peak_active, s->active);
+      r->worker = std::thread(run_request, s, r);
+      admitted = true;
+    }
+    if (!admitted) s->cv.wait_for(lk, std::chrono::milliseconds(50));
+  }
+}
+
+extern "C" {
+
+int rf_server_config_default(rf_server_config* c) {
+  if (!c) return RF_E_INPUT;
+  std::memset(c, 0, sizeof(*c));
+  c->max_active = 16;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c->hbm_budget_bytes = (int64_t)(0.8 * (double)fr);
+  else c->hbm_budget_bytes = (int64_t)64 << 30;
+  return RF_OK;
+}
+
+int rf_server_create(const rf_server_config* cfg, rf_server** out) {
+  if (!cfg || !out || cfg->max_active < 1 || cfg->hbm_budget_bytes <= 0) {
+    rf::set_last_error_str("rf_server_create: max_active >= 1 and a positive memory budget");
+    return RF_E_INPUT;
+  }
+  rf_server* s = new rf_server();
+  s->cfg = *cfg;
+  cudaGetDevice(&s->device);
+  s->t0 = now_s();
+  s->dispatcher = std::thread(dispatch_loop, s);
+  *out = s;
+  return RF_OK;
+}
+
+int rf_server_submit(rf_server* s, const rf_config* cfg, int N, const double* pos, const double* ori, int nsteps,
+                     int64_t* id) {
+  if (!s || !cfg || !pos || !ori || !id || N < 1 || nsteps < 0) return RF_E_INPUT;
+  auto r = std::make_unique<Request>();
+  r->cfg = *cfg;
+  r->N = N;
+  r->nsteps = nsteps;
+  r->pos.assign(pos, pos + 3 * (size_t)N);
+  r->ori.assign(ori, ori + 3 * (size_t)N);
+  r->tvel.assign(3 * (size_t)N, 0.0);
+  r->rvel.assign(3 * (size_t)N, 0.0);
+  r->bytes = rf_device_bytes_estimate(cfg, N);   // also validates the configuration
+  if (r->bytes < 0) return RF_E_INPUT;
+  r->t_submit = now_s();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) return RF_E_STATE;
+  if (r->bytes > s->cfg.hbm_budget_bytes) {
+    rf::set_last_error_str("rf_server_submit: the request needs more device memory than the budget");
+    return RF_E_OOM;
+  }
+  r->id = s->next_id++;
+  *id = r->id;
+  s->queue.push_back(r->id);
+  s->reqs[r->id] = std::move(r);
+  s->cv.notify_all();
+  return RF_OK;
+}
+
+int rf_server_poll(rf_server* s, int64_t id, int* status, int* steps_done) {
+  if (!s || !status) return RF_E_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return RF_E_INPUT;
+  *status = it->second->status;
+  if (steps_done) *steps_done = it->second->steps_done;
+  return RF_OK;
+}
+
+int rf_server_cancel(rf_server* s, int64_t id) {
+  if (!s) return RF_E_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return RF_E_INPUT;
+  it->second->cancel = true;
+  s->cv.notify_all();
+  return RF_OK;
+}
+
+int rf_server_wait(rf_server* s, int64_t id, double timeout_s) {
+  if (!s) return RF_E_INPUT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return RF_E_INPUT;
+  Request* r = it->second.get();
+  const bool ok = s->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    return r->status == RF_REQ_DONE || r->status == RF_REQ_FAILED || r->status == RF_REQ_CANCELLED;
+  });
+  return ok ? RF_OK : RF_E_TIMEOUT;
+}
+
+int rf_server_drain(rf_server* s, double timeout_s) {
+  if (!s) return RF_E_INPUT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  const bool ok = s->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                      [&] { return s->queue.empty() && s->active == 0; });
+  return ok ? RF_OK : RF_E_TIMEOUT;
+}
+
+int rf_server_result(rf_server* s, int64_t id, double* pos, double* ori, double* tvel, double* rvel,
+                     rf_request_stats* st) {
+  if (!s) return RF_E_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return RF_E_INPUT;
+  Request* r = it->second.get();
+  if (r->status != RF_REQ_DONE && r->status != RF_REQ_CANCELLED && r->status != RF_REQ_FAILED) return RF_E_STATE;
+  if (r->status == RF_REQ_FAILED) return r->error;
+  const size_t n = 3 * (size_t)r->N;
+  if (pos) std::memcpy(pos, r->pos.data(), n * sizeof(double));
+  if (ori) std::memcpy(ori, r->ori.data(), n * sizeof(double));
+  if (tvel) std::memcpy(tvel, r->tvel.data(), n * sizeof(double));
+  if (rvel) std::memcpy(rvel, r->rvel.data(), n * sizeof(double));
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->steps_done = r->steps_done;
+    st->queue_ms = 1000.0 * (r->t_start - r->t_submit);
+    st->run_ms = 1000.0 * (r->t_end - r->t_start);
+    double sum = 0;
+    for (double v : r->step_ms) sum += v;
+    st->mean_step_ms = r->step_ms.empty() ? 0.0 : sum / r->step_ms.size();
+    st->device_bytes = r->bytes;
+  }
+  return RF_OK;
+}
+
+int rf_server_get_stats(rf_server* s, rf_server_stats* out) {
+  if (!s || !out) return RF_E_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(out, 0, sizeof(*out));
+  std::vector<double> v = s->all_step_ms;
+  std::sort(v.begin(), v.end());
+  auto pct = [&](double p) -> double {
+    if (v.empty()) return 0.0;
+    const size_t k = (size_t)std::min<double>(v.size() - 1, std::ceil(p * v.size()) - 1);
+    return v[k];
+  };
+  out->steps = (int64_t)v.size();
+  out->p50_step_ms = pct(0.50);
+  out->p99_step_ms = pct(0.99);
+  out->fiber_steps = s->fiber_steps;
+  out->elapsed_s = s->t_last - s->t0;
+  out->peak_active = s->peak_active;
+  out->peak_bytes = s->peak_bytes;
+  int done = 0, failed = 0, queued = 0;
+  for (auto& kv : s->reqs) {
+    done += kv.second->status == RF_REQ_DONE;
+    failed += kv.second->status == RF_REQ_FAILED;
+    queued += kv.second->status == RF_REQ_QUEUED;
+  }
+  out->completed = done;
+  out->failed = failed;
+  out->queued = queued;
+  out->active = s->active;
+  return RF_OK;
+}
+
+int rf_server_destroy(rf_server* s) {
+  if (!s) return RF_E_INPUT;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+    for (auto& kv : s->reqs) kv.second->cancel = true;
+    s->cv.notify_all();
+  }
+  if (s->dispatcher.joinable()) s->dispatcher.join();
+  for (auto& kv : s->reqs)
+    if (kv.second->worker.joinable()) kv.second->worker.join();
+  for (auto& t : s->finished_workers)
+    if (t.joinable()) t.join();
+  delete s;
+  return RF_OK;
+}
+
+}  // extern "C"

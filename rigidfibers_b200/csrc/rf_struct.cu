@@ -641,12 +641,9 @@ static int launch_z_one(int N, const float* S32, const uint32_t* S16, const XT* 
                         cudaStream_t st) {
   constexpr bool kPrefetch = SMODE != 0;   // 16-bit rows are small enough to double-buffer
   constexpr size_t smem = ZSmem<M, sizeof(ACC)>::kBytes;
-  static bool attr_set = false;
-  if (!attr_set) {
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  static const cudaError_t attr = cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  RF_CUDA_TRY(attr);
   const unsigned grid = (unsigned)struct_store_tiles(N);
   k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch><<<grid, 256, smem, st>>>(N, S32, S16, x, zpart, skip);
   RF_LAUNCH_CHECK();
@@ -666,14 +663,12 @@ template <int M, int SMODE>
 static int launch_z16_bulk(int N, const uint32_t* S16, const float* x, float* zpart, const int* skip, int* err,
                            cudaStream_t st) {
   using B = BulkShape<M>;
-  static int nsm = 0;
-  if (nsm == 0) {
-    int dev = 0;
-    RF_CUDA_TRY(cudaGetDevice(&dev));
-    RF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    RF_CUDA_TRY(cudaFuncSetAttribute(k_struct_z16_bulk<M, SMODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)B::kBytes));
-  }
+  static const cudaError_t attr = cudaFuncSetAttribute(k_struct_z16_bulk<M, SMODE>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::kBytes);
+  RF_CUDA_TRY(attr);
+  int dev = 0, nsm = 0;
+  RF_CUDA_TRY(cudaGetDevice(&dev));
+  RF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int64_t ntiles = struct_store_tiles(N);
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
   k_struct_z16_bulk<M, SMODE><<<grid, B::kThreads, B::kBytes, st>>>(N, S16, x, zpart, skip, err);

@@ -191,3 +191,21 @@ def grown_sphere_layout(n, min_distance=0.2, seed=0, max_retries=1000, batch=64)
                 break
             radius += min_distance
     return pos, ori
+
+
+def serving_requests(count=512, seed=0, n_min=16, n_max=1000, steps_min=5, steps_max=50,
+                     slenderness=(0.01, 0.005)):
+    """The serving ensemble: `count` independent suspensions with N drawn
+    log-uniform in [n_min, n_max], slenderness from `slenderness`, and
+    steps_min..steps_max time steps each.  Layouts are drawn per request by
+    request_layout() (centres in a sphere of volume fraction ~1%)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max + 1), size=count)).astype(int).clip(n_min, n_max)
+    eps = rng.choice(np.asarray(slenderness, np.float64), size=count)
+    steps = rng.integers(steps_min, steps_max + 1, size=count)
+    return [dict(id=i, n=int(ns[i]), slenderness=float(eps[i]), nsteps=int(steps[i]), seed=int(seed) * 100003 + i)
+            for i in range(count)]
+
+
+def request_layout(req):
+    return sphere_layout(req["n"], serving_radius(req["n"]), seed=req["seed"])
