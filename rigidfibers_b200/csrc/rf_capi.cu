@@ -452,6 +452,13 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(RF_E_CUDA);
   int rc = allocate_buffers(h, cfg);
   if (rc) return fail(rc);
+  if (h->mixed) {
+    // records that the assembly never writes (fibers >= N, the lower sub-tile
+    // of a diagonal storage tile) hold zeros rather than whatever the pool had
+    if (cudaMemsetAsync(h->S32, 0, (size_t)struct_floats32(h->M, N) * sizeof(float), h->st) != cudaSuccess ||
+        cudaMemsetAsync(h->S16, 0, (size_t)struct_words16(h->M, N) * sizeof(uint32_t), h->st) != cudaSuccess)
+      return fail(RF_E_CUDA);
+  }
   h->stats.device_bytes = h->device_bytes;
   rc = rf_set_state(h, pos, ori);
   if (rc) return fail(rc);
