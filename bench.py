@@ -47,6 +47,8 @@ def parse():
                     help="suspensions in the served ensemble (0: skip the serving leg)")
     ap.add_argument("--serve-max-active", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--direct-fibers", type=int, default=2000,
+                    help="fibers of the direct-solver leg (0: skip it)")
     return ap.parse_args()
 
 
@@ -395,6 +397,34 @@ def serve_ensemble(args, dist):
                         "while the others run (rank 0's percentiles)"}
 
 
+def direct_leg(args):
+    """The thesis-scale configuration: N fibers (radius 14 sphere at N=2000),
+    analytical integration, one step solved by the blocked LU (in place of
+    MAGMA's sgesv) and by GMRES on the same system.  LU rate = 2/3 R^3 flops over
+    the solve time (factorisation, triangular solves and FP64 refinement)."""
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    n = args.direct_fibers
+    radius = 14.0 * (n / 2000.0) ** (1.0 / 3.0)
+    pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(2, n))
+    out = {"fibers": n, "radius": radius, "integration": "analytical"}
+    for solver in ("direct", "gmres"):
+        sim = Simulation(Config(solver=solver, integration="analytical"), pos, ori)
+        sim.step(0)                      # warm-up (first-touch of the kernels)
+        sim.assembleSystem()
+        sim.solveSystem()
+        st = sim.stats()
+        sim.close()
+        R = 15 * n
+        leg = {"ms_solve": st["ms_solve_system"], "ms_assemble": st["ms_assemble_system"],
+               "relative_residual": st["relative_residual"], "iterations": st["iterations"],
+               "refinements": st["refinement_steps"]}
+        if solver == "direct":
+            leg["tflops"] = (2.0 / 3.0) * R ** 3 / (st["ms_solve_system"] / 1e3) / 1e12
+        out[solver] = leg
+    return out
+
+
 def run_ours(args, dist):
     import torch
 
@@ -463,6 +493,8 @@ def run_ours(args, dist):
     }
     if args.serve_requests > 0:
         out["serving"] = serve_ensemble(args, dist)
+    if args.direct_fibers > 0 and dist.rank == 0:
+        out["direct_solver"] = direct_leg(args)
     if comparison:
         out["fp32_path"] = comparison
         out["speedup_vs_fp32"] = value / comparison["value"]

@@ -145,6 +145,17 @@ int rf_last_stats(rf_handle* h, rf_stats* s);
 int rf_get_config(rf_handle* h, rf_config* cfg);
 int rf_number_of_fibers(rf_handle* h);
 
+/* Checkpoint / resume (the reference writes state files only,
+ * src/simulation.cu:530-604; it cannot resume a second-order run).  The
+ * checkpoint holds the FP64 current and previous fiber states, their FP32
+ * copies, both velocity buffers, the buffer rotation and the number of steps
+ * taken; loading it into a handle created with the same configuration and
+ * fiber count continues the run bit for bit (continue with rf_step(h, t) for
+ * t = *steps_taken, ...).  RF_E_INPUT on a mismatch or a corrupt buffer. */
+int64_t rf_checkpoint_bytes(rf_handle* h);
+int rf_checkpoint_save(rf_handle* h, void* buf, int64_t bytes);
+int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* steps_taken);
+
 /* y = A x with the assembled operator (3MN doubles in and out; after
  * rf_assemble).  which = 0: the working-precision operator (dense FP32 A, or
  * the FP32 pair blocks with FP64 accumulation in mixed mode); which = 1: the

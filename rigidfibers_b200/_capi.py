@@ -120,6 +120,9 @@ SIGNATURES = {
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
+    "rf_checkpoint_bytes": (ctypes.c_int64, [_H]),
+    "rf_checkpoint_save": (ctypes.c_int, [_H, _P, ctypes.c_int64]),
+    "rf_checkpoint_load": (ctypes.c_int, [_H, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "rf_device_bytes_estimate": (ctypes.c_int64, [ctypes.POINTER(rf_config), ctypes.c_int]),
     "rf_server_config_default": (ctypes.c_int, [ctypes.POINTER(rf_server_config)]),
     "rf_server_create": (ctypes.c_int, [ctypes.POINTER(rf_server_config), ctypes.POINTER(_S)]),

@@ -166,6 +166,7 @@ struct rf_handle {
   int matvecs_done = 0;
   int refinements = 0;
   int restart = 10;          // Krylov dimension per cycle
+  int64_t steps_taken = 0;   // completed rf_update_fibers calls (checkpoint metadata)
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -658,6 +659,7 @@ int rf_update_fibers(rf_handle* h, int first_step) {
   h->inext = p;
   std::swap(h->vprev, h->vcur);
   h->assembled = h->solved = false;
+  h->steps_taken += 1;
   return RF_OK;
 }
 
@@ -787,6 +789,122 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
   for (int64_t r = 0; r < R; ++r) y[r] = hy[r];
   h->solved = false;
+  return RF_OK;
+}
+
+// ---- checkpoint / resume --------------------------------------------------
+// Everything the next step reads besides the configuration: the FP64 current
+// and previous fiber states (second-order update), their FP32 copies, both
+// velocity buffers (U^{n-1}, Omega^{n-1}), the buffer rotation and the step
+// count.  Host-endian binary; the configuration is stored field by field and
+// must match on load, so a resumed run repeats the uninterrupted one bit for bit.
+namespace {
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int32_t N, M, Q, solver, integration, precision, velocity_integration;
+  int32_t gmres_restart, gmres_max_iterations, bicgstab_max_iterations, refinement_max_iterations,
+      refinement_restart;
+  double timestep, slenderness, gmres_tolerance, bicgstab_tolerance, refinement_tolerance;
+  int64_t steps_taken;
+  int32_t iprev, icur, vprev, vcur, vlast, pad;
+};
+const char kCkptMagic[8] = {'R', 'F', 'C', 'K', 'P', 'T', '0', '1'};
+
+CkptHeader ckpt_header(const rf_handle* h) {
+  CkptHeader c;
+  std::memset(&c, 0, sizeof(c));
+  std::memcpy(c.magic, kCkptMagic, 8);
+  c.version = 1;
+  c.header_bytes = sizeof(CkptHeader);
+  const rf_config& f = h->cfg;
+  c.N = h->N; c.M = h->M; c.Q = h->Q;
+  c.solver = f.solver; c.integration = f.integration; c.precision = f.precision;
+  c.velocity_integration = f.velocity_integration;
+  c.gmres_restart = f.gmres_restart; c.gmres_max_iterations = f.gmres_max_iterations;
+  c.bicgstab_max_iterations = f.bicgstab_max_iterations;
+  c.refinement_max_iterations = f.refinement_max_iterations; c.refinement_restart = f.refinement_restart;
+  c.timestep = f.timestep; c.slenderness = f.slenderness; c.gmres_tolerance = f.gmres_tolerance;
+  c.bicgstab_tolerance = f.bicgstab_tolerance; c.refinement_tolerance = f.refinement_tolerance;
+  c.steps_taken = h->steps_taken;
+  c.iprev = h->iprev; c.icur = h->icur; c.vprev = h->vprev; c.vcur = h->vcur; c.vlast = h->vlast;
+  return c;
+}
+}  // namespace
+
+int64_t rf_checkpoint_bytes(rf_handle* h) {
+  if (!h) return -1;
+  const int64_t n = h->N;
+  return (int64_t)sizeof(CkptHeader) + 2 * 2 * n * (int64_t)sizeof(double4) + 2 * n * (int64_t)sizeof(float4) +
+         2 * 2 * n * (int64_t)sizeof(float4);
+}
+
+// device buffers in checkpoint order: pos64/ori64 of (prev, cur), pos32, ori32, tv[0..1], rv[0..1]
+static void ckpt_layout(rf_handle* h, std::vector<std::pair<void*, size_t>>& parts) {
+  const size_t b64 = (size_t)h->N * sizeof(double4), b32 = (size_t)h->N * sizeof(float4);
+  parts = {{h->pos64[h->iprev], b64}, {h->ori64[h->iprev], b64}, {h->pos64[h->icur], b64},
+           {h->ori64[h->icur], b64},  {h->pos32, b32},           {h->ori32, b32},
+           {h->tv[0], b32},           {h->tv[1], b32},           {h->rv[0], b32},
+           {h->rv[1], b32}};
+}
+
+int rf_checkpoint_save(rf_handle* h, void* buf, int64_t bytes) {
+  if (!h || !buf || bytes < rf_checkpoint_bytes(h)) {
+    set_last_error_str("rf_checkpoint_save: buffer smaller than rf_checkpoint_bytes");
+    return RF_E_INPUT;
+  }
+  const CkptHeader c = ckpt_header(h);
+  unsigned char* out = static_cast<unsigned char*>(buf);
+  std::memcpy(out, &c, sizeof(c));
+  size_t off = sizeof(c);
+  std::vector<std::pair<void*, size_t>> parts;
+  ckpt_layout(h, parts);
+  for (auto& pt : parts) {
+    RF_CUDA_TRY(cudaMemcpyAsync(out + off, pt.first, pt.second, cudaMemcpyDeviceToHost, h->st));
+    off += pt.second;
+  }
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return RF_OK;
+}
+
+int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* steps_taken) {
+  if (!h || !buf || bytes < (int64_t)sizeof(CkptHeader)) return RF_E_INPUT;
+  CkptHeader c;
+  std::memcpy(&c, buf, sizeof(c));
+  if (std::memcmp(c.magic, kCkptMagic, 8) != 0 || c.version != 1 || c.header_bytes != sizeof(CkptHeader)) {
+    set_last_error_str("rf_checkpoint_load: not a checkpoint of this library version");
+    return RF_E_INPUT;
+  }
+  if (bytes < rf_checkpoint_bytes(h)) { set_last_error_str("rf_checkpoint_load: truncated checkpoint"); return RF_E_INPUT; }
+  CkptHeader mine = ckpt_header(h);
+  // the state fields come from the checkpoint; everything else must match
+  mine.steps_taken = c.steps_taken;
+  mine.iprev = c.iprev; mine.icur = c.icur; mine.vprev = c.vprev; mine.vcur = c.vcur; mine.vlast = c.vlast;
+  if (std::memcmp(&mine, &c, sizeof(c)) != 0) {
+    set_last_error_str("rf_checkpoint_load: checkpoint of another configuration or fiber count");
+    return RF_E_INPUT;
+  }
+  const bool idx_ok = c.iprev >= 0 && c.iprev < 3 && c.icur >= 0 && c.icur < 3 && c.iprev != c.icur &&
+                      (c.vprev == 0 || c.vprev == 1) && c.vcur == 1 - c.vprev && c.vlast >= -1 && c.vlast < 2;
+  if (!idx_ok) { set_last_error_str("rf_checkpoint_load: corrupt buffer indices"); return RF_E_INPUT; }
+  h->iprev = c.iprev;
+  h->icur = c.icur;
+  h->inext = 3 - c.iprev - c.icur;
+  h->vprev = c.vprev;
+  h->vcur = c.vcur;
+  h->vlast = c.vlast;
+  h->steps_taken = c.steps_taken;
+  const unsigned char* in = static_cast<const unsigned char*>(buf);
+  size_t off = sizeof(c);
+  std::vector<std::pair<void*, size_t>> parts;
+  ckpt_layout(h, parts);
+  for (auto& pt : parts) {
+    RF_CUDA_TRY(cudaMemcpyAsync(pt.first, in + off, pt.second, cudaMemcpyHostToDevice, h->st));
+    off += pt.second;
+  }
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  h->assembled = h->solved = false;
+  if (steps_taken) *steps_taken = c.steps_taken;
   return RF_OK;
 }
 

@@ -172,6 +172,31 @@ class Simulation:
         C.check(self._lib.rf_operator_apply(self._h, C.ptr(xx), C.ptr(y), int(which)), "rf_operator_apply")
         return y
 
+    # -- checkpoint / resume ---------------------------------------------------
+    def checkpoint(self):
+        """The run's resumable state as bytes (rf_checkpoint_save)."""
+        n = self._lib.rf_checkpoint_bytes(self._h)
+        buf = np.empty(n, np.uint8)
+        C.check(self._lib.rf_checkpoint_save(self._h, C.ptr(buf), n), "rf_checkpoint_save")
+        return buf.tobytes()
+
+    def restore(self, data):
+        """Load a checkpoint taken with the same configuration and fiber count;
+        returns the number of steps it had taken (the next step's index)."""
+        buf = np.frombuffer(data, np.uint8)
+        steps = ctypes.c_int64()
+        C.check(self._lib.rf_checkpoint_load(self._h, C.ptr(buf), buf.size, ctypes.byref(steps)),
+                "rf_checkpoint_load")
+        return steps.value
+
+    def save_checkpoint(self, path):
+        with open(path, "wb") as fh:
+            fh.write(self.checkpoint())
+
+    def load_checkpoint(self, path):
+        with open(path, "rb") as fh:
+            return self.restore(fh.read())
+
     def stats(self):
         s = C.rf_stats()
         C.check(self._lib.rf_last_stats(self._h, ctypes.byref(s)), "rf_last_stats")

@@ -225,3 +225,48 @@ def test_analytic_with_numerical_velocities_matches_committed_reference_code():
     for t in range(2):
         for k in ("b", "x", "tvel", "rvel", "pos", "ori"):
             assert _rel(res[t][k], ref[t][k]) <= 1e-5, (t, k, _rel(res[t][k], ref[t][k]))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed_fp16"])
+def test_checkpoint_resume_is_bit_exact(tmp_path, prec):
+    """A run stopped after 3 steps and resumed from its checkpoint in a new
+    handle repeats the uninterrupted 6-step run bit for bit."""
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200.generate import sphere_layout
+    pos, ori = sphere_layout(40, 3.0, seed=17)
+    cfg = dict(precision=prec)
+    ref = Simulation(Config(**cfg), pos, ori)
+    ref.run(6)
+    p_ref, o_ref = ref.state()
+    v_ref = ref.velocities()
+    first = Simulation(Config(**cfg), pos, ori)
+    first.run(3)
+    path = tmp_path / "run.ckpt"
+    first.save_checkpoint(str(path))
+    first.close()
+    resumed = Simulation(Config(**cfg), np.zeros((40, 3)), np.tile([0.0, 0.0, 1.0], (40, 1)))
+    t0 = resumed.load_checkpoint(str(path))
+    assert t0 == 3
+    for t in range(t0, 6):
+        resumed.step(t)
+    p, o = resumed.state()
+    v = resumed.velocities()
+    assert np.array_equal(p, p_ref) and np.array_equal(o, o_ref)
+    assert np.array_equal(v[0], v_ref[0]) and np.array_equal(v[1], v_ref[1])
+
+
+def test_checkpoint_rejects_other_configuration():
+    from rigidfibers_b200 import Config, RigidFibersError, Simulation
+    from rigidfibers_b200.generate import sphere_layout
+    pos, ori = sphere_layout(20, 2.5, seed=3)
+    a = Simulation(Config(), pos, ori)
+    a.run(1)
+    data = a.checkpoint()
+    b = Simulation(Config(timestep=0.05), pos, ori)
+    with pytest.raises(RigidFibersError):
+        b.restore(data)
+    c = Simulation(Config(), pos[:19], ori[:19])
+    with pytest.raises(RigidFibersError):
+        c.restore(data)
+    with pytest.raises(RigidFibersError):
+        a.restore(b"not a checkpoint" * 4)
