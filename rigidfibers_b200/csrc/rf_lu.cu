@@ -179,59 +179,125 @@ __global__ void __launch_bounds__(256) k_lu_trsm(float* __restrict__ A, int64_t 
 
 // C -= A_panel * B_panel on the trailing block: C = A[k+nb.., k+nb..],
 // A_panel = A[k+nb.., k..k+nb) (L21), B_panel = A[k..k+nb, k+nb..) (U12).
-// 128x128 output tiles, 256 threads with 8x8 register tiles, K = NB staged
-// through shared memory in chunks of 16.
+// Trailing update A22 -= L21 U12 on the tensor cores (mma.sync m16n8k8, TF32
+// inputs, FP32 accumulation) with the operands split as a = a_hi + a_lo (both
+// TF32) and a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi: three tensor-core products
+// give FP32-level accuracy, so the factors are as accurate as an FP32 update and
+// the FP64 refinement needs no more steps than with one.
+// 128x128 output tile per CTA, 8 warps of 64x32; K = NB in chunks of 32 staged
+// through shared memory with float4 loads (L21 columns and U12 columns are both
+// contiguous in the column-major matrix).  Padded strides put the fragment
+// loads on distinct banks: a (row g, k t) at 8t + g, b (k t, col g) at 4g + t.
+// The output is updated straight from the accumulator fragments: each column's
+// 8 consecutive rows fill a 32-byte sector.
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 template <int NB>
-__global__ void __launch_bounds__(256) k_lu_gemm(float* __restrict__ A, int64_t lda, int64_t R, int64_t k) {
-  constexpr int TM = 128, TN = 128, TK = 16;
-  __shared__ float sa[TK][TM + 4];
-  __shared__ float sb[TK][TN + 4];
+__global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
+                                                    bool vec4) {
+  constexpr int TM = 128, TN = 128, TK = 32;
+  constexpr int LA = TM + 8, LB = TK + 4;
+  static_assert(NB % TK == 0, "K chunks");
+  __shared__ __align__(16) float sa[TK * LA];   // [k][m]
+  __shared__ __align__(16) float sb[TN * LB];   // [n][k]
   const int64_t m0 = k + NB + (int64_t)blockIdx.x * TM;
   const int64_t n0 = k + NB + (int64_t)blockIdx.y * TN;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  float acc[8][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  float acc[4][4][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-    for (int jx = 0; jx < 8; ++jx) acc[i][jx] = 0.f;
-  for (int kk = 0; kk < NB; kk += TK) {
-    // L21 tile: rows m0.., cols k+kk..  (column-major: consecutive rows contiguous)
-    for (int e = threadIdx.x; e < TK * TM; e += blockDim.x) {
-      const int r = e % TM, c = e / TM;
-      const int64_t gr = m0 + r;
-      sa[c][r] = gr < R ? A[gr + (k + kk + c) * lda] : 0.f;
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.f;
+  for (int kc = 0; kc < NB; kc += TK) {
+    // L21 chunk: TK columns of TM rows
+    for (int e = threadIdx.x; e < TK * TM / 4; e += blockDim.x) {
+      const int c = e / (TM / 4), r4 = (e % (TM / 4)) * 4;
+      const int64_t gr = m0 + r4;
+      const float* src = A + gr + (k + kc + c) * lda;
+      float4 v;
+      if (vec4 && gr + 3 < R) {
+        v = *reinterpret_cast<const float4*>(src);
+      } else {
+        v.x = gr < R ? src[0] : 0.f;
+        v.y = gr + 1 < R ? src[1] : 0.f;
+        v.z = gr + 2 < R ? src[2] : 0.f;
+        v.w = gr + 3 < R ? src[3] : 0.f;
+      }
+      *reinterpret_cast<float4*>(&sa[c * LA + r4]) = v;
     }
-    // U12 tile: rows k+kk.., cols n0..
-    for (int e = threadIdx.x; e < TK * TN; e += blockDim.x) {
-      const int r = e % TK, c = e / TK;
-      const int64_t gc = n0 + c;
-      sb[r][c] = gc < R ? A[(k + kk + r) + gc * lda] : 0.f;
+    // U12 chunk: TN columns of TK rows (rows k+kc.., always inside the matrix)
+    for (int e = threadIdx.x; e < TN * TK / 4; e += blockDim.x) {
+      const int n = e / (TK / 4), r4 = (e % (TK / 4)) * 4;
+      const int64_t gc = n0 + n;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (gc < R) {
+        const float* src = A + (k + kc + r4) + gc * lda;
+        if (vec4) v = *reinterpret_cast<const float4*>(src);
+        else v = make_float4(src[0], src[1], src[2], src[3]);
+      }
+      *reinterpret_cast<float4*>(&sb[n * LB + r4]) = v;
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < TK; ++q) {
-      float av[8], bv[8];
+    for (int ks = 0; ks < TK; ks += 8) {
+      uint32_t ah[4][4], al[4][4], bh[4][2], bl[4][2];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) av[i] = sa[q][ty * 8 + i];
+      for (int mi = 0; mi < 4; ++mi) {
+        const int mr = wm + mi * 16 + g;
+        const float v[4] = {sa[(ks + t) * LA + mr], sa[(ks + t) * LA + mr + 8], sa[(ks + t + 4) * LA + mr],
+                            sa[(ks + t + 4) * LA + mr + 8]};
 #pragma unroll
-      for (int jx = 0; jx < 8; ++jx) bv[jx] = sb[q][tx * 8 + jx];
+        for (int e = 0; e < 4; ++e) {
+          ah[mi][e] = tf32_bits(v[e]);
+          al[mi][e] = tf32_bits(v[e] - __uint_as_float(ah[mi][e]));
+        }
+      }
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int ni = 0; ni < 4; ++ni) {
+        const int nc = wn + ni * 8 + g;
+        const float v[2] = {sb[nc * LB + ks + t], sb[nc * LB + ks + t + 4]};
 #pragma unroll
-        for (int jx = 0; jx < 8; ++jx) acc[i][jx] = fmaf(av[i], bv[jx], acc[i][jx]);
+        for (int e = 0; e < 2; ++e) {
+          bh[ni][e] = tf32_bits(v[e]);
+          bl[ni][e] = tf32_bits(v[e] - __uint_as_float(bh[ni][e]));
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
+        }
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int jx = 0; jx < 8; ++jx) {
-    const int64_t gc = n0 + tx * 8 + jx;
-    if (gc >= R) continue;
+  for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t gr = m0 + ty * 8 + i;
-      if (gr < R) A[gr + gc * lda] -= acc[i][jx];
+    for (int ni = 0; ni < 4; ++ni) {
+      const int64_t r0 = m0 + wm + mi * 16 + g, c0 = n0 + wn + ni * 8 + 2 * t;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int64_t r = r0 + (e >> 1) * 8, c = c0 + (e & 1);
+        if (r < R && c < R) A[r + c * lda] -= acc[mi][ni][e];
+      }
     }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -364,6 +430,9 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
                                 cudaMemcpyDeviceToDevice, st));
   RF_CUDA_TRY(cudaMemsetAsync(s.info, 0, sizeof(int), st));
   int launches = 0;
+  // float4 staging needs every column start 16-byte aligned (k and the chunk
+  // offsets are multiples of 4)
+  const bool vec4 = (lda % 4 == 0) && (reinterpret_cast<uintptr_t>(s.LU) % 16 == 0);
   for (int64_t k = 0; k < R; k += NB) {
     const int nb = (int)std::min<int64_t>(NB, R - k);
     PanelArgs pa{s.LU, lda, R, k, nb, s.ipiv, s.pmax, s.pidx, s.info};
@@ -379,7 +448,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
       }
       k_lu_trsm<NB><<<(unsigned)ceil_div(R - k - NB, 256), 256, 0, st>>>(s.LU, lda, R, k);
       dim3 g((unsigned)ceil_div(R - k - NB, 128), (unsigned)ceil_div(R - k - NB, 128));
-      k_lu_gemm<NB><<<g, 256, 0, st>>>(s.LU, lda, R, k);
+      k_lu_gemm<NB><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
       launches += 2;
     }
     RF_LAUNCH_CHECK();
