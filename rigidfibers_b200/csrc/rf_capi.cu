@@ -386,12 +386,14 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     L.lda = h->lda;
     L.tol = cfg->refinement_tolerance;
     L.max_refine = cfg->refinement_max_iterations;
-    L.coop_blocks = h->coop_blocks;
+    L.coop_blocks = std::max(h->coop_blocks, coop_blocks_per_sm_capped(h->num_sms));
     if (!rc) rc = h->alloc((void**)&L.LU, (size_t)h->lda * (size_t)R * sizeof(float));
     if (!rc) rc = h->alloc((void**)&L.ipiv, (size_t)R * sizeof(int));
     if (!rc) rc = h->alloc((void**)&L.perm, (size_t)R * sizeof(int));
-    if (!rc) rc = h->alloc((void**)&L.pmax, (size_t)h->coop_blocks * sizeof(float));
-    if (!rc) rc = h->alloc((void**)&L.pidx, (size_t)h->coop_blocks * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.pmax, (size_t)2 * L.coop_blocks * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.pidx, (size_t)2 * L.coop_blocks * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.prow, (size_t)2 * L.coop_blocks * 64 * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.jrow, (size_t)2 * 64 * sizeof(float));
     if (!rc) rc = h->alloc((void**)&L.info, sizeof(int));
     if (!rc) rc = h->alloc((void**)&L.d, (size_t)R * sizeof(float));
     if (!rc) rc = h->alloc((void**)&L.x64, (size_t)R * sizeof(double));
@@ -941,7 +943,7 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
   L.lda = R;
   L.tol = tol;
   L.max_refine = 20;
-  L.coop_blocks = krylov_coop_blocks(R, sms);
+  L.coop_blocks = std::max(krylov_coop_blocks(R, sms), coop_blocks_per_sm_capped(sms));
   std::vector<void*> mem;
   auto get = [&](void** p, size_t bytes) -> int {
     cudaError_t e = cudaMallocAsync(p, bytes, st);
@@ -952,8 +954,10 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
   int rc = get((void**)&L.LU, (size_t)R * R * sizeof(float));
   if (!rc) rc = get((void**)&L.ipiv, R * sizeof(int));
   if (!rc) rc = get((void**)&L.perm, R * sizeof(int));
-  if (!rc) rc = get((void**)&L.pmax, L.coop_blocks * sizeof(float));
-  if (!rc) rc = get((void**)&L.pidx, L.coop_blocks * sizeof(int));
+  if (!rc) rc = get((void**)&L.pmax, 2 * L.coop_blocks * sizeof(float));
+  if (!rc) rc = get((void**)&L.pidx, 2 * L.coop_blocks * sizeof(int));
+  if (!rc) rc = get((void**)&L.prow, 2 * L.coop_blocks * 64 * sizeof(float));
+  if (!rc) rc = get((void**)&L.jrow, 2 * 64 * sizeof(float));
   if (!rc) rc = get((void**)&L.info, sizeof(int));
   if (!rc) rc = get((void**)&L.d, R * sizeof(float));
   if (!rc) rc = get((void**)&L.x64, R * sizeof(double));

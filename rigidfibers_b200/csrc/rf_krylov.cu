@@ -383,6 +383,8 @@ static thread_local int t_coop_cap = 0;
 
 void set_coop_block_cap(int cap) { t_coop_cap = cap; }
 
+int coop_blocks_per_sm_capped(int num_sms) { return t_coop_cap > 0 ? std::min(num_sms, t_coop_cap) : num_sms; }
+
 int krylov_coop_blocks(int64_t R, int num_sms) {
   // 256-thread blocks; at most 2 per SM (always co-resident), fewer for small systems
   int want = (int)ceil_div(R, 256 * 4);

@@ -62,6 +62,8 @@ int krylov_coop_blocks(int64_t R, int num_sms);
 // Upper bound on krylov_coop_blocks for handles created on the calling thread
 // (0 = none); set by the serving loop, whose handles run concurrently.
 void set_coop_block_cap(int cap);
+// One cooperative block per SM, within that bound (the LU panel's grid).
+int coop_blocks_per_sm_capped(int num_sms);
 int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
                 GmresResult* res);
 // GMRES with iterative refinement at every restart: the Arnoldi steps use

@@ -17,6 +17,7 @@
 // with the factors until ||r|| / ||b|| meets the tolerance.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -136,6 +137,110 @@ __global__ void __launch_bounds__(256) k_lu_panel(PanelArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same panel factorisation with the panel held in shared memory: block b
+// owns rows [k + b*rows_per, ...) of the panel's nb columns (column-major in
+// shared memory) for the whole kernel, so the panel is read and written once,
+// and one grid sync per column suffices: before it, every block publishes its
+// candidate pivot (largest |a| of the column among its rows, smallest row on
+// ties) together with that row's values, and the owner of the diagonal row
+// publishes it; after it, every block reduces the candidates in the same way,
+// the owners of the two rows exchange them, and each block scales and updates
+// its rows and publishes the next column's candidate.  The candidate buffers
+// alternate by column parity.  Per element the arithmetic is that of
+// k_lu_panel (a * (1 / pivot), then fmaf(-l, u, a) per column), so both give
+// the same factors.
+// ---------------------------------------------------------------------------
+struct PanelSmArgs {
+  float* A;
+  int64_t lda, R, k;
+  int nb, rows_per;
+  int* ipiv;
+  float* pmax;   // [2][gridDim.x]
+  int* pidx;     // [2][gridDim.x]
+  float* prow;   // [2][gridDim.x][64]
+  float* jrow;   // [2][64]
+  int* info;
+};
+
+constexpr int kPanelSmemBytes = 192 * 1024;
+
+__global__ void __launch_bounds__(256) k_lu_panel_smem(PanelSmArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ float sp[];   // [nb][rows_per]
+  __shared__ float s_prow[64];
+  __shared__ int s_p, s_loc;
+  __shared__ float s_pabs;
+  const int nb = a.nb, rp = a.rows_per, nblk = (int)gridDim.x;
+  const int64_t k = a.k, R = a.R, lda = a.lda;
+  const int64_t r0 = k + (int64_t)blockIdx.x * rp;
+  const int nloc = (int)max((int64_t)0, min((int64_t)rp, R - r0));
+  float* A = a.A;
+  for (int c = 0; c < nb; ++c)
+    for (int r = threadIdx.x; r < nloc; r += blockDim.x) sp[c * rp + r] = A[r0 + r + (k + c) * lda];
+  __syncthreads();
+  // candidate of column jj (rows >= k + jj) into buffer buf, and the diagonal row
+  auto publish = [&](int jj, int buf) {
+    float bv = -1.f;
+    int bi = INT_MAX;
+    for (int r = threadIdx.x; r < nloc; r += blockDim.x)
+      if (r0 + r >= k + jj) better(bv, bi, fabsf(sp[jj * rp + r]), (int)(r0 + r));
+    block_argmax(bv, bi, a.pmax + buf * nblk, a.pidx + buf * nblk);   // writes [blockIdx.x], syncs
+    if (threadIdx.x == 0) s_loc = a.pidx[buf * nblk + blockIdx.x];
+    __syncthreads();
+    const int loc = s_loc;
+    if (loc != INT_MAX && threadIdx.x < nb)
+      a.prow[((int64_t)buf * nblk + blockIdx.x) * 64 + threadIdx.x] = sp[threadIdx.x * rp + (loc - r0)];
+    const int64_t j = k + jj;
+    if (j >= r0 && j < r0 + nloc && threadIdx.x < nb) a.jrow[buf * 64 + threadIdx.x] = sp[threadIdx.x * rp + (j - r0)];
+  };
+  publish(0, 0);
+  for (int jj = 0; jj < nb; ++jj) {
+    const int buf = jj & 1;
+    const int64_t j = k + jj;
+    grid.sync();
+    if (threadIdx.x < 32) {
+      float bv = -1.f;
+      int bi = INT_MAX;
+      for (int b = threadIdx.x; b < nblk; b += 32) better(bv, bi, a.pmax[buf * nblk + b], a.pidx[buf * nblk + b]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_down_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        better(bv, bi, ov, oi);
+      }
+      if (threadIdx.x == 0) { s_p = bi; s_pabs = bv; }
+    }
+    __syncthreads();
+    const int64_t p = s_p == INT_MAX ? j : (int64_t)s_p;   // an all-zero column keeps its row
+    const int bw = (int)((p - k) / rp);
+    if (threadIdx.x < nb) s_prow[threadIdx.x] = a.prow[((int64_t)buf * nblk + bw) * 64 + threadIdx.x];
+    __syncthreads();
+    if (p != j && threadIdx.x < nb) {
+      if (j >= r0 && j < r0 + nloc) sp[threadIdx.x * rp + (j - r0)] = s_prow[threadIdx.x];
+      if (p >= r0 && p < r0 + nloc) sp[threadIdx.x * rp + (p - r0)] = a.jrow[buf * 64 + threadIdx.x];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.ipiv[j] = (int)p;
+      if (!(s_pabs > 0.f) && *a.info == 0) *a.info = (int)(j + 1);
+    }
+    __syncthreads();
+    const float piv = s_prow[jj];
+    const float inv = piv != 0.f ? 1.f / piv : 0.f;
+    for (int r = threadIdx.x; r < nloc; r += blockDim.x) {
+      if (r0 + r <= j) continue;
+      const float l = sp[jj * rp + r] * inv;
+      sp[jj * rp + r] = l;
+      for (int c = jj + 1; c < nb; ++c) sp[c * rp + r] = fmaf(-l, s_prow[c], sp[c * rp + r]);
+    }
+    __syncthreads();
+    if (jj + 1 < nb) publish(jj + 1, buf ^ 1);
+  }
+  __syncthreads();
+  for (int c = 0; c < nb; ++c)
+    for (int r = threadIdx.x; r < nloc; r += blockDim.x) A[r0 + r + (k + c) * lda] = sp[c * rp + r];
+}
+
 // Row swaps of the panel [k, k+nb) on the columns outside it.
 __global__ void k_lu_laswp(float* __restrict__ A, int64_t lda, int64_t R, int64_t k, int nb,
                            const int* __restrict__ ipiv) {
@@ -180,10 +285,11 @@ __global__ void __launch_bounds__(256) k_lu_trsm(float* __restrict__ A, int64_t 
 // C -= A_panel * B_panel on the trailing block: C = A[k+nb.., k+nb..],
 // A_panel = A[k+nb.., k..k+nb) (L21), B_panel = A[k..k+nb, k+nb..) (U12).
 // Trailing update A22 -= L21 U12 on the tensor cores (mma.sync m16n8k8, TF32
-// inputs, FP32 accumulation) with the operands split as a = a_hi + a_lo (both
-// TF32) and a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi: three tensor-core products
-// give FP32-level accuracy, so the factors are as accurate as an FP32 update and
-// the FP64 refinement needs no more steps than with one.
+// inputs, FP32 accumulation).  SPLIT = false: one TF32 product (the operands
+// keep 10 mantissa bits; the FP64 refinement wins the accuracy back).  SPLIT =
+// true: a = a_hi + a_lo (both TF32) and a b ~ a_hi b_hi + a_hi b_lo + a_lo
+// b_hi, three products with FP32-level accuracy, for matrices whose
+// conditioning makes the refinement of TF32 factors stall.
 // 128x128 output tile per CTA, 8 warps of 64x32; K = NB in chunks of 32 staged
 // through shared memory with float4 loads (L21 columns and U12 columns are both
 // contiguous in the column-major matrix).  Padded strides put the fragment
@@ -203,7 +309,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-template <int NB>
+template <int NB, bool SPLIT>
 __global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
                                                     bool vec4) {
   constexpr int TM = 128, TN = 128, TK = 32;
@@ -263,7 +369,7 @@ __global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           ah[mi][e] = tf32_bits(v[e]);
-          al[mi][e] = tf32_bits(v[e] - __uint_as_float(ah[mi][e]));
+          if constexpr (SPLIT) al[mi][e] = tf32_bits(v[e] - __uint_as_float(ah[mi][e]));
         }
       }
 #pragma unroll
@@ -273,15 +379,17 @@ __global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           bh[ni][e] = tf32_bits(v[e]);
-          bl[ni][e] = tf32_bits(v[e] - __uint_as_float(bh[ni][e]));
+          if constexpr (SPLIT) bl[ni][e] = tf32_bits(v[e] - __uint_as_float(bh[ni][e]));
         }
       }
 #pragma unroll
       for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) {
-          mma_tf32(acc[mi][ni], al[mi], bh[ni]);
-          mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+          if constexpr (SPLIT) {
+            mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+            mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+          }
           mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
         }
     }
@@ -423,7 +531,9 @@ __global__ void k_axpy64(double* __restrict__ x, const float* __restrict__ d, in
     x[i] = (init ? 0.0 : x[i]) + (double)d[i];
 }
 
-int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res) {
+// Factor a copy of A (panels, swaps, triangular block rows, trailing updates)
+// and compose the row permutation.
+static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t st, int* launches_out) {
   const int64_t R = s.R, lda = s.lda;
   constexpr int NB = 64;
   RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, lda * sizeof(float), R * sizeof(float), R,
@@ -433,12 +543,30 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   // float4 staging needs every column start 16-byte aligned (k and the chunk
   // offsets are multiples of 4)
   const bool vec4 = (lda % 4 == 0) && (reinterpret_cast<uintptr_t>(s.LU) % 16 == 0);
+  static const cudaError_t smem_attr =
+      cudaFuncSetAttribute(k_lu_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBytes);
+  int dev = 0, num_sms = 148;
+  RF_CUDA_TRY(cudaGetDevice(&dev));
+  RF_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
   for (int64_t k = 0; k < R; k += NB) {
     const int nb = (int)std::min<int64_t>(NB, R - k);
-    PanelArgs pa{s.LU, lda, R, k, nb, s.ipiv, s.pmax, s.pidx, s.info};
-    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(s.coop_blocks, ceil_div(R - k, 256)));
-    void* args[] = {&pa};
-    RF_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_lu_panel, dim3(nblk), dim3(256), args, 0, st));
+    // shared-memory panel: one block per SM at most (its rows of the panel
+    // fit in kPanelSmemBytes); the global-memory panel otherwise
+    const int sm_blocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>(std::min<int64_t>((int64_t)s.coop_blocks, (int64_t)num_sms), ceil_div(R - k, 32)));
+    const int rows_per = (int)ceil_div(R - k, sm_blocks);
+    const size_t psmem = (size_t)rows_per * nb * sizeof(float);
+    if (smem_attr == cudaSuccess && psmem <= (size_t)kPanelSmemBytes) {
+      const int nblk = (int)ceil_div(R - k, rows_per);
+      PanelSmArgs pa{s.LU, lda, R, k, nb, rows_per, s.ipiv, s.pmax, s.pidx, s.prow, s.jrow, s.info};
+      void* args[] = {&pa};
+      RF_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_lu_panel_smem, dim3(nblk), dim3(256), args, psmem, st));
+    } else {
+      PanelArgs pa{s.LU, lda, R, k, nb, s.ipiv, s.pmax, s.pidx, s.info};
+      const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(s.coop_blocks, ceil_div(R - k, 256)));
+      void* args[] = {&pa};
+      RF_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_lu_panel, dim3(nblk), dim3(256), args, 0, st));
+    }
     k_lu_laswp<<<(unsigned)ceil_div(R, 256), 256, 0, st>>>(s.LU, lda, R, k, nb, s.ipiv);
     launches += 2;
     if (k + nb < R) {
@@ -448,7 +576,8 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
       }
       k_lu_trsm<NB><<<(unsigned)ceil_div(R - k - NB, 256), 256, 0, st>>>(s.LU, lda, R, k);
       dim3 g((unsigned)ceil_div(R - k - NB, 128), (unsigned)ceil_div(R - k - NB, 128));
-      k_lu_gemm<NB><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
+      if (split) k_lu_gemm<NB, true><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
+      else k_lu_gemm<NB, false><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
       launches += 2;
     }
     RF_LAUNCH_CHECK();
@@ -457,6 +586,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   RF_CUDA_TRY(cudaMemcpyAsync(&info, s.info, sizeof(int), cudaMemcpyDeviceToHost, st));
   RF_CUDA_TRY(cudaMemcpyAsync(s.host_ipiv, s.ipiv, R * sizeof(int), cudaMemcpyDeviceToHost, st));
   RF_CUDA_TRY(cudaStreamSynchronize(st));
+  *launches_out += launches;
   if (info != 0) {
     set_last_error_str("lu: zero pivot");
     return RF_E_SINGULAR;
@@ -468,27 +598,46 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
     if (p != j) std::swap(s.host_perm[j], s.host_perm[p]);
   }
   RF_CUDA_TRY(cudaMemcpyAsync(s.perm, s.host_perm, R * sizeof(int), cudaMemcpyHostToDevice, st));
-  // x0 = (LU)^{-1} P b, then refine: r = b - A x (FP64), d = (LU)^{-1} P r
-  RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, b, s.d, st));
+  return RF_OK;
+}
+
+// The TF32 factors first; FP64-residual refinement until ||b - A x|| / ||b||
+// <= tol.  If the refinement stalls (the residual falls by less than half in a
+// step, after the first two), the matrix is factored again with the split
+// 3xTF32 update and refined from the start.
+int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res) {
+  const int64_t R = s.R, lda = s.lda;
   const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 4096);
-  k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 1);
-  double h[2] = {0, 0};
-  int steps = 0;
+  int launches = 0, steps = 0;
   double rel = 0.0;
-  for (;;) {
-    k_residual64<<<(unsigned)ceil_div(R, 256), 256, 0, st>>>(A, lda, R, s.x64, b, s.r64);
-    k_norm2_pair<<<1, 256, 0, st>>>(s.r64, b, R, s.norms);
-    RF_LAUNCH_CHECK();
-    RF_CUDA_TRY(cudaMemcpyAsync(h, s.norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    RF_CUDA_TRY(cudaStreamSynchronize(st));
-    rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
-    if (!std::isfinite(rel)) return RF_E_NAN;
-    if (rel <= s.tol || steps >= s.max_refine) break;
-    // the FP32 residual goes through the output vector, which is overwritten at the end
-    k_to_float<<<eb, 256, 0, st>>>(s.r64, x, R);
-    RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, x, s.d, st));
-    k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 0);
-    ++steps;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool split = pass == 1;
+    RF_TRY_RF(lu_factor(s, A, split, st, &launches));
+    // x0 = (LU)^{-1} P b, then refine: r = b - A x (FP64), d = (LU)^{-1} P r
+    RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, b, s.d, st));
+    k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 1);
+    double h[2] = {0, 0};
+    steps = 0;
+    double prev = 0.0;
+    bool stalled = false;
+    for (;;) {
+      k_residual64<<<(unsigned)ceil_div(R, 256), 256, 0, st>>>(A, lda, R, s.x64, b, s.r64);
+      k_norm2_pair<<<1, 256, 0, st>>>(s.r64, b, R, s.norms);
+      RF_LAUNCH_CHECK();
+      RF_CUDA_TRY(cudaMemcpyAsync(h, s.norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      RF_CUDA_TRY(cudaStreamSynchronize(st));
+      rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
+      if (!std::isfinite(rel)) return RF_E_NAN;
+      if (rel <= s.tol || steps >= s.max_refine) break;
+      if (!split && steps >= 2 && rel > 0.5 * prev) { stalled = true; break; }
+      prev = rel;
+      // the FP32 residual goes through the output vector, which is overwritten at the end
+      k_to_float<<<eb, 256, 0, st>>>(s.r64, x, R);
+      RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, x, s.d, st));
+      k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 0);
+      ++steps;
+    }
+    if (!stalled) break;
   }
   k_to_float<<<eb, 256, 0, st>>>(s.x64, x, R);
   RF_LAUNCH_CHECK();

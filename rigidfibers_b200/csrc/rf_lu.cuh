@@ -12,8 +12,10 @@ struct LuSetup {
   int* perm;          // R: final row permutation, perm[i] = original row of row i
   int* host_ipiv;     // R pinned (permutation composed on the host)
   int* host_perm;     // R pinned
-  float* pmax;        // coop_blocks
-  int* pidx;          // coop_blocks
+  float* pmax;        // 2 x coop_blocks
+  int* pidx;          // 2 x coop_blocks
+  float* prow;        // 2 x coop_blocks x 64: candidate pivot rows (shared-memory panel)
+  float* jrow;        // 2 x 64: the diagonal row of the current column
   int* info;          // 1
   float* d;           // R: right-hand side / correction
   double* x64;        // R: refined solution
