@@ -310,90 +310,94 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 }
 
 template <int NB, bool SPLIT>
-__global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
+__global__ void __launch_bounds__(256, 1) k_lu_gemm(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
                                                     bool vec4) {
-  constexpr int TM = 128, TN = 128, TK = 32;
+  constexpr int TM = 128, TN = 128, TK = NB;
   constexpr int LA = TM + 8, LB = TK + 4;
-  static_assert(NB % TK == 0, "K chunks");
-  __shared__ __align__(16) float sa[TK * LA];   // [k][m]
-  __shared__ __align__(16) float sb[TN * LB];   // [n][k]
+  extern __shared__ __align__(16) float gsm[];
+  float* sa = gsm;              // [k][m], -L21
+  float* sb = gsm + TK * LA;    // [n][k], U12
   const int64_t m0 = k + NB + (int64_t)blockIdx.x * TM;
   const int64_t n0 = k + NB + (int64_t)blockIdx.y * TN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  // the output tile goes into the accumulators first (its loads overlap the
+  // staging below) and the product is subtracted by staging -L21
   float acc[4][4][4];
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
+    for (int ni = 0; ni < 4; ++ni) {
+      const int64_t r0 = m0 + wm + mi * 16 + g, c0 = n0 + wn + ni * 8 + 2 * t;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.f;
-  for (int kc = 0; kc < NB; kc += TK) {
-    // L21 chunk: TK columns of TM rows
-    for (int e = threadIdx.x; e < TK * TM / 4; e += blockDim.x) {
-      const int c = e / (TM / 4), r4 = (e % (TM / 4)) * 4;
-      const int64_t gr = m0 + r4;
-      const float* src = A + gr + (k + kc + c) * lda;
-      float4 v;
-      if (vec4 && gr + 3 < R) {
-        v = *reinterpret_cast<const float4*>(src);
-      } else {
-        v.x = gr < R ? src[0] : 0.f;
-        v.y = gr + 1 < R ? src[1] : 0.f;
-        v.z = gr + 2 < R ? src[2] : 0.f;
-        v.w = gr + 3 < R ? src[3] : 0.f;
+      for (int e = 0; e < 4; ++e) {
+        const int64_t r = r0 + (e >> 1) * 8, c = c0 + (e & 1);
+        acc[mi][ni][e] = (r < R && c < R) ? A[r + c * lda] : 0.f;
       }
-      *reinterpret_cast<float4*>(&sa[c * LA + r4]) = v;
     }
-    // U12 chunk: TN columns of TK rows (rows k+kc.., always inside the matrix)
-    for (int e = threadIdx.x; e < TN * TK / 4; e += blockDim.x) {
-      const int n = e / (TK / 4), r4 = (e % (TK / 4)) * 4;
-      const int64_t gc = n0 + n;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (gc < R) {
-        const float* src = A + (k + kc + r4) + gc * lda;
-        if (vec4) v = *reinterpret_cast<const float4*>(src);
-        else v = make_float4(src[0], src[1], src[2], src[3]);
-      }
-      *reinterpret_cast<float4*>(&sb[n * LB + r4]) = v;
+  // -L21: TK columns of TM rows
+  for (int e = threadIdx.x; e < TK * TM / 4; e += blockDim.x) {
+    const int c = e / (TM / 4), r4 = (e % (TM / 4)) * 4;
+    const int64_t gr = m0 + r4;
+    const float* src = A + gr + (k + c) * lda;
+    float4 v;
+    if (vec4 && gr + 3 < R) {
+      v = *reinterpret_cast<const float4*>(src);
+    } else {
+      v.x = gr < R ? src[0] : 0.f;
+      v.y = gr + 1 < R ? src[1] : 0.f;
+      v.z = gr + 2 < R ? src[2] : 0.f;
+      v.w = gr + 3 < R ? src[3] : 0.f;
     }
-    __syncthreads();
+    *reinterpret_cast<float4*>(&sa[c * LA + r4]) = make_float4(-v.x, -v.y, -v.z, -v.w);
+  }
+  // U12: TN columns of TK rows (rows k.., always inside the matrix)
+  for (int e = threadIdx.x; e < TN * TK / 4; e += blockDim.x) {
+    const int n = e / (TK / 4), r4 = (e % (TK / 4)) * 4;
+    const int64_t gc = n0 + n;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (gc < R) {
+      const float* src = A + (k + r4) + gc * lda;
+      if (vec4) v = *reinterpret_cast<const float4*>(src);
+      else v = make_float4(src[0], src[1], src[2], src[3]);
+    }
+    *reinterpret_cast<float4*>(&sb[n * LB + r4]) = v;
+  }
+  __syncthreads();
 #pragma unroll
-    for (int ks = 0; ks < TK; ks += 8) {
-      uint32_t ah[4][4], al[4][4], bh[4][2], bl[4][2];
+  for (int ks = 0; ks < TK; ks += 8) {
+    uint32_t ah[4][4], al[4][4], bh[4][2], bl[4][2];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
-        const int mr = wm + mi * 16 + g;
-        const float v[4] = {sa[(ks + t) * LA + mr], sa[(ks + t) * LA + mr + 8], sa[(ks + t + 4) * LA + mr],
-                            sa[(ks + t + 4) * LA + mr + 8]};
+    for (int mi = 0; mi < 4; ++mi) {
+      const int mr = wm + mi * 16 + g;
+      const float v[4] = {sa[(ks + t) * LA + mr], sa[(ks + t) * LA + mr + 8], sa[(ks + t + 4) * LA + mr],
+                          sa[(ks + t + 4) * LA + mr + 8]};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          ah[mi][e] = tf32_bits(v[e]);
-          if constexpr (SPLIT) al[mi][e] = tf32_bits(v[e] - __uint_as_float(ah[mi][e]));
-        }
+      for (int e = 0; e < 4; ++e) {
+        ah[mi][e] = tf32_bits(v[e]);
+        if constexpr (SPLIT) al[mi][e] = tf32_bits(v[e] - __uint_as_float(ah[mi][e]));
       }
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+      const int nc = wn + ni * 8 + g;
+      const float v[2] = {sb[nc * LB + ks + t], sb[nc * LB + ks + t + 4]};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        bh[ni][e] = tf32_bits(v[e]);
+        if constexpr (SPLIT) bl[ni][e] = tf32_bits(v[e] - __uint_as_float(bh[ni][e]));
+      }
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
       for (int ni = 0; ni < 4; ++ni) {
-        const int nc = wn + ni * 8 + g;
-        const float v[2] = {sb[nc * LB + ks + t], sb[nc * LB + ks + t + 4]};
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          bh[ni][e] = tf32_bits(v[e]);
-          if constexpr (SPLIT) bl[ni][e] = tf32_bits(v[e] - __uint_as_float(bh[ni][e]));
+        if constexpr (SPLIT) {
+          mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
         }
+        mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
       }
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-          if constexpr (SPLIT) {
-            mma_tf32(acc[mi][ni], al[mi], bh[ni]);
-            mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
-          }
-          mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
-        }
-    }
-    __syncthreads();
   }
 #pragma unroll
   for (int mi = 0; mi < 4; ++mi)
@@ -403,10 +407,13 @@ __global__ void __launch_bounds__(256, 2) k_lu_gemm(float* __restrict__ A, int64
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int64_t r = r0 + (e >> 1) * 8, c = c0 + (e & 1);
-        if (r < R && c < R) A[r + c * lda] -= acc[mi][ni][e];
+        if (r < R && c < R) A[r + c * lda] = acc[mi][ni][e];
       }
     }
 }
+
+template <int NB>
+constexpr size_t lu_gemm_smem() { return sizeof(float) * ((size_t)NB * (128 + 8) + (size_t)128 * (NB + 4)); }
 
 // ---------------------------------------------------------------------------
 // solve L U x = P r for one right-hand side (in place in x):
@@ -545,6 +552,10 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
   const bool vec4 = (lda % 4 == 0) && (reinterpret_cast<uintptr_t>(s.LU) % 16 == 0);
   static const cudaError_t smem_attr =
       cudaFuncSetAttribute(k_lu_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBytes);
+  static const cudaError_t gemm_attr[2] = {
+      cudaFuncSetAttribute(k_lu_gemm<NB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_gemm_smem<NB>()),
+      cudaFuncSetAttribute(k_lu_gemm<NB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_gemm_smem<NB>())};
+  RF_CUDA_TRY(gemm_attr[split ? 1 : 0]);
   int dev = 0, num_sms = 148;
   RF_CUDA_TRY(cudaGetDevice(&dev));
   RF_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -576,8 +587,8 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
       }
       k_lu_trsm<NB><<<(unsigned)ceil_div(R - k - NB, 256), 256, 0, st>>>(s.LU, lda, R, k);
       dim3 g((unsigned)ceil_div(R - k - NB, 128), (unsigned)ceil_div(R - k - NB, 128));
-      if (split) k_lu_gemm<NB, true><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
-      else k_lu_gemm<NB, false><<<g, 256, 0, st>>>(s.LU, lda, R, k, vec4);
+      if (split) k_lu_gemm<NB, true><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
+      else k_lu_gemm<NB, false><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
       launches += 2;
     }
     RF_LAUNCH_CHECK();
