@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
+    ap.add_argument("--legs", default="headline,serving,direct",
+                    help="comma-separated subset of headline,serving,direct; a subset other than the default "
+                         "prints the requested legs only (for profiling one part)")
     return ap.parse_args()
 
 
@@ -508,6 +511,20 @@ def run_ours(args, dist):
         print(json.dumps(out), flush=True)
 
 
+def run_legs(args, dist):
+    """Only the legs named in --legs (no headline metric line)."""
+    import torch
+    torch.cuda.set_device(dist.local)
+    legs = set(args.legs.split(","))
+    out = {"legs": sorted(legs)}
+    if "serving" in legs:
+        out["serving"] = serve_ensemble(args, dist)
+    if "direct" in legs and dist.rank == 0:
+        out["direct_solver"] = direct_leg(args)
+    if dist.rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -517,7 +534,14 @@ def main():
         return
     dist = Dist(args.gpus)
     try:
-        run_ours(args, dist)
+        if "headline" in args.legs.split(","):
+            if "serving" not in args.legs.split(","):
+                args.serve_requests = 0
+            if "direct" not in args.legs.split(","):
+                args.direct_fibers = 0
+            run_ours(args, dist)
+        else:
+            run_legs(args, dist)
     finally:
         dist.close()
 
