@@ -166,6 +166,10 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
     // step jl still reads, so one barrier per step suffices after phase 2
     float* const sTflat = sTbase + (jl & 1) * (TI * S::TP);
     auto sT = [&](int tl, int k, int kj) -> float* { return sTflat + tl * S::TP + (k * K1 + kj) * 6; };
+    // structured storage keeps T as [value q][i] (the storage record's own
+    // order, so phase 3 is a straight copy); dense keeps [i][value]
+    constexpr bool QT = MODE != kAsmDense;
+    auto tv = [&](int tl, int q) -> float& { return QT ? sTflat[q * TI + tl] : sTflat[tl * S::TP + q]; };
     const bool pair_ok = unit_ok && (!diag || (SYM ? il < jl : il != jl));
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj] (numerical, mirror-
     // folded over qj) or the closed-form integral (analytical)
@@ -238,7 +242,7 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
         for (int k = 0; k < K1; ++k) acc[k] = fmaf((k & 1) ? od : ev, tab.W[k][q], acc[k]);
       }
 #pragma unroll
-      for (int k = 0; k < K1; ++k) sT(tl, k, kj)[c] = acc[k];
+      for (int k = 0; k < K1; ++k) tv(tl, (k * K1 + kj) * 6 + c) = acc[k];
     }
     __syncthreads();
 
@@ -302,28 +306,29 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
       const int sub = (I % S::SUB) * S::SUB + (J % S::SUB);
       const int64_t L16 = (int64_t)J16 * (J16 + 1) / 2 + I16;
       const int64_t rec = (L16 * S::SUB * S::SUB + sub) * TI + jl;
+      // T is already in the record order [q][tl]; pairs that do not exist
+      // (i >= N, i >= j on a diagonal tile) came out of phases 1-2 as exact zeros
       float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
-      for (int v = tid; v < S::NQ32 * TI; v += blockDim.x) {
-        const int tl = v % TI, q = v / TI;   // q is the flat (k, kj, c) index of the pair's T
-        const bool ok = (i0 + tl < N) && (!diag || tl < jl);
-        d32[v] = ok ? sTflat[tl * S::TP + q] : 0.f;
-      }
+      for (int v = tid; v < S::NQ32 * TI / 4; v += blockDim.x)
+        reinterpret_cast<float4*>(d32)[v] = reinterpret_cast<const float4*>(sTflat)[v];
       uint32_t* d16 = out.S16 + rec * (int64_t)(S::NQ16 * TI);
-      for (int v = tid; v < S::NQ16 * TI; v += blockDim.x) {
-        const int tl = v % TI, q2 = v / TI;
-        const bool ok = (i0 + tl < N) && (!diag || tl < jl);
-        float f[2];
+      for (int v = tid; v < S::NQ16 * (TI / 4); v += blockDim.x) {
+        const int q2 = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
+        const float4 a = *reinterpret_cast<const float4*>(&sTflat[sMap16[2 * q2] * TI + g4]);
+        const float4 b = *reinterpret_cast<const float4*>(&sTflat[sMap16[2 * q2 + 1] * TI + g4]);
+        const float lo[4] = {a.x, a.y, a.z, a.w}, hi[4] = {b.x, b.y, b.z, b.w};
+        uint32_t w[4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) f[h] = ok ? sTflat[tl * S::TP + sMap16[2 * q2 + h]] : 0.f;
-        uint32_t word;
-        if constexpr (MODE == kAsmStructF16) {
-          __half2 hv = __floats2half2_rn(f[0], f[1]);
-          word = *reinterpret_cast<uint32_t*>(&hv);
-        } else {
-          __nv_bfloat162 hv = __floats2bfloat162_rn(f[0], f[1]);
-          word = *reinterpret_cast<uint32_t*>(&hv);
+        for (int u = 0; u < 4; ++u) {
+          if constexpr (MODE == kAsmStructF16) {
+            __half2 hv = __floats2half2_rn(lo[u], hi[u]);
+            w[u] = *reinterpret_cast<uint32_t*>(&hv);
+          } else {
+            __nv_bfloat162 hv = __floats2bfloat162_rn(lo[u], hi[u]);
+            w[u] = *reinterpret_cast<uint32_t*>(&hv);
+          }
         }
-        d16[v] = word;
+        *reinterpret_cast<uint4*>(&d16[q2 * TI + g4]) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
     // ---- phase 3c: force terms F_i[k] += T^{ij}[k][P0] F/2 and
@@ -331,10 +336,10 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
     if (tid < TI * K1) {
       const int tl = tid / K1, k = tid % K1;
       if (i0 + tl < N && (!diag || (SYM ? tl < jl : tl != jl))) {
-        const float* T6 = sT(tl, k, 0);
-        facc[0] = fmaf(T6[4], fz, facc[0]);
-        facc[1] = fmaf(T6[5], fz, facc[1]);
-        facc[2] = fmaf(T6[2], fz, facc[2]);
+        const int q0 = (k * K1 + 0) * 6;
+        facc[0] = fmaf(tv(tl, q0 + 4), fz, facc[0]);
+        facc[1] = fmaf(tv(tl, q0 + 5), fz, facc[1]);
+        facc[2] = fmaf(tv(tl, q0 + 2), fz, facc[2]);
       }
     }
     if (SYM && tid < K1) {
@@ -342,10 +347,10 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
       float s[3] = {0.f, 0.f, 0.f};
       for (int tl = 0; tl < TI; ++tl) {
         if (i0 + tl >= N || (diag && tl >= jl)) continue;
-        const float* T6 = sT(tl, 0, kj);
-        s[0] = fmaf(T6[4], fz, s[0]);
-        s[1] = fmaf(T6[5], fz, s[1]);
-        s[2] = fmaf(T6[2], fz, s[2]);
+        const int q0 = (0 * K1 + kj) * 6;
+        s[0] = fmaf(tv(tl, q0 + 4), fz, s[0]);
+        s[1] = fmaf(tv(tl, q0 + 5), fz, s[1]);
+        s[2] = fmaf(tv(tl, q0 + 2), fz, s[2]);
       }
 #pragma unroll
       for (int a = 0; a < 3; ++a) sfJ[jl][3 * kj + a] += s[a];
