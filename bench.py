@@ -47,6 +47,7 @@ def parse():
                     help="suspensions in the served ensemble (0: skip the serving leg)")
     ap.add_argument("--serve-max-active", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-graphs", type=int, default=1, help="replay GMRES cycles from CUDA graphs (1) or not (0)")
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
     ap.add_argument("--legs", default="headline,serving,direct",
@@ -374,7 +375,7 @@ def serve_ensemble(args, dist):
     rng = np.random.default_rng(5 + dist.rank)
     gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
     dist.barrier()
-    with Server(max_active=args.serve_max_active) as srv:
+    with Server(max_active=args.serve_max_active, use_cuda_graphs=args.serve_graphs) as srv:
         t0 = time.perf_counter()
         due = t0
         for r, (p, o), c, g in zip(reqs, layouts, cfgs, gaps):
@@ -394,6 +395,7 @@ def serve_ensemble(args, dist):
             "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"],
             "fiber_steps_per_s": fiber_steps / wall_max, "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
             "max_active": args.serve_max_active, "peak_active": st["peak_active"],
+            "cuda_graphs": bool(args.serve_graphs),
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps in {0.01, 0.005}, 5-50 steps, volume fraction 1%, "
                         "M=5, 8x3 quadrature, Poisson arrivals; latency = host wall time of one rf_step "

@@ -103,6 +103,8 @@ typedef struct rf_stats {
   double ms_update_fibers;
   int64_t device_bytes;      /* device memory held by the handle */
   int kernel_launches;       /* kernels launched by the last rf_step */
+  int graph_replays;         /* GMRES restart cycles of the last solve run from a
+                                captured CUDA graph (0 while profiling is on) */
 } rf_stats;
 
 typedef struct rf_handle rf_handle;
@@ -174,6 +176,9 @@ int rf_get_stream(rf_handle* h, void** stream);
  * (launches issued after convergence return at once and are not counted)
  * and the summed milliseconds of all its matvec launches. */
 int rf_set_profiling(rf_handle* h, int enable);
+/* GMRES restart cycles are captured as CUDA graphs on their second use and
+ * replayed afterwards (default on; results are identical either way). */
+int rf_set_cuda_graphs(rf_handle* h, int enable);
 int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
 
 /* Device-pointer entry points (no host copies; pointers are device memory
@@ -214,6 +219,7 @@ typedef struct rf_server rf_server;
 typedef struct rf_server_config {
   int max_active;            /* requests running at once */
   int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
+  int use_cuda_graphs;       /* rf_set_cuda_graphs for every request's handle */
 } rf_server_config;
 
 typedef struct rf_request_stats {

@@ -55,6 +55,7 @@ class rf_stats(ctypes.Structure):
         ("ms_update_fibers", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int),
+        ("graph_replays", ctypes.c_int),
     ]
 
 
@@ -62,7 +63,7 @@ RF_REQ_QUEUED, RF_REQ_RUNNING, RF_REQ_DONE, RF_REQ_FAILED, RF_REQ_CANCELLED = ra
 
 
 class rf_server_config(ctypes.Structure):
-    _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64)]
+    _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64), ("use_cuda_graphs", ctypes.c_int)]
 
 
 class rf_request_stats(ctypes.Structure):
@@ -119,6 +120,7 @@ SIGNATURES = {
     "rf_operator_apply": (ctypes.c_int, [_H, _P, _P, ctypes.c_int]),
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_set_cuda_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "rf_checkpoint_bytes": (ctypes.c_int64, [_H]),
     "rf_checkpoint_save": (ctypes.c_int, [_H, _P, ctypes.c_int64]),

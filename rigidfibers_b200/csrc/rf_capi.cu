@@ -167,6 +167,8 @@ struct rf_handle {
   int refinements = 0;
   int restart = 10;          // Krylov dimension per cycle
   int64_t steps_taken = 0;   // completed rf_update_fibers calls (checkpoint metadata)
+  GmresGraphCache gmres_graphs;   // captured restart cycles (GMRES)
+  bool use_graphs = true;
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -192,6 +194,7 @@ struct rf_handle {
     return RF_OK;
   }
   ~rf_handle() {
+    gmres_graphs.release();
     for (auto e : mv_events) cudaEventDestroy(e);
     for (void* p : allocations) cudaFreeAsync(p, st);
     if (st) cudaStreamSynchronize(st);
@@ -504,6 +507,7 @@ int rf_solve(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("rf_solve before rf_assemble"); return RF_E_STATE; }
   RF_CUDA_TRY(cudaEventRecord(h->ev[2], h->st));
+  h->stats.graph_replays = 0;
   GmresSetup s;
   s.R = h->R;
   s.m = h->restart;
@@ -521,6 +525,9 @@ int rf_solve(rf_handle* h) {
   s.ctl = h->ctl;
   s.host_ctl = h->host_ctl;
   s.coop_blocks = h->coop_blocks;
+  // per-matvec profiling events are recorded by the callbacks, so profiling runs
+  // launch every cycle directly; otherwise the cycles replay captured graphs
+  s.graphs = (h->profile || !h->use_graphs) ? nullptr : &h->gmres_graphs;
   h->mv_used = 0;
   int mv_launches = 0;
   MatvecFn mv = [h, &mv_launches](const float* xin, const int* skip, cudaStream_t st) -> int {
@@ -594,12 +601,12 @@ int rf_solve(rf_handle* h) {
   int rc;
   if (h->mixed) {
     ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
-      h->refinements += 1;
       return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
                                       h->b, r, skip, st);
     };
     h->refinements = 0;
     rc = gmres_solve_ex(s, mv, resid, h->b, h->x64, true, h->st, &res);
+    h->refinements = res.residual_calls;
     if (rc == RF_OK || rc == RF_E_NOCONV) {
       int rc2 = launch_cast_to_float(h->x64, h->x, h->R, h->st);
       if (rc2) return rc2;
@@ -616,6 +623,7 @@ int rf_solve(rf_handle* h) {
   h->stats.restarts = res.restarts;
   h->stats.refinement_steps = h->mixed ? h->refinements : 0;
   h->stats.relative_residual = res.relative_residual;
+  h->stats.graph_replays = res.graph_replays;
   if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
   h->solved = true;
   return rc;
@@ -907,6 +915,12 @@ int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* st
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
   h->assembled = h->solved = false;
   if (steps_taken) *steps_taken = c.steps_taken;
+  return RF_OK;
+}
+
+int rf_set_cuda_graphs(rf_handle* h, int enable) {
+  if (!h) return RF_E_INPUT;
+  h->use_graphs = enable != 0;
   return RF_OK;
 }
 

@@ -16,6 +16,8 @@
 //    kernel reads first), so the host never waits per iteration.
 #include <cooperative_groups.h>
 
+#include <vector>
+
 #include "rf_common.cuh"
 #include "rf_krylov.cuh"
 
@@ -385,6 +387,14 @@ void set_coop_block_cap(int cap) { t_coop_cap = cap; }
 
 int coop_blocks_per_sm_capped(int num_sms) { return t_coop_cap > 0 ? std::min(num_sms, t_coop_cap) : num_sms; }
 
+void GmresGraphCache::release() {
+  for (int v = 0; v < 2; ++v) {
+    if (exec[v]) cudaGraphExecDestroy(exec[v]);
+    exec[v] = nullptr;
+    state[v] = 0;
+  }
+}
+
 int krylov_coop_blocks(int64_t R, int num_sms) {
   // 256-thread blocks; at most 2 per SM (always co-resident), fewer for small systems
   int want = (int)ceil_div(R, 256 * 4);
@@ -442,25 +452,19 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   }
   res->launches = 2;
   GmresCtl h{};
-  int x_zero = 1;
   int cycles_run = 0;
-  for (int cycle = 0;; ++cycle) {
-    ++cycles_run;
-    int mode = x_zero ? 0 : 1;
-    if (!x_zero) {
-      int rc;
-      if (residual) {
-        rc = residual(x, s.V, &s.ctl->converged, st);
-        mode = 2;
-      } else {
-        rc = matvec(static_cast<const float*>(x), &s.ctl->converged, st);
-      }
+  // one restart cycle: [residual of x], residual kernel, m x (matvec + Arnoldi step), update
+  auto enqueue_cycle = [&](bool first) -> int {
+    int mode = 0;
+    if (!first) {
+      const int rc = residual ? residual(x, s.V, &s.ctl->converged, st)
+                              : matvec(static_cast<const float*>(x), &s.ctl->converged, st);
       if (rc) return rc;
-      ++res->launches;
+      mode = residual ? 2 : 1;
     }
     {
       void* args[] = {&a, &mode};
-      int rc = coop_launch((const void*)k_gmres_residual, nblk, 256, args, st);
+      const int rc = coop_launch((const void*)k_gmres_residual, nblk, 256, args, st);
       if (rc) return rc;
     }
     for (int j = 0; j < m; ++j) {
@@ -472,15 +476,72 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
     }
     k_gmres_update<<<nblk, 256, 0, st>>>(a);
     RF_LAUNCH_CHECK();
-    res->launches += 2 + m;
+    return RF_OK;
+  };
+  for (int cycle = 0;; ++cycle) {
+    ++cycles_run;
+    const bool first = cycle == 0;
+    const int v = first ? 0 : 1;
+    bool from_graph = false;
+    GmresGraphCache* gc = s.graphs;
+    if (gc && gc->state[v] == 2) {
+      // capture this cycle once (the capture does not run it; the replay below
+      // does).  A variant is captured on its second use, so the kernels' one-time
+      // set-up (function attributes) has run outside any capture.
+      cudaGraph_t graph = nullptr;
+      int rc = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? RF_OK : RF_E_CUDA;
+      if (rc == RF_OK) {
+        rc = enqueue_cycle(first);
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        if (rc == RF_OK && ec == cudaSuccess && graph &&
+            cudaGraphInstantiate(&gc->exec[v], graph, 0) == cudaSuccess) {
+          size_t n = 0;
+          cudaGraphGetNodes(graph, nullptr, &n);
+          std::vector<cudaGraphNode_t> nodes(n);
+          if (n) cudaGraphGetNodes(graph, nodes.data(), &n);
+          int kn = 0;
+          for (auto nd : nodes) {
+            cudaGraphNodeType ty;
+            if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++kn;
+          }
+          gc->kernels[v] = kn;
+          gc->state[v] = 1;
+        } else {
+          gc->exec[v] = nullptr;
+          gc->state[v] = -1;
+        }
+        if (graph) cudaGraphDestroy(graph);
+      } else {
+        gc->state[v] = -1;
+      }
+      cudaGetLastError();   // a refused capture leaves no sticky error; clear the non-sticky one
+      if (gc->state[v] == 1) {
+        // the callbacks counted their kernels while capturing; count ours as a direct cycle does
+        res->launches += 2 + m + (first ? 0 : 1);
+        RF_CUDA_TRY(cudaGraphLaunch(gc->exec[v], st));
+        from_graph = true;
+      }
+    } else if (gc && gc->state[v] == 1) {
+      RF_CUDA_TRY(cudaGraphLaunch(gc->exec[v], st));
+      res->launches += gc->kernels[v];
+      from_graph = true;
+    }
+    if (from_graph) {
+      ++res->graph_replays;
+    } else {
+      const int rc = enqueue_cycle(first);
+      if (rc) return rc;
+      res->launches += 2 + m + (first ? 0 : 1);
+      if (gc && gc->state[v] == 0) gc->state[v] = 2;
+    }
     RF_CUDA_TRY(cudaMemcpyAsync(s.host_ctl, s.ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, st));
     RF_CUDA_TRY(cudaStreamSynchronize(st));
     h = *s.host_ctl;
-    x_zero = 0;
     if (h.converged || h.nan || h.timeout) break;
     if (h.total_iters >= s.maxit && cycle > 0 && h.jconv == 0) break;
     if (cycle > s.maxit + 2) break;
   }
+  res->residual_calls = residual ? cycles_run - 1 : 0;
   res->iterations = h.total_iters;
   res->restarts = h.restarts;
   res->matvecs = h.total_iters + (cycles_run - 1);

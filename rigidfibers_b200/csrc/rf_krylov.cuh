@@ -31,6 +31,20 @@ using MatvecFn = std::function<int(const float* x, const int* skip, cudaStream_t
 // operator / accumulation than the matvec's.
 using ResidualFn = std::function<int(const void* x, float* r, const int* skip, cudaStream_t st)>;
 
+// A restart cycle of GMRES captured as a CUDA graph: [0] the first cycle
+// (x = 0), [1] the later ones (residual of the current x first).  Kernel
+// arguments and buffers are fixed per handle and the tolerance / iteration
+// limit live in the device control block, so a replay is exactly the launch
+// sequence it was captured from.  state: 0 not run yet, 2 run once directly
+// (captured on the next use), 1 ready, -1 capture not possible here (the cycle
+// is then launched directly).
+struct GmresGraphCache {
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int state[2] = {0, 0};
+  int kernels[2] = {0, 0};   // kernel nodes per replay
+  void release();
+};
+
 struct GmresSetup {
   int64_t R;
   int m;               // restart length
@@ -48,6 +62,7 @@ struct GmresSetup {
   GmresCtl* ctl;       // device
   GmresCtl* host_ctl;  // pinned host
   int coop_blocks;
+  GmresGraphCache* graphs = nullptr;   // null: launch every cycle directly
 };
 
 struct GmresResult {
@@ -56,6 +71,8 @@ struct GmresResult {
   double relative_residual = 0.0;
   int launches = 0;       // kernels launched (matvec launches counted by the caller's MatvecFn)
   int matvecs = 0;        // matvecs that did work (launches after convergence return at once)
+  int residual_calls = 0; // calls of the ResidualFn (cycles after the first)
+  int graph_replays = 0;  // cycles run from a captured graph
 };
 
 int krylov_coop_blocks(int64_t R, int num_sms);

@@ -84,6 +84,7 @@ static void run_request(rf_server* s, Request* r) {
   int rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
   std::vector<double> lat;
   if (rc == RF_OK) {
+    rf_set_cuda_graphs(h, s->cfg.use_cuda_graphs);
     for (int t = 0; t < r->nsteps; ++t) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -164,6 +165,7 @@ int rf_server_config_default(rf_server_config* c) {
   if (!c) return RF_E_INPUT;
   std::memset(c, 0, sizeof(*c));
   c->max_active = 16;
+  c->use_cuda_graphs = 1;
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c->hbm_budget_bytes = (int64_t)(0.8 * (double)fr);
   else c->hbm_budget_bytes = (int64_t)64 << 30;

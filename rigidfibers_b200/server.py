@@ -33,7 +33,7 @@ def device_bytes(config, number_of_fibers):
 
 
 class Server:
-    def __init__(self, max_active=None, hbm_budget_bytes=None):
+    def __init__(self, max_active=None, hbm_budget_bytes=None, use_cuda_graphs=None):
         self._lib = C.load()
         sc = C.rf_server_config()
         C.check(self._lib.rf_server_config_default(ctypes.byref(sc)), "rf_server_config_default")
@@ -41,6 +41,8 @@ class Server:
             sc.max_active = int(max_active)
         if hbm_budget_bytes is not None:
             sc.hbm_budget_bytes = int(hbm_budget_bytes)
+        if use_cuda_graphs is not None:
+            sc.use_cuda_graphs = int(bool(use_cuda_graphs))
         self.max_active = sc.max_active
         self.hbm_budget_bytes = sc.hbm_budget_bytes
         s = ctypes.c_void_p()
