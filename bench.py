@@ -266,6 +266,7 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
     stream = torch.cuda.ExternalStream(sp.value)
     for t in range(args.warmup):
         sim.step(t)
+    tuned = sim.autotune()          # matvec launch choice, timed on this operator
     lib.rf_set_profiling(sim._h, 1)
     dist.barrier()
     torch.cuda.synchronize()
@@ -297,6 +298,7 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
     dist.barrier()
     acc["ms"] = e0.elapsed_time(e1)
     acc["device_bytes"] = sim.stats()["device_bytes"]
+    acc["autotune"] = tuned
     sim.close()
     return acc
 
@@ -460,7 +462,8 @@ def run_ours(args, dist):
                       "ms_per_step": plain_ms / args.steps,
                       "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
                       "gmres_iterations_per_step": plain["iters"] / args.steps,
-                      "matvec_ms": plain["mv_ms"] / max(plain["mv_launches"], 1)}
+                      "matvec_ms": plain["mv_ms"] / max(plain["mv_launches"], 1),
+                      "autotune": plain["autotune"]}
 
     hbm, peak_kind = peaks()
     mvn = max(head["mv_launches"], 1)
@@ -495,6 +498,7 @@ def run_ours(args, dist):
         "roofline": roof, "clocks": head["clocks"],
         "e2e": {"value": e2e_value, "unit": "fiber-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": head["launches"],
+        "autotune": head["autotune"],
     }
     if args.serve_requests > 0:
         out["serving"] = serve_ensemble(args, dist)

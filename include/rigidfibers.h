@@ -176,6 +176,24 @@ int rf_get_stream(rf_handle* h, void** stream);
  * (launches issued after convergence return at once and are not counted)
  * and the summed milliseconds of all its matvec launches. */
 int rf_set_profiling(rf_handle* h, int enable);
+/* Autotuning of launch choices that leave the method unchanged: the 16-bit
+ * structured matvec kernel (matvec_variant 0 = TMA-staged, 2 = register-staged;
+ * matvec_ms[0], [1] their times) in mixed precision, the column splits of the
+ * dense FP32 matvec (gemv_ctas_per_sm of 2, 4, 8, 16; gemv_ms[] their times,
+ * -1 when not tried) in FP32.  Call after rf_assemble; times each candidate with
+ * CUDA events on the assembled operator, keeps the fastest for this handle and
+ * caches it per (device, precision, M, N) for later calls (cached = 1).  The
+ * summation order, hence the last bits of the solution, follow the choice.
+ * (The reference compiles one kernel variant per run, runner/cuda_runner.py:49-117.) */
+typedef struct rf_tune_report {
+  int matvec_variant;
+  double matvec_ms[2];
+  int gemv_ctas_per_sm;
+  double gemv_ms[4];
+  int cached;
+} rf_tune_report;
+int rf_autotune(rf_handle* h, rf_tune_report* report);
+
 /* GMRES restart cycles are captured as CUDA graphs on their second use and
  * replayed afterwards (default on; results are identical either way). */
 int rf_set_cuda_graphs(rf_handle* h, int enable);

@@ -59,6 +59,16 @@ class rf_stats(ctypes.Structure):
     ]
 
 
+class rf_tune_report(ctypes.Structure):
+    _fields_ = [
+        ("matvec_variant", ctypes.c_int),
+        ("matvec_ms", ctypes.c_double * 2),
+        ("gemv_ctas_per_sm", ctypes.c_int),
+        ("gemv_ms", ctypes.c_double * 4),
+        ("cached", ctypes.c_int),
+    ]
+
+
 RF_REQ_QUEUED, RF_REQ_RUNNING, RF_REQ_DONE, RF_REQ_FAILED, RF_REQ_CANCELLED = range(5)
 
 
@@ -121,6 +131,7 @@ SIGNATURES = {
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_cuda_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_autotune": (ctypes.c_int, [_H, ctypes.POINTER(rf_tune_report)]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "rf_checkpoint_bytes": (ctypes.c_int64, [_H]),
     "rf_checkpoint_save": (ctypes.c_int, [_H, _P, ctypes.c_int64]),

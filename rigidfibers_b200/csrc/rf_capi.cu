@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -169,6 +171,8 @@ struct rf_handle {
   int64_t steps_taken = 0;   // completed rf_update_fibers calls (checkpoint metadata)
   GmresGraphCache gmres_graphs;   // captured restart cycles (GMRES)
   bool use_graphs = true;
+  int mv_variant = 0;             // structured matvec kernel (rf_autotune)
+  int64_t ypart_floats = 0;       // capacity of ypart
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
   std::vector<void*> allocations;
@@ -332,6 +336,8 @@ int rf_set_state(rf_handle* h, const double* pos, const double* ori) {
 
 // Every device buffer of a handle.  With h->dry set nothing is allocated and
 // h->device_bytes is the exact footprint (admission control of the server).
+constexpr int kTuneMaxCtasPerSm = 16;
+
 static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   const int64_t R = h->R;
   const int N = h->N;
@@ -375,7 +381,10 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   h->coop_blocks = krylov_coop_blocks(R, h->num_sms);
   const int64_t ldv = ceil_div(R, 32) * 32;
   if (!rc) rc = h->alloc((void**)&h->V, (size_t)(m + 1) * (size_t)ldv * sizeof(float));
-  if (!rc) rc = h->alloc((void**)&h->ypart, (size_t)h->gemv_plan.splits * (size_t)R * sizeof(float));
+  // room for the most column splits rf_autotune tries
+  h->ypart_floats = (int64_t)(h->mixed ? 1 : plan_dense_gemv(R, h->num_sms, kTuneMaxCtasPerSm).splits) * R;
+  h->ypart_floats = std::max<int64_t>(h->ypart_floats, (int64_t)h->gemv_plan.splits * R);
+  if (!rc) rc = h->alloc((void**)&h->ypart, (size_t)h->ypart_floats * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->part, (size_t)3 * h->coop_blocks * (kMaxRestart + 2) * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->H, (size_t)(m + 1) * m * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->cs, (size_t)m * sizeof(double));
@@ -548,7 +557,7 @@ int rf_solve(rf_handle* h) {
     if (h->mixed) {
       const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
       rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
-                                &h->ctl->timeout, st);
+                                &h->ctl->timeout, st, h->mv_variant);
       mv_launches += 2;
     } else {
       rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
@@ -915,6 +924,104 @@ int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* st
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
   h->assembled = h->solved = false;
   if (steps_taken) *steps_taken = c.steps_taken;
+  return RF_OK;
+}
+
+// ---- autotuning ----------------------------------------------------------
+// The matvec of the Krylov solve has launch choices that do not change the
+// method: the 16-bit structured kernel (TMA-staged or register-staged) and the
+// number of column splits of the dense FP32 kernel.  rf_autotune times each
+// candidate with CUDA events on this handle's assembled operator and keeps the
+// fastest; the choice is cached per (device, precision, M, N).
+namespace {
+struct TuneKey {
+  int dev, prec, M, N;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, prec, M, N) < std::tie(o.dev, o.prec, o.M, o.N);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, rf_tune_report> g_tune_cache;
+}  // namespace
+
+static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
+  if (h->mixed) {
+    h->mv_variant = t.matvec_variant;
+  } else {
+    h->gemv_plan = plan_dense_gemv(h->R, h->num_sms, t.gemv_ctas_per_sm);
+  }
+  h->gmres_graphs.release();   // the captured cycles hold the old launch parameters
+}
+
+int rf_autotune(rf_handle* h, rf_tune_report* out) {
+  if (!h) return RF_E_INPUT;
+  if (!h->assembled) { set_last_error_str("rf_autotune needs an assembled system (rf_assemble)"); return RF_E_STATE; }
+  const TuneKey key{h->dev, h->cfg.precision, h->M, h->N};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      apply_tuning(h, it->second);
+      if (out) { *out = it->second; out->cached = 1; }
+      return RF_OK;
+    }
+  }
+  rf_tune_report t;
+  std::memset(&t, 0, sizeof(t));
+  const int64_t R = h->R;
+  const float* xin = h->b;                            // any vector of the right size
+  float* y = h->V + ceil_div(R, 32) * 32;             // Krylov basis as scratch (the handle is idle)
+  cudaEvent_t e0 = h->ev[2], e1 = h->ev[3];
+  auto time_it = [&](auto&& launch, double* ms) -> int {
+    for (int r = 0; r < 2; ++r) RF_TRY(launch());
+    RF_CUDA_TRY(cudaEventRecord(e0, h->st));
+    const int reps = 8;
+    for (int r = 0; r < reps; ++r) RF_TRY(launch());
+    RF_CUDA_TRY(cudaEventRecord(e1, h->st));
+    RF_CUDA_TRY(cudaEventSynchronize(e1));
+    float f = 0.f;
+    RF_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
+    *ms = f / reps;
+    return RF_OK;
+  };
+  if (h->mixed) {
+    const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+    RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
+    double best = 1e30;
+    for (int v = 0; v < 2; ++v) {
+      const int variant = v == 0 ? 0 : 2;
+      double ms = 0;
+      RF_TRY(time_it([&]() {
+        return launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, y, nullptr,
+                                    &h->ctl->timeout, h->st, variant);
+      }, &ms));
+      t.matvec_ms[v] = ms;
+      if (ms < best) { best = ms; t.matvec_variant = variant; }
+    }
+    int timeout = 0;
+    RF_CUDA_TRY(cudaMemcpyAsync(&timeout, &h->ctl->timeout, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    if (timeout) { set_last_error_str("rf_autotune: a bounded device-side wait timed out"); return RF_E_TIMEOUT; }
+    t.gemv_ctas_per_sm = 0;
+  } else {
+    const int cand[4] = {2, 4, 8, 16};
+    double best = 1e30;
+    for (int c = 0; c < 4; ++c) {
+      const DenseGemvPlan p = plan_dense_gemv(R, h->num_sms, cand[c]);
+      if ((int64_t)p.splits * R > h->ypart_floats) { t.gemv_ms[c] = -1; continue; }
+      double ms = 0;
+      RF_TRY(time_it([&]() { return launch_dense_gemv(p, h->A, h->lda, R, xin, h->ypart, nullptr, h->st); }, &ms));
+      t.gemv_ms[c] = ms;
+      if (ms < best) { best = ms; t.gemv_ctas_per_sm = cand[c]; }
+    }
+    t.matvec_variant = 0;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = t;
+  }
+  apply_tuning(h, t);
+  if (out) *out = t;
   return RF_OK;
 }
 

@@ -35,9 +35,11 @@ int64_t struct_words16(int M, int N);
 // zpart: (ceil(N/16) + 1) x R floats.
 // err: device word set to 1 if a bounded wait inside the kernel gave up (may be null:
 // then the register-staged kernel is used)
+// variant: 0 the TMA-staged kernel where it is built (M <= 5, Q = 24, 16 bit, err
+// given), else the register-staged one; 2 always the register-staged one.
 int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
-                         cudaStream_t st);
+                         cudaStream_t st, int variant = 0);
 // r = b - A x with the FP32 blocks, x and accumulation in FP64; zpart64: (ceil(N/16) + 1) x R doubles.
 int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
                              double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st);

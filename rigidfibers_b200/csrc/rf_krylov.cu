@@ -76,11 +76,11 @@ k_gemv_cm_f32(const float* __restrict__ A, int64_t lda, int64_t R, const float* 
   }
 }
 
-DenseGemvPlan plan_dense_gemv(int64_t R, int num_sms) {
+DenseGemvPlan plan_dense_gemv(int64_t R, int num_sms, int ctas_per_sm) {
   DenseGemvPlan p;
   p.row_blocks = (int)ceil_div(R, 1024);
-  // about 8 CTAs of 256 threads per SM in flight
-  int splits = (int)ceil_div((int64_t)num_sms * 8, p.row_blocks);
+  // about ctas_per_sm CTAs of 256 threads per SM in flight
+  int splits = (int)ceil_div((int64_t)num_sms * ctas_per_sm, p.row_blocks);
   splits = std::max(1, std::min<int>(splits, (int)ceil_div(R, 64)));
   p.cps = ceil_div(R, splits);
   p.splits = (int)ceil_div(R, p.cps);

@@ -139,7 +139,7 @@ struct DenseGemvPlan {
   int splits;
   int64_t cps;  // columns per split
 };
-DenseGemvPlan plan_dense_gemv(int64_t R, int num_sms);
+DenseGemvPlan plan_dense_gemv(int64_t R, int num_sms, int ctas_per_sm = 8);
 int launch_dense_gemv(const DenseGemvPlan& p, const float* A, int64_t lda, int64_t R, const float* x, float* ypart,
                       const int* skip, cudaStream_t st);
 

@@ -678,9 +678,9 @@ static int launch_z16_bulk(int N, const uint32_t* S16, const float* x, float* zp
 
 int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, const uint32_t* S16,
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
-                         cudaStream_t st) {
+                         cudaStream_t st, int variant) {
   int rc = RF_E_UNSUPPORTED;
-  if (tab.Q == 24 && smode != 0 && err != nullptr && tab.M <= 5) {
+  if (variant != 2 && tab.Q == 24 && smode != 0 && err != nullptr && tab.M <= 5) {
     // tiles staged by TMA bulk copies (two 3072*M-byte tiles per SM fit in shared memory for M <= 5)
     switch (tab.M) {
       case 1: rc = smode == 1 ? launch_z16_bulk<1, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<1, 2>(N, S16, x, zpart, skip, err, st); break;

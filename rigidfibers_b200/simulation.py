@@ -172,6 +172,18 @@ class Simulation:
         C.check(self._lib.rf_operator_apply(self._h, C.ptr(xx), C.ptr(y), int(which)), "rf_operator_apply")
         return y
 
+    def autotune(self):
+        """Time the matvec launch choices on the assembled operator and keep the
+        fastest (rf_autotune); assembles first if needed."""
+        t = C.rf_tune_report()
+        rc = self._lib.rf_autotune(self._h, ctypes.byref(t))
+        if rc == C.RF_E_STATE:
+            self.assembleSystem()
+            rc = self._lib.rf_autotune(self._h, ctypes.byref(t))
+        C.check(rc, "rf_autotune")
+        return {"matvec_variant": t.matvec_variant, "matvec_ms": list(t.matvec_ms),
+                "gemv_ctas_per_sm": t.gemv_ctas_per_sm, "gemv_ms": list(t.gemv_ms), "cached": bool(t.cached)}
+
     # -- checkpoint / resume ---------------------------------------------------
     def checkpoint(self):
         """The run's resumable state as bytes (rf_checkpoint_save)."""

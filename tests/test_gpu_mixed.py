@@ -100,3 +100,28 @@ def test_mixed_requires_numerical_integration():
     with pytest.raises(RigidFibersError) as e:
         _sim(pos, ori, precision="mixed_fp16", integration="analytical")
     assert e.value.status == C.RF_E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("prec", ["fp32", "mixed_fp16"])
+def test_autotune_keeps_the_solution(prec):
+    """rf_autotune times the matvec launch choices and keeps the fastest; the
+    solution stays within 1e-5 of the untuned one (only the summation order of
+    the matvec changes) and a second call is served from the cache."""
+    from rigidfibers_b200 import Config, Simulation
+    pos, ori = sphere_layout(80, 4.0, seed=31)
+    ref = Simulation(Config(precision=prec), pos, ori)
+    ref.run(2)
+    p0, o0 = ref.state()
+    ref.close()
+    sim = Simulation(Config(precision=prec), pos, ori)
+    rep = sim.autotune()
+    if prec == "fp32":
+        assert rep["gemv_ctas_per_sm"] in (2, 4, 8, 16)
+        assert min(v for v in rep["gemv_ms"] if v > 0) > 0
+    else:
+        assert rep["matvec_variant"] in (0, 2) and min(rep["matvec_ms"]) > 0
+    sim.run(2)
+    p1, o1 = sim.state()
+    assert _rel(p1, p0) <= 1e-5 and _rel(o1, o0) <= 1e-5
+    again = Simulation(Config(precision=prec), pos, ori)
+    assert again.autotune()["cached"]
