@@ -71,46 +71,58 @@ def workload_name(args):
 # distributed plumbing (replicas only)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self, want):
+    """One process per GPU (torchrun env); replicas, no collective on the data
+    path: only the barrier around the timed region and the max / sum of the
+    per-rank results.  NCCL on GPUs, gloo on the host (tests)."""
+
+    def __init__(self, want, backend=None):
         self.rank = int(os.environ.get("RANK", "0"))
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.dev = "cuda"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            self.dev = "cuda" if backend == "nccl" else "cpu"
+            if self.dev == "cuda":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.pg = dist
+
+    def _reduce(self, v, op):
+        import torch
+        t = torch.tensor([float(v)], device=self.dev, dtype=torch.float64)
+        self.pg.all_reduce(t, op=op)
+        return float(t.item())
 
     def barrier(self):
         if self.pg:
             import torch
-            t = torch.zeros(1, device="cuda")
-            self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            self._reduce(0.0, self.pg.ReduceOp.SUM)
+            if self.dev == "cuda":
+                torch.cuda.synchronize()
 
     def max(self, v):
-        if not self.pg:
-            return v
-        import torch
-        t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
+        return self._reduce(v, self.pg.ReduceOp.MAX) if self.pg else v
 
     def sum(self, v):
-        if not self.pg:
-            return v
-        import torch
-        t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
-        self.pg.all_reduce(t)
-        return float(t.item())
+        return self._reduce(v, self.pg.ReduceOp.SUM) if self.pg else v
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def whole_job_rate(dist, local_ms, local_units):
+    """(slowest rank's ms, units of all ranks, units per second of the whole job)."""
+    ms_max = dist.max(local_ms)
+    total = dist.sum(local_units)
+    return ms_max, total, total / (ms_max / 1000.0)
 
 
 # ---------------------------------------------------------------------------
@@ -444,9 +456,7 @@ def run_ours(args, dist):
     precision = "mixed_fp16" if args.precision == "auto" else args.precision
     cfg = Config(precision=precision, refinement_restart=args.mixed_restart)
     head = time_path(args, dist, cfg, pos, ori, clocks=Clocks(dist.local))
-    ms_max = dist.max(head["ms"])
-    total_fiber_steps = dist.sum(N * args.steps)
-    value = total_fiber_steps / (ms_max / 1000.0)
+    ms_max, total_fiber_steps, value = whole_job_rate(dist, head["ms"], N * args.steps)
     e2e_s = e2e_path(args, dist, cfg, pos, ori)
     e2e_value = total_fiber_steps / e2e_s
     # bytes the C ABI moves per step: rf_set_state uploads double4 prev+cur
@@ -476,8 +486,14 @@ def run_ours(args, dist):
                   "TMA bulk-copy pipeline, GMRES)")
         bytes_per_matvec = 2.0 * 150 * N * (N - 1) / 2
     achieved = bytes_per_matvec / (mv_avg_ms / 1000.0) / 1e9 if head["mv_launches"] else None
+    # DRAM traffic per launch from one ncu capture of the same kernel at N=1500
+    # (dram__bytes_read.sum 343.2 MB + dram__bytes_write.sum 7.3 MB for 1124250
+    # unordered pairs, profiles/struct_z16_bulk_N1500.md), scaled by the pairs
+    # one launch processes; not captured for the dense FP32 kernel
+    traffic = 350.5e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision != "fp32" else None
     roof = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
+            "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+            "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
             "algorithmic_bytes_per_launch": bytes_per_matvec, "avg_launch_ms": mv_avg_ms,
             "launches": head["mv_launches"], "share_of_step_time": head["mv_ms"] / head["ms"] if head["ms"] else None}
     out = {
