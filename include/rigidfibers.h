@@ -105,6 +105,8 @@ typedef struct rf_stats {
   int kernel_launches;       /* kernels launched by the last rf_step */
   int graph_replays;         /* GMRES restart cycles of the last solve run from a
                                 captured CUDA graph (0 while profiling is on) */
+  int factorizations;        /* direct solver: 1 = TF32 tensor-core factors refined,
+                                2 = refactored with the 3xTF32 split update */
 } rf_stats;
 
 typedef struct rf_handle rf_handle;

@@ -56,6 +56,7 @@ class rf_stats(ctypes.Structure):
         ("device_bytes", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int),
         ("graph_replays", ctypes.c_int),
+        ("factorizations", ctypes.c_int),
     ]
 
 

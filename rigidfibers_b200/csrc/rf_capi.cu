@@ -574,6 +574,7 @@ int rf_solve(rf_handle* h) {
     h->stats.iterations = 0;
     h->stats.restarts = 0;
     h->stats.refinement_steps = lr.refinement_steps;
+    h->stats.factorizations = lr.factorizations;
     h->stats.relative_residual = lr.relative_residual;
     if (lrc != RF_OK && lrc != RF_E_NOCONV) return lrc;
     h->solved = true;
@@ -769,6 +770,7 @@ int rf_last_stats(rf_handle* h, rf_stats* s) {
   if (!h || !s) return RF_E_INPUT;
   *s = h->stats;
   s->device_bytes = h->device_bytes;
+  s->kernel_launches = h->launches;   // since the last rf_step began (or the handle was created)
   return RF_OK;
 }
 

@@ -412,6 +412,186 @@ __global__ void __launch_bounds__(256, 1) k_lu_gemm(float* __restrict__ A, int64
     }
 }
 
+// ---------------------------------------------------------------------------
+// The TF32 trailing update with the 5th-generation tensor cores: tcgen05.mma
+// (kind::tf32, M = 128, N = 128, K = 8 per instruction) reading both operands
+// from shared memory through matrix descriptors and accumulating in tensor
+// memory.  One 128x128 output tile per CTA of 4 warps:
+//  * all threads stage -L21 (128 x 64) and U12 (64 x 128) into the canonical
+//    non-swizzled K-major layout (core matrices of 8 rows x 4 k = 16 bytes per
+//    row: [k-chunk][row-group][8 rows][4 k]), rounding to TF32 on the way:
+//    U12 with 16-byte loads (k is contiguous), L21 with 4-byte loads that are
+//    coalesced over its m-contiguous columns (TF32 operands in the MN-major
+//    form left the accumulator untouched on this part, so both are K-major);
+//  * one thread issues the 8 MMAs (K = 64) into a 128-column accumulator and
+//    commits them to an mbarrier, which all threads wait on (bounded);
+//  * the epilogue reads the accumulator rows (thread = row = TMEM lane) 32
+//    columns at a time and adds them to C (-L21 U12), coalesced per column.
+// 64 KB of shared memory per CTA keeps at most 3 CTAs (384 TMEM columns) on an
+// SM, so the allocation never waits.  A timed-out wait records -1 in *info.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lu_smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// mbarrier wait (phase parity) bounded in time: non-blocking test_wait polled
+// for at most one second of %globaltimer; false on timeout
+__device__ __forceinline__ bool lu_mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(lu_smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 1000000000ull) return false;
+  }
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // start address, leading / stride byte offsets (16-byte units), version 1,
+  // base offset 0, no swizzle
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128, 1) k_lu_gemm_tc(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
+                                                       bool vec4, int* __restrict__ info) {
+  constexpr int TM = 128, TN = 128;
+  static_assert(NB == 64, "the staging below is written for a 64-column panel");
+  constexpr uint32_t kABytes = TM * NB * 4, kBBytes = TN * NB * 4;
+  constexpr uint32_t kAKChunk = (TM / 8) * 128;   // bytes per k-chunk of 4 (A)
+  constexpr uint32_t kBKChunk = (TN / 8) * 128;   // bytes per k-chunk of 4 (B)
+  constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                              ((uint32_t)(TM >> 4) << 24);   // F32 accum, TF32 A and B, both K-major
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  float* sA = reinterpret_cast<float*>(tsm);
+  float* sB = reinterpret_cast<float*>(tsm + kABytes);
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t m0 = k + NB + (int64_t)blockIdx.x * TM;
+  const int64_t n0 = k + NB + (int64_t)blockIdx.y * TN;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(lu_smem_u32(&s_tmem)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(lu_smem_u32(&bar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // -L21: 4 consecutive k of row m (4-byte loads, coalesced over m across the
+  // warp) -> A[kc][mg][mr][0..3]
+  for (int e = tid; e < TM * NB / 4; e += blockDim.x) {
+    const int m = e % TM, kc = e / TM;
+    const int64_t gr = m0 + m;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (gr < R) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = A[gr + (k + 4 * kc + i) * lda];
+    }
+    const float4 t = make_float4(__uint_as_float(tf32_bits(-v[0])), __uint_as_float(tf32_bits(-v[1])),
+                                 __uint_as_float(tf32_bits(-v[2])), __uint_as_float(tf32_bits(-v[3])));
+    *reinterpret_cast<float4*>(&sA[((kc * (TM / 8) + (m >> 3)) * 8 + (m & 7)) * 4]) = t;
+  }
+  // U12: float4 of 4 consecutive k of column n -> B[kc][ng][nr][0..3]
+  for (int e = tid; e < TN * NB / 4; e += blockDim.x) {
+    const int n = e / (NB / 4), r4 = (e % (NB / 4)) * 4;
+    const int64_t gc = n0 + n;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (gc < R) {
+      const float* src = A + (k + r4) + gc * lda;
+      if (vec4) v = *reinterpret_cast<const float4*>(src);
+      else v = make_float4(src[0], src[1], src[2], src[3]);
+    }
+    const float4 t = make_float4(__uint_as_float(tf32_bits(v.x)), __uint_as_float(tf32_bits(v.y)),
+                                 __uint_as_float(tf32_bits(v.z)), __uint_as_float(tf32_bits(v.w)));
+    *reinterpret_cast<float4*>(&sB[(((r4 >> 2) * (TN / 8) + (n >> 3)) * 8 + (n & 7)) * 4]) = t;
+  }
+  // generic-proxy stores -> tensor-core (async proxy) reads
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  if (tid == 0) {
+    const uint32_t a0 = lu_smem_u32(sA), b0 = lu_smem_u32(sB);
+#pragma unroll
+    for (int g = 0; g < NB / 8; ++g) {
+      const uint64_t da = umma_desc(a0 + 2 * g * kAKChunk, kAKChunk, 128);
+      const uint64_t db = umma_desc(b0 + 2 * g * kBKChunk, kBKChunk, 128);
+      const uint32_t acc = g > 0 ? 1u : 0u;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+          "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     lu_smem_u32(&bar))
+                 : "memory");
+  }
+  bool ok = lu_mbar_wait(&bar, 0);
+  const bool all_ok = __syncthreads_and(ok) != 0;
+  if (!all_ok) {
+    if (tid == 0) {
+      atomicCAS(info, 0, -1);
+      (void)lu_mbar_wait(&bar, 0);   // let the issued MMAs drain (bounded) before freeing
+    }
+    __syncthreads();
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = tid;                      // TMEM lane = accumulator row
+    const int64_t gr = m0 + row;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int cc = 0; cc < TN; cc += 32) {
+      float cv[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int64_t gc = n0 + cc + j;
+        cv[j] = (gr < R && gc < R) ? A[gr + gc * lda] : 0.f;
+      }
+      uint32_t d[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+            "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+            "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]),
+            "=r"(d[23]), "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]),
+            "=r"(d[30]), "=r"(d[31])
+          : "r"(lane_addr + (uint32_t)cc));
+      // the registers are valid only after wait::ld: tie them to it so that no
+      // use is scheduled before
+      asm volatile("tcgen05.wait::ld.sync.aligned;"
+                   : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7]),
+                     "+r"(d[8]), "+r"(d[9]), "+r"(d[10]), "+r"(d[11]), "+r"(d[12]), "+r"(d[13]), "+r"(d[14]),
+                     "+r"(d[15]), "+r"(d[16]), "+r"(d[17]), "+r"(d[18]), "+r"(d[19]), "+r"(d[20]), "+r"(d[21]),
+                     "+r"(d[22]), "+r"(d[23]), "+r"(d[24]), "+r"(d[25]), "+r"(d[26]), "+r"(d[27]), "+r"(d[28]),
+                     "+r"(d[29]), "+r"(d[30]), "+r"(d[31])
+                   :
+                   : "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int64_t gc = n0 + cc + j;
+        if (gr < R && gc < R) A[gr + gc * lda] = cv[j] + __uint_as_float(d[j]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+  }
+}
+
 template <int NB>
 constexpr size_t lu_gemm_smem() { return sizeof(float) * ((size_t)NB * (128 + 8) + (size_t)128 * (NB + 4)); }
 
@@ -556,6 +736,9 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
       cudaFuncSetAttribute(k_lu_gemm<NB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_gemm_smem<NB>()),
       cudaFuncSetAttribute(k_lu_gemm<NB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_gemm_smem<NB>())};
   RF_CUDA_TRY(gemm_attr[split ? 1 : 0]);
+  constexpr int kTcSmem = 2 * 128 * NB * 4;
+  static const cudaError_t tc_attr =
+      cudaFuncSetAttribute(k_lu_gemm_tc<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
   int dev = 0, num_sms = 148;
   RF_CUDA_TRY(cudaGetDevice(&dev));
   RF_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -587,8 +770,13 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
       }
       k_lu_trsm<NB><<<(unsigned)ceil_div(R - k - NB, 256), 256, 0, st>>>(s.LU, lda, R, k);
       dim3 g((unsigned)ceil_div(R - k - NB, 128), (unsigned)ceil_div(R - k - NB, 128));
-      if (split) k_lu_gemm<NB, true><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
-      else k_lu_gemm<NB, false><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
+      if (split) {
+        k_lu_gemm<NB, true><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
+      } else if (tc_attr == cudaSuccess) {
+        k_lu_gemm_tc<NB><<<g, 128, kTcSmem, st>>>(s.LU, lda, R, k, vec4, s.info);
+      } else {
+        k_lu_gemm<NB, false><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
+      }
       launches += 2;
     }
     RF_LAUNCH_CHECK();
@@ -598,6 +786,10 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
   RF_CUDA_TRY(cudaMemcpyAsync(s.host_ipiv, s.ipiv, R * sizeof(int), cudaMemcpyDeviceToHost, st));
   RF_CUDA_TRY(cudaStreamSynchronize(st));
   *launches_out += launches;
+  if (info < 0) {
+    set_last_error_str("lu: a bounded device-side wait timed out");
+    return RF_E_TIMEOUT;
+  }
   if (info != 0) {
     set_last_error_str("lu: zero pivot");
     return RF_E_SINGULAR;
@@ -621,9 +813,11 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 4096);
   int launches = 0, steps = 0;
   double rel = 0.0;
+  int factorizations = 0;
   for (int pass = 0; pass < 2; ++pass) {
     const bool split = pass == 1;
     RF_TRY_RF(lu_factor(s, A, split, st, &launches));
+    ++factorizations;
     // x0 = (LU)^{-1} P b, then refine: r = b - A x (FP64), d = (LU)^{-1} P r
     RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, b, s.d, st));
     k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 1);
@@ -655,6 +849,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   res->refinement_steps = steps;
   res->relative_residual = rel;
   res->launches = launches;
+  res->factorizations = factorizations;
   return rel <= s.tol ? RF_OK : RF_E_NOCONV;
 }
 

@@ -28,6 +28,7 @@ struct LuSetup {
 
 struct LuResult {
   int refinement_steps = 0;
+  int factorizations = 0;   // 2 when the TF32 factors stalled and the split update was used
   int launches = 0;
   double relative_residual = 0.0;
 };

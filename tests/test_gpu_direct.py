@@ -39,7 +39,10 @@ def test_golden_direct(golden, integ):
         for f, k in FIELDS:
             ref = golden["%s_direct/%d_%s" % (integ, t, f)]
             assert _rel(got[k], ref) <= 1e-5, (t, f, _rel(got[k], ref))
-        assert sim.stats()["relative_residual"] <= 1e-6
+        st = sim.stats()
+        assert st["relative_residual"] <= 1e-6
+        # the TF32 tensor-core factors alone suffice for these systems
+        assert st["factorizations"] == 1 and st["refinement_steps"] <= 4
 
 
 def _lu_solve(A, b, tol=1e-7):
