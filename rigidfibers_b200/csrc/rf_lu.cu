@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(256, 1) k_lu_gemm(float* __restrict__ A, int64
 //    form left the accumulator untouched on this part, so both are K-major);
 //  * one thread issues the 8 MMAs (K = 64) into a 128-column accumulator and
 //    commits them to an mbarrier, which all threads wait on (bounded);
-//  * the epilogue reads the accumulator rows (thread = row = TMEM lane) 32
+//  * the epilogue reads the accumulator rows (thread = row = TMEM lane) 16
 //    columns at a time and adds them to C (-L21 U12), coalesced per column.
 // 64 KB of shared memory per CTA keeps at most 3 CTAs (384 TMEM columns) on an
 // SM, so the allocation never waits.  A timed-out wait records -1 in *info.
@@ -460,7 +460,7 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 template <int NB>
-__global__ void __launch_bounds__(128, 1) k_lu_gemm_tc(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
+__global__ void __launch_bounds__(128, 3) k_lu_gemm_tc(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
                                                        bool vec4, int* __restrict__ info) {
   constexpr int TM = 128, TN = 128;
   static_assert(NB == 64, "the staging below is written for a 64-column panel");
@@ -550,35 +550,30 @@ __global__ void __launch_bounds__(128, 1) k_lu_gemm_tc(float* __restrict__ A, in
     const int64_t gr = m0 + row;
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-    for (int cc = 0; cc < TN; cc += 32) {
-      float cv[32];
+    for (int cc = 0; cc < TN; cc += 16) {
+      float cv[16];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
+      for (int j = 0; j < 16; ++j) {
         const int64_t gc = n0 + cc + j;
         cv[j] = (gr < R && gc < R) ? A[gr + gc * lda] : 0.f;
       }
-      uint32_t d[32];
+      uint32_t d[16];
       asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
           : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-            "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
-            "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]),
-            "=r"(d[23]), "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]),
-            "=r"(d[30]), "=r"(d[31])
+            "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
           : "r"(lane_addr + (uint32_t)cc));
       // the registers are valid only after wait::ld: tie them to it so that no
       // use is scheduled before
       asm volatile("tcgen05.wait::ld.sync.aligned;"
                    : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3]), "+r"(d[4]), "+r"(d[5]), "+r"(d[6]), "+r"(d[7]),
                      "+r"(d[8]), "+r"(d[9]), "+r"(d[10]), "+r"(d[11]), "+r"(d[12]), "+r"(d[13]), "+r"(d[14]),
-                     "+r"(d[15]), "+r"(d[16]), "+r"(d[17]), "+r"(d[18]), "+r"(d[19]), "+r"(d[20]), "+r"(d[21]),
-                     "+r"(d[22]), "+r"(d[23]), "+r"(d[24]), "+r"(d[25]), "+r"(d[26]), "+r"(d[27]), "+r"(d[28]),
-                     "+r"(d[29]), "+r"(d[30]), "+r"(d[31])
+                     "+r"(d[15])
                    :
                    : "memory");
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
+      for (int j = 0; j < 16; ++j) {
         const int64_t gc = n0 + cc + j;
         if (gr < R && gc < R) A[gr + gc * lda] = cv[j] + __uint_as_float(d[j]);
       }
