@@ -430,6 +430,7 @@ def direct_leg(args):
     for solver in ("direct", "gmres"):
         sim = Simulation(Config(solver=solver, integration="analytical"), pos, ori)
         sim.step(0)                      # warm-up (first-touch of the kernels)
+        tuned = sim.autotune()
         sim.assembleSystem()
         sim.solveSystem()
         st = sim.stats()
@@ -437,7 +438,7 @@ def direct_leg(args):
         R = 15 * n
         leg = {"ms_solve": st["ms_solve_system"], "ms_assemble": st["ms_assemble_system"],
                "relative_residual": st["relative_residual"], "iterations": st["iterations"],
-               "refinements": st["refinement_steps"]}
+               "refinements": st["refinement_steps"], "autotune": tuned}
         if solver == "direct":
             leg["tflops"] = (2.0 / 3.0) * R ** 3 / (st["ms_solve_system"] / 1e3) / 1e12
         out[solver] = leg

@@ -193,6 +193,9 @@ typedef struct rf_tune_report {
   int gemv_ctas_per_sm;
   double gemv_ms[4];
   int cached;
+  int panel_blocks;         /* direct solver: blocks of the LU panel kernel (one
+                               grid sync per column): SMs, SMs/2, SMs/4 tried */
+  double panel_ms[3];       /* first panel's time per candidate (-1: rows do not fit) */
 } rf_tune_report;
 int rf_autotune(rf_handle* h, rf_tune_report* report);
 

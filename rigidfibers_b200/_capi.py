@@ -67,6 +67,8 @@ class rf_tune_report(ctypes.Structure):
         ("gemv_ctas_per_sm", ctypes.c_int),
         ("gemv_ms", ctypes.c_double * 4),
         ("cached", ctypes.c_int),
+        ("panel_blocks", ctypes.c_int),
+        ("panel_ms", ctypes.c_double * 3),
     ]
 
 

@@ -947,6 +947,7 @@ std::map<TuneKey, rf_tune_report> g_tune_cache;
 }  // namespace
 
 static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
+  if (h->cfg.solver == RF_SOLVER_DIRECT && t.panel_blocks > 0) h->lu.panel_blocks = t.panel_blocks;
   if (h->mixed) {
     h->mv_variant = t.matvec_variant;
   } else {
@@ -958,7 +959,7 @@ static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
 int rf_autotune(rf_handle* h, rf_tune_report* out) {
   if (!h) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("rf_autotune needs an assembled system (rf_assemble)"); return RF_E_STATE; }
-  const TuneKey key{h->dev, h->cfg.precision, h->M, h->N};
+  const TuneKey key{h->dev, h->cfg.precision * 4 + h->cfg.solver, h->M, h->N};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -1017,6 +1018,20 @@ int rf_autotune(rf_handle* h, rf_tune_report* out) {
       if (ms < best) { best = ms; t.gemv_ctas_per_sm = cand[c]; }
     }
     t.matvec_variant = 0;
+  }
+  if (h->cfg.solver == RF_SOLVER_DIRECT) {
+    // LU panel: fewer blocks make each grid sync cheaper but give each block
+    // more rows (they must fit in shared memory); time the first panel
+    const int cand[3] = {h->num_sms, std::max(1, h->num_sms / 2), std::max(1, h->num_sms / 4)};
+    double best = 1e30;
+    for (int c = 0; c < 3; ++c) {
+      float ms = 0.f;
+      const int rc = lu_time_panel(h->lu, h->A, cand[c], h->st, e0, e1, &ms);
+      if (rc == RF_E_UNSUPPORTED) { t.panel_ms[c] = -1; continue; }
+      RF_TRY(rc);
+      t.panel_ms[c] = ms;
+      if (ms < best) { best = ms; t.panel_blocks = cand[c]; }
+    }
   }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -741,8 +741,9 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
     const int nb = (int)std::min<int64_t>(NB, R - k);
     // shared-memory panel: one block per SM at most (its rows of the panel
     // fit in kPanelSmemBytes); the global-memory panel otherwise
+    const int want = s.panel_blocks > 0 ? s.panel_blocks : num_sms;
     const int sm_blocks = (int)std::max<int64_t>(
-        1, std::min<int64_t>(std::min<int64_t>((int64_t)s.coop_blocks, (int64_t)num_sms), ceil_div(R - k, 32)));
+        1, std::min<int64_t>(std::min<int64_t>((int64_t)s.coop_blocks, (int64_t)want), ceil_div(R - k, 32)));
     const int rows_per = (int)ceil_div(R - k, sm_blocks);
     const size_t psmem = (size_t)rows_per * nb * sizeof(float);
     if (smem_attr == cudaSuccess && psmem <= (size_t)kPanelSmemBytes) {
@@ -796,6 +797,32 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
     if (p != j) std::swap(s.host_perm[j], s.host_perm[p]);
   }
   RF_CUDA_TRY(cudaMemcpyAsync(s.perm, s.host_perm, R * sizeof(int), cudaMemcpyHostToDevice, st));
+  return RF_OK;
+}
+
+int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
+                  float* ms) {
+  const int64_t R = s.R, lda = s.lda, k = 0;
+  const int nb = (int)std::min<int64_t>(64, R);
+  static const cudaError_t smem_attr =
+      cudaFuncSetAttribute(k_lu_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBytes);
+  RF_CUDA_TRY(smem_attr);
+  const int nblk0 = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::min(blocks, s.coop_blocks),
+                                                                ceil_div(R - k, 32)));
+  const int rows_per = (int)ceil_div(R - k, nblk0);
+  const size_t psmem = (size_t)rows_per * nb * sizeof(float);
+  if (psmem > (size_t)kPanelSmemBytes) return RF_E_UNSUPPORTED;
+  const int nblk = (int)ceil_div(R - k, rows_per);
+  RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, lda * sizeof(float), R * sizeof(float), R,
+                                cudaMemcpyDeviceToDevice, st));
+  RF_CUDA_TRY(cudaMemsetAsync(s.info, 0, sizeof(int), st));
+  PanelSmArgs pa{s.LU, lda, R, k, nb, rows_per, s.ipiv, s.pmax, s.pidx, s.prow, s.jrow, s.info};
+  void* args[] = {&pa};
+  RF_CUDA_TRY(cudaEventRecord(e0, st));
+  RF_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_lu_panel_smem, dim3(nblk), dim3(256), args, psmem, st));
+  RF_CUDA_TRY(cudaEventRecord(e1, st));
+  RF_CUDA_TRY(cudaEventSynchronize(e1));
+  RF_CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
   return RF_OK;
 }
 

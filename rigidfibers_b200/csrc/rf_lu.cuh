@@ -24,6 +24,7 @@ struct LuSetup {
   double tol;         // refinement target on ||b - A x|| / ||b||
   int max_refine;
   int coop_blocks;
+  int panel_blocks = 0;   // blocks of the shared-memory panel kernel (0: one per SM)
 };
 
 struct LuResult {
@@ -35,5 +36,9 @@ struct LuResult {
 
 // Factor A (column-major, lda) into s.LU and solve A x = b with refinement.
 int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res);
+// Time the first panel factorisation (k = 0) of A with `blocks` panel blocks
+// (A is copied into s.LU first); RF_E_UNSUPPORTED if the rows do not fit.
+int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
+                  float* ms);
 
 }  // namespace rf

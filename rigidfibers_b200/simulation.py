@@ -182,7 +182,8 @@ class Simulation:
             rc = self._lib.rf_autotune(self._h, ctypes.byref(t))
         C.check(rc, "rf_autotune")
         return {"matvec_variant": t.matvec_variant, "matvec_ms": list(t.matvec_ms),
-                "gemv_ctas_per_sm": t.gemv_ctas_per_sm, "gemv_ms": list(t.gemv_ms), "cached": bool(t.cached)}
+                "gemv_ctas_per_sm": t.gemv_ctas_per_sm, "gemv_ms": list(t.gemv_ms), "cached": bool(t.cached),
+                "panel_blocks": t.panel_blocks, "panel_ms": list(t.panel_ms)}
 
     # -- checkpoint / resume ---------------------------------------------------
     def checkpoint(self):
