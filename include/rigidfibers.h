@@ -283,6 +283,16 @@ int rf_server_get_stats(rf_server* s, rf_server_stats* stats);
 /* Cancels what has not finished, waits for running steps, frees everything. */
 int rf_server_destroy(rf_server* s);
 
+/* Fault injection for tests (no counterpart in the reference, which prints and
+ * continues).  rf_debug_set_device_wait_limit(0) makes the first bounded
+ * device-side wait of the TMA-pipelined matvec and of the tensor-core LU
+ * update give up at once, so the calls return RF_E_TIMEOUT and the handle stays
+ * usable; -1 restores the limits (2^24 polls, one second).
+ * rf_debug_fail_allocation_after(n): the n-th device allocation of rf_create
+ * from now on fails (RF_E_OOM); -1 disables. */
+int rf_debug_set_device_wait_limit(int64_t limit);
+int rf_debug_fail_allocation_after(int n);
+
 const char* rf_status_string(int status);
 const char* rf_last_error(void);
 

@@ -151,6 +151,8 @@ SIGNATURES = {
     "rf_server_result": (ctypes.c_int, [_S, ctypes.c_int64, _P, _P, _P, _P, ctypes.POINTER(rf_request_stats)]),
     "rf_server_get_stats": (ctypes.c_int, [_S, ctypes.POINTER(rf_server_stats)]),
     "rf_server_destroy": (ctypes.c_int, [_S]),
+    "rf_debug_set_device_wait_limit": (ctypes.c_int, [ctypes.c_int64]),
+    "rf_debug_fail_allocation_after": (ctypes.c_int, [ctypes.c_int]),
     "rf_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "rf_last_error": (ctypes.c_char_p, []),
 }

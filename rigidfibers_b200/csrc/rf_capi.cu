@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -16,6 +17,8 @@
 #include "rf_krylov.cuh"
 #include "rf_lu.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace rf {
 
 static thread_local std::string g_last_error;
@@ -24,6 +27,10 @@ void set_last_error(const char* msg, const char* file, int line) {
   g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
 }
 void set_last_error_str(const char* msg) { g_last_error = msg; }
+
+static std::atomic<int64_t> g_wait_limit{-1};
+static std::atomic<int> g_fail_alloc_after{-1};
+int64_t device_wait_limit() { return g_wait_limit.load(); }
 
 bool mq_supported(int M, int Q) {
 #define RF_MQ_CASE(MM, QQ) \
@@ -139,6 +146,7 @@ struct rf_handle {
   float* ffpart = nullptr;   // force-term partials
   float* F = nullptr;        // force terms sum_j T^{ij}[k][P0] F/2
   float* svpart = nullptr;   // structured velocity partials
+  int* vflag = nullptr;      // set when a velocity is not finite
   // Krylov scratch
   float* V = nullptr;
   float* ypart = nullptr;
@@ -186,6 +194,14 @@ struct rf_handle {
       *p = nullptr;
       device_bytes += (int64_t)bytes;
       return RF_OK;
+    }
+    // fault injection: the n-th allocation from now fails (tests)
+    int left = g_fail_alloc_after.load();
+    while (left >= 0 && !g_fail_alloc_after.compare_exchange_weak(left, left - 1)) {}
+    if (left == 0) {
+      *p = nullptr;
+      set_last_error_str("device allocation failed (injected)");
+      return RF_E_OOM;
     }
     cudaError_t e = cudaMallocAsync(p, bytes, st);
     if (e != cudaSuccess) {
@@ -422,6 +438,7 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   // velocities
   if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
   if (!rc) rc = h->alloc((void**)&h->vpart, (size_t)velocity_chunks(N) * N * 6 * sizeof(float));
+  if (!rc) rc = h->alloc((void**)&h->vflag, sizeof(int));
   return rc;
 }
 
@@ -536,7 +553,8 @@ int rf_solve(rf_handle* h) {
   s.coop_blocks = h->coop_blocks;
   // per-matvec profiling events are recorded by the callbacks, so profiling runs
   // launch every cycle directly; otherwise the cycles replay captured graphs
-  s.graphs = (h->profile || !h->use_graphs) ? nullptr : &h->gmres_graphs;
+  // (an injected device-wait limit is a kernel argument: no capture or replay then)
+  s.graphs = (h->profile || !h->use_graphs || device_wait_limit() >= 0) ? nullptr : &h->gmres_graphs;
   h->mv_used = 0;
   int mv_launches = 0;
   MatvecFn mv = [h, &mv_launches](const float* xin, const int* skip, cudaStream_t st) -> int {
@@ -657,6 +675,9 @@ int rf_update_velocities(rf_handle* h) {
                                      h->rv[h->vcur], h->st));
     h->launches += 3;
   }
+  // non-finite guard on the new velocities (read by rf_step after its sync)
+  RF_TRY(launch_check_finite(h->tv[h->vcur], h->rv[h->vcur], h->N, h->vflag, h->st));
+  h->launches += 1;
   RF_CUDA_TRY(cudaEventRecord(h->ev[5], h->st));
   h->vlast = h->vcur;
   return RF_OK;
@@ -686,12 +707,37 @@ int rf_update_fibers(rf_handle* h, int first_step) {
 int rf_step(rf_handle* h, int t) {
   if (!h) return RF_E_INPUT;
   h->launches = 0;
-  RF_TRY(rf_assemble(h));
-  int rc = rf_solve(h);
+  // NVTX ranges with the reference's step names (src/performance.cc)
+  struct Range {
+    explicit Range(const char* n) { nvtxRangePushA(n); }
+    ~Range() { nvtxRangePop(); }
+  };
+  Range step_range("rf_step");
+  int rc;
+  {
+    Range r("assemble_system");
+    RF_TRY(rf_assemble(h));
+  }
+  {
+    Range r("solve_system");
+    rc = rf_solve(h);
+  }
   if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
-  RF_TRY(rf_update_velocities(h));
-  RF_TRY(rf_update_fibers(h, t == 0));
+  {
+    Range r("update_velocities");
+    RF_TRY(rf_update_velocities(h));
+  }
+  {
+    Range r("update_fibers");
+    RF_TRY(rf_update_fibers(h, t == 0));
+  }
+  int vbad = 0;
+  RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (vbad) {
+    set_last_error_str("non-finite velocity");
+    return RF_E_NAN;
+  }
   h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
   h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
   h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
@@ -1042,6 +1088,18 @@ int rf_autotune(rf_handle* h, rf_tune_report* out) {
   return RF_OK;
 }
 
+int rf_debug_set_device_wait_limit(int64_t limit) {
+  if (limit < -1) return RF_E_INPUT;
+  g_wait_limit.store(limit);
+  return RF_OK;
+}
+
+int rf_debug_fail_allocation_after(int n) {
+  if (n < -1) return RF_E_INPUT;
+  g_fail_alloc_after.store(n);
+  return RF_OK;
+}
+
 int rf_set_cuda_graphs(rf_handle* h, int enable) {
   if (!h) return RF_E_INPUT;
   h->use_graphs = enable != 0;
@@ -1084,6 +1142,14 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
   L.coop_blocks = std::max(krylov_coop_blocks(R, sms), coop_blocks_per_sm_capped(sms));
   std::vector<void*> mem;
   auto get = [&](void** p, size_t bytes) -> int {
+    // fault injection: the n-th allocation from now fails (tests)
+    int left = g_fail_alloc_after.load();
+    while (left >= 0 && !g_fail_alloc_after.compare_exchange_weak(left, left - 1)) {}
+    if (left == 0) {
+      *p = nullptr;
+      set_last_error_str("device allocation failed (injected)");
+      return RF_E_OOM;
+    }
     cudaError_t e = cudaMallocAsync(p, bytes, st);
     if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return RF_E_OOM; }
     mem.push_back(*p);

@@ -52,6 +52,11 @@ struct Tables {
 
 void set_last_error(const char* msg, const char* file, int line);
 void set_last_error_str(const char* msg);
+// Fault injection (tests): limit of the first bounded device-side wait of the
+// TMA and tensor-core kernels (polls for the TMA pipeline, nanoseconds for the
+// tensor-core commit); -1 keeps the defaults.  Waits that drain in-flight work
+// after a failure always use the defaults.
+int64_t device_wait_limit();
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

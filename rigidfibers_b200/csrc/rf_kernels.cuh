@@ -56,6 +56,7 @@ int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t s
 namespace rf {
 int velocity_chunks(int N);
 // fw: N*Q float4 scratch; vpart: velocity_chunks(N) * N * 6 floats scratch.
+int launch_check_finite(const float4* a, const float4* b, int N, int* flag, cudaStream_t st);
 int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
                               float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 // analytical inner integrals (FP64 moments); vpart as for the numerical kernel

@@ -434,8 +434,8 @@ __device__ __forceinline__ uint32_t lu_smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 // mbarrier wait (phase parity) bounded in time: non-blocking test_wait polled
-// for at most one second of %globaltimer; false on timeout
-__device__ __forceinline__ bool lu_mbar_wait(uint64_t* bar, uint32_t parity) {
+// for at most limit_ns of %globaltimer (one second by default); false on timeout
+__device__ __forceinline__ bool lu_mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = 1000000000ull) {
   uint64_t t0;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
   for (;;) {
@@ -448,7 +448,7 @@ __device__ __forceinline__ bool lu_mbar_wait(uint64_t* bar, uint32_t parity) {
     if (done) return true;
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    if (t - t0 > 1000000000ull) return false;
+    if (t - t0 > limit_ns) return false;
   }
 }
 
@@ -461,7 +461,7 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 
 template <int NB>
 __global__ void __launch_bounds__(128, 3) k_lu_gemm_tc(float* __restrict__ A, int64_t lda, int64_t R, int64_t k,
-                                                       bool vec4, int* __restrict__ info) {
+                                                       bool vec4, int* __restrict__ info, uint64_t wait_ns) {
   constexpr int TM = 128, TN = 128;
   static_assert(NB == 64, "the staging below is written for a 64-column panel");
   constexpr uint32_t kABytes = TM * NB * 4, kBBytes = TN * NB * 4;
@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(128, 3) k_lu_gemm_tc(float* __restrict__ A, in
                      lu_smem_u32(&bar))
                  : "memory");
   }
-  bool ok = lu_mbar_wait(&bar, 0);
+  bool ok = lu_mbar_wait(&bar, 0, wait_ns);
   const bool all_ok = __syncthreads_and(ok) != 0;
   if (!all_ok) {
     if (tid == 0) {
@@ -734,6 +734,8 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
   constexpr int kTcSmem = 2 * 128 * NB * 4;
   static const cudaError_t tc_attr =
       cudaFuncSetAttribute(k_lu_gemm_tc<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+  const int64_t lim = device_wait_limit();
+  const uint64_t wait_ns = lim < 0 ? 1000000000ull : (uint64_t)lim;
   int dev = 0, num_sms = 148;
   RF_CUDA_TRY(cudaGetDevice(&dev));
   RF_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -769,7 +771,7 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
       if (split) {
         k_lu_gemm<NB, true><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
       } else if (tc_attr == cudaSuccess) {
-        k_lu_gemm_tc<NB><<<g, 128, kTcSmem, st>>>(s.LU, lda, R, k, vec4, s.info);
+        k_lu_gemm_tc<NB><<<g, 128, kTcSmem, st>>>(s.LU, lda, R, k, vec4, s.info, wait_ns);
       } else {
         k_lu_gemm<NB, false><<<g, 256, lu_gemm_smem<NB>(), st>>>(s.LU, lda, R, k, vec4);
       }

@@ -295,8 +295,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // bounded wait; returns false on timeout
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 24); ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t polls = (1u << 24)) {
+  for (uint32_t it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -327,7 +327,7 @@ struct BulkShape {
 template <int M, int SMODE>
 __global__ void __launch_bounds__(512, 1)
 k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restrict__ x, float* __restrict__ zpart,
-                  const int* __restrict__ skip, int* __restrict__ err) {
+                  const int* __restrict__ skip, int* __restrict__ err, uint32_t wait_polls) {
   constexpr int TI = 8, M3 = 3 * M;
   using B = BulkShape<M>;
   using RL = RowLoader<M, TI, SMODE>;
@@ -386,7 +386,7 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     tile_pair16(L, I16, J16);
     const bool diag = I16 == J16;
     const float xnext = xval(L + gridDim.x);   // in flight while this tile is computed
-    const bool ok_wait = mbar_wait_bounded(&bar[s], parity);
+    const bool ok_wait = mbar_wait_bounded(&bar[s], parity, wait_polls);
     if (__syncthreads_or(!ok_wait)) {
       failed = true;
       break;
@@ -671,7 +671,9 @@ static int launch_z16_bulk(int N, const uint32_t* S16, const float* x, float* zp
   RF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int64_t ntiles = struct_store_tiles(N);
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
-  k_struct_z16_bulk<M, SMODE><<<grid, B::kThreads, B::kBytes, st>>>(N, S16, x, zpart, skip, err);
+  const int64_t lim = device_wait_limit();
+  const uint32_t polls = lim < 0 ? (1u << 24) : (uint32_t)std::min<int64_t>(lim, 1 << 24);
+  k_struct_z16_bulk<M, SMODE><<<grid, B::kThreads, B::kBytes, st>>>(N, S16, x, zpart, skip, err, polls);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }

@@ -223,6 +223,23 @@ int velocity_chunks(int N) {
   return chunks;
 }
 
+// flag = 1 if any component of a or b (N float4, xyz used) is not finite
+__global__ void k_check_finite(const float4* __restrict__ a, const float4* __restrict__ b, int N,
+                               int* __restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float4 u = a[i], w = b[i];
+    const bool ok = isfinite(u.x) && isfinite(u.y) && isfinite(u.z) && isfinite(w.x) && isfinite(w.y) && isfinite(w.z);
+    if (!ok) *flag = 1;   // every writer stores the same value
+  }
+}
+
+int launch_check_finite(const float4* a, const float4* b, int N, int* flag, cudaStream_t st) {
+  RF_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), st));
+  k_check_finite<<<(unsigned)std::min<int64_t>(ceil_div(N, 256), 592), 256, 0, st>>>(a, b, N, flag);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
 int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
                               float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
   const int Q = tab.Q;
