@@ -28,6 +28,7 @@ Outputs (same formats as the reference):
 """
 import argparse
 import csv
+import json
 import math
 import os
 import sys
@@ -73,9 +74,13 @@ def run(args):
     sim = Simulation(make_config(params, args), pos, ori)
     steps = params["NUMBER_OF_TIMESTEPS"]
     ssi, vsi = params["STATE_SAVE_INTERVAL"], params["VELOCITY_SAVE_INTERVAL"]
+    log = open(args.json_log, "w") if getattr(args, "json_log", None) else None
     t0 = time.time()
     for t in range(steps):
         sim.step(t)
+        if log is not None:
+            log.write(step_record(t, sim.N, sim.stats()) + "\n")
+            log.flush()
         if ssi > 0 and t % ssi == 0:
             p, o = sim.state()
             F.write_fibers(_out(args, "XcT_res_%05d.out" % (t + 1)), p, o)
@@ -87,9 +92,21 @@ def run(args):
             print("[GPU] step %d: %s, %d iterations, residual %.2e" % (
                 t, ", ".join("%s %.3f ms" % (n, st["ms_" + n]) for n in STEP_NAMES), st["iterations"],
                 st["relative_residual"]))
+    if log is not None:
+        log.close()
     print("**************************************************")
     print("  %d fibers, %d steps in %.3f s" % (sim.N, steps, time.time() - t0))
     return 0
+
+
+def step_record(t, n_fibers, st):
+    """One JSON line per time step: the per-stage device times and the solver
+    counters of that step (the numbers the reference prints per step under
+    --verbose, src/main.cu:85-99, as machine-readable records)."""
+    rec = {"step": t, "fibers": n_fibers}
+    rec.update({k: (round(v, 6) if isinstance(v, float) else v) for k, v in st.items()})
+    rec["ms_step"] = round(sum(st["ms_" + n] for n in STEP_NAMES), 6)
+    return json.dumps(rec, sort_keys=True)
 
 
 # ---------------------------------------------------------------------------
@@ -263,6 +280,8 @@ def build_parser():
         p.add_argument("--precision", default="fp32", choices=["fp32", "mixed_fp16", "mixed_bf16"])
         p.add_argument("--velocity-integration", default="same", choices=["same", "numerical", "analytical"])
         p.add_argument("--output", default=".", help="directory for the output files")
+        if name == "run":
+            p.add_argument("--json-log", default=None, help="write one JSON line of step statistics per time step")
         if name == "validate":
             p.add_argument("--reference", default=None, help="directory of {t}_{field}.ref reference vectors")
         if name == "benchmark":

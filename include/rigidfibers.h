@@ -176,7 +176,7 @@ int rf_get_stream(rf_handle* h, void** stream);
  * launch, the role of src/performance.cc's trackers for that kernel).
  * rf_matvec_profile returns the matvecs that did work in the last solve
  * (launches issued after convergence return at once and are not counted)
- * and the summed milliseconds of all its matvec launches. */
+ * and the summed milliseconds of those launches (the longest windows). */
 int rf_set_profiling(rf_handle* h, int enable);
 /* Autotuning of launch choices that leave the method unchanged: the 16-bit
  * structured matvec kernel (matvec_variant 0 = TMA-staged, 2 = register-staged;

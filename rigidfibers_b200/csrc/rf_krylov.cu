@@ -544,7 +544,8 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   res->residual_calls = residual ? cycles_run - 1 : 0;
   res->iterations = h.total_iters;
   res->restarts = h.restarts;
-  res->matvecs = h.total_iters + (cycles_run - 1);
+  // a restart cycle opens with a matvec of x, or with the caller's residual (not a matvec)
+  res->matvecs = h.total_iters + (residual ? 0 : cycles_run - 1);
   res->relative_residual = h.bnorm > 0 ? h.beta / h.bnorm : 0.0;
   if (h.timeout) {
     set_last_error_str("a bounded device-side wait timed out");

@@ -37,6 +37,20 @@ def test_parser_accepts_reference_command_lines():
         p.parse_args(["cuda", "run", "--gmres", "--D2", "c.ini", "f.in"])
 
 
+def test_step_record_is_one_json_object():
+    st = {"iterations": 7, "restarts": 0, "refinement_steps": 1, "relative_residual": 3.5e-7,
+          "ms_assemble_system": 1.25, "ms_solve_system": 2.5, "ms_update_velocities": 0.25, "ms_update_fibers": 0.0,
+          "device_bytes": 1 << 20, "kernel_launches": 40, "graph_replays": 2, "factorizations": 0}
+    line = FR.step_record(3, 100, st)
+    assert "\n" not in line
+    rec = json.loads(line)
+    assert rec["step"] == 3 and rec["fibers"] == 100 and rec["iterations"] == 7
+    assert rec["ms_step"] == 4.0
+    a = FR.build_parser().parse_args(["cuda", "run", "--gmres", "--numerical", "--D2", "c.ini", "f.in",
+                                      "--json-log", "s.jsonl"])
+    assert a.json_log == "s.jsonl"
+
+
 def test_fortran_platform_is_reported_unavailable():
     assert FR.main(["fortran", "run", "--direct", "--numerical", "c.ini", "f.in"]) == 2
 
@@ -51,6 +65,19 @@ def test_run_writes_reference_state_files(tmp_path, golden):
     assert np.abs(o.reshape(-1) - golden["numeric_gmres/1_ORIENT"]).max() < 1e-5
     tv, rv = F.read_fibers(str(out / "TcR_res_00001.out"))
     assert np.abs(tv.reshape(-1) - golden["numeric_gmres/0_TRANSVel"]).max() < 1e-4
+
+
+@pytest.mark.gpu
+def test_run_writes_json_step_log(tmp_path, golden):
+    ini, fib = write_inputs(tmp_path, golden, steps=3)
+    log = tmp_path / "steps.jsonl"
+    assert FR.main(["cuda", "run", "--gmres", "--numerical", "--D2", ini, fib, "--output", str(tmp_path / "o"),
+                    "--json-log", str(log)]) == 0
+    recs = [json.loads(line) for line in open(str(log))]
+    assert [r["step"] for r in recs] == [0, 1, 2]
+    for r in recs:
+        assert r["fibers"] == 100 and r["iterations"] > 0 and r["relative_residual"] < 1e-5
+        assert r["ms_step"] > 0 and r["kernel_launches"] > 0
 
 
 @pytest.mark.gpu
