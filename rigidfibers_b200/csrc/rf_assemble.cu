@@ -311,24 +311,27 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
       float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
       for (int v = tid; v < S::NQ32 * TI / 4; v += blockDim.x)
         reinterpret_cast<float4*>(d32)[v] = reinterpret_cast<const float4*>(sTflat)[v];
-      uint32_t* d16 = out.S16 + rec * (int64_t)(S::NQ16 * TI);
-      for (int v = tid; v < S::NQ16 * (TI / 4); v += blockDim.x) {
-        const int q2 = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
-        const float4 a = *reinterpret_cast<const float4*>(&sTflat[sMap16[2 * q2] * TI + g4]);
-        const float4 b = *reinterpret_cast<const float4*>(&sTflat[sMap16[2 * q2 + 1] * TI + g4]);
-        const float lo[4] = {a.x, a.y, a.z, a.w}, hi[4] = {b.x, b.y, b.z, b.w};
+      // 16-bit records [tl][NW]: pair tl's words are contiguous; a warp stores
+      // 64-byte runs of 8 records
+      constexpr int NW = s16_record_words(M);
+      uint32_t* d16 = out.S16 + rec * (int64_t)(NW * TI);
+      for (int v = tid; v < TI * NW / 4; v += blockDim.x) {
+        const int tl = v % TI, w4 = v / TI;
         uint32_t w[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
+          const int q2 = 4 * w4 + u;
+          const float lo = q2 < S::NQ16 ? sTflat[sMap16[2 * q2] * TI + tl] : 0.f;
+          const float hi = q2 < S::NQ16 ? sTflat[sMap16[2 * q2 + 1] * TI + tl] : 0.f;
           if constexpr (MODE == kAsmStructF16) {
-            __half2 hv = __floats2half2_rn(lo[u], hi[u]);
+            __half2 hv = __floats2half2_rn(lo, hi);
             w[u] = *reinterpret_cast<uint32_t*>(&hv);
           } else {
-            __nv_bfloat162 hv = __floats2bfloat162_rn(lo[u], hi[u]);
+            __nv_bfloat162 hv = __floats2bfloat162_rn(lo, hi);
             w[u] = *reinterpret_cast<uint32_t*>(&hv);
           }
         }
-        *reinterpret_cast<uint4*>(&d16[q2 * TI + g4]) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(&d16[tl * NW + 4 * w4]) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
     // ---- phase 3c: force terms F_i[k] += T^{ij}[k][P0] F/2 and
@@ -438,7 +441,7 @@ int64_t struct_floats32(int M, int N) {
 }
 
 int64_t struct_words16(int M, int N) {
-  return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * M * M * 3;
+  return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * s16_record_words(M);
 }
 
 template <int M, int Q, int MODE, int INTEG>

@@ -11,6 +11,10 @@ namespace rf {
 
 // Structured storage tile: 16 x 16 fibers (a multiple of every assembly tile side).
 constexpr int kStoreTile = 16;
+// 16-bit storage: one record per pair, the 3 M^2 words (two 16-bit values each:
+// block kI*M + kJ, values (0,1), (2,3), (4,5) of its symmetric 3x3) padded to a
+// multiple of 4 words so that every record starts on a 16-byte boundary.
+__host__ __device__ constexpr int s16_record_words(int M) { return (3 * M * M + 3) / 4 * 4; }
 
 bool mq_supported(int M, int Q);
 // out[r] = sum_p part[p*R + r], fixed order

@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(128, 3) k_lu_gemm_tc(float* __restrict__ A, in
                                                        bool vec4, int* __restrict__ info, uint64_t wait_ns) {
   constexpr int TM = 128, TN = 128;
   static_assert(NB == 64, "the staging below is written for a 64-column panel");
-  constexpr uint32_t kABytes = TM * NB * 4, kBBytes = TN * NB * 4;
+  constexpr uint32_t kABytes = TM * NB * 4;   // B follows A in shared memory
   constexpr uint32_t kAKChunk = (TM / 8) * 128;   // bytes per k-chunk of 4 (A)
   constexpr uint32_t kBKChunk = (TN / 8) * 128;   // bytes per k-chunk of 4 (B)
   constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) |

@@ -11,8 +11,11 @@
 //
 // Storage (written by k_assemble_numerical in structured mode): 16x16 fiber
 // storage tiles over the upper triangle; inside, (16/TI)^2 assembly
-// sub-tiles of TI x TI pairs, each as [j][value][i], so a warp reads whole
-// 32-byte sectors.  One CTA = one storage tile = 256 pairs = 256 threads.
+// sub-tiles of TI x TI pairs.  FP32 blocks as [j][value][i], so a warp reads
+// whole 32-byte sectors; 16-bit blocks as [j][i][record], one 16-byte aligned
+// record of s16_record_words(M) words per pair (copied whole into shared
+// memory and read there with 16-byte loads).  One CTA = one storage tile =
+// 256 pairs.
 // z is reduced deterministically: per-tile partial rows, fixed-order sums.
 // The velocities reuse the FP32 blocks with P_0 / P_1 on the receiving side
 // (fortran/update_velocities.incl:64-86: TFA0 and TFA1 are exactly those).
@@ -82,7 +85,6 @@ struct TileMap {
 // Shared memory: x of both tiles, then per-warp partial sums of z for the 16
 // row fibers of each side (zero-filled; warps that do not touch a fiber leave
 // zeros), summed in a fixed order at the end.
-constexpr int kZWarps = 8;   // 256 threads
 
 // Shared memory of the z kernel (8x8 assembly sub-tiles, 8 warps):
 //  x rows of both tiles (padded: 20 floats / 17 doubles per fiber so the
@@ -114,9 +116,9 @@ struct RowLoader {
         for (int c = 0; c < 6; ++c)
           w[kJ * 6 + c] = __float_as_uint(__ldcs(p + (((kI + 1) * K1 + (kJ + 1)) * 6 + c) * TI));
     } else {
-      const uint32_t* p = static_cast<const uint32_t*>(base);
+      const uint32_t* p = static_cast<const uint32_t*>(base);   // this pair's record (L1 keeps its sectors)
 #pragma unroll
-      for (int q = 0; q < 3 * M; ++q) w[q] = __ldcs(p + (kI * 3 * M + q) * TI);
+      for (int q = 0; q < 3 * M; ++q) w[q] = __ldg(p + kI * 3 * M + q);
     }
   }
   template <typename ACC>
@@ -167,7 +169,7 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
   if (skip != nullptr && *skip) return;
   constexpr int K1 = M + 1, M3 = 3 * M;
   constexpr int XS = ZSmem<M, sizeof(ACC)>::XS;
-  constexpr int NQ32 = K1 * K1 * 6, NQ16 = M * M * 3;
+  constexpr int NQ32 = K1 * K1 * 6;
   constexpr int SUB = kStoreTile / TI;
   using RL = RowLoader<M, TI, SMODE>;
   extern __shared__ __align__(16) unsigned char zsm[];
@@ -185,7 +187,7 @@ k_struct_z(int N, const float* __restrict__ S32, const uint32_t* __restrict__ S1
   const bool active = i < j && j < N;
   const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
   const void* base = SMODE == 0 ? (const void*)(S32 + rec * (int64_t)(NQ32 * TI) + mp.tl)
-                                : (const void*)(S16 + rec * (int64_t)(NQ16 * TI) + mp.tl);
+                                : (const void*)(S16 + (rec * TI + mp.tl) * (int64_t)s16_record_words(M));
   // first block row in flight before the x prologue
   uint32_t wa[RL::NW], wb[RL::NW];
   if (active) RL::load(wa, base, 0);
@@ -310,39 +312,148 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 template <int M>
 struct BulkShape {
   static constexpr int M3 = 3 * M;
-  static constexpr int NQ16 = M * M * 3;                         // words per pair
-  static constexpr uint32_t kTileBytes = 4u * 8 * NQ16 * 8 * 4;  // 4 sub-tiles x 8 j x NQ16 x 8 i words
-  static constexpr int XS = (M3 + 3) / 4 * 4 + 4;
-  static constexpr size_t kX = (size_t)2 * 2 * kStoreTile * XS * 4;   // double-buffered x rows
-  static constexpr size_t kWI = (size_t)kStoreTile * 4 * M3 * 4;
-  static constexpr size_t kWJ = (size_t)kStoreTile * 4 * M3 * 4;
+  static constexpr int NW = s16_record_words(M);                                   // words per pair record
+  static constexpr uint32_t kTileBytes = 4u * kStoreTile * kStoreTile * NW;       // 256 records
+  static constexpr int M3P = (M3 + 3) / 4 * 4;
+  static constexpr int XS = M3P + 4;                                              // x row stride (floats)
+  // the M^2 blocks of a pair are split between two threads at a 16-byte
+  // boundary of the record: blocks [0, B0) and [B0, M^2), B0 a multiple of 4
+  static constexpr int B0 = 4 * ((M * M + 4) / 8);
+  static constexpr int ZW = 12;                                                   // z_i values per half (<= 3 rows + pad)
+  static constexpr size_t kX = (size_t)2 * 2 * kStoreTile * XS * 4;              // double-buffered x rows
+  static constexpr size_t kWI = (size_t)2 * kStoreTile * 4 * ZW * 4;
+  static constexpr size_t kWJ = (size_t)kStoreTile * 4 * 16 * 4;
   static constexpr size_t kBytes = 2 * (size_t)kTileBytes + kX + kWI + kWJ;
-  static constexpr int kThreads = 512;                            // two threads per pair
-  static constexpr int KSPLIT = (M + 1) / 2;                       // block rows of the first half
+  static constexpr int kThreads = 512;                                            // two threads per pair
+  static_assert(M3 <= 16, "z_j is reduced as 16 values");
 };
 
-// Thread t: half h = t / 256 takes block rows [h ? KSPLIT : 0, h ? M : KSPLIT)
-// of pair tt = t % 256 (TileMap).  z_i of a row comes from one half only;
-// z_j gets one partial per half (4 slots per row fiber).
+template <int M, int H>
+struct BulkHalf {
+  static constexpr int BB = H ? BulkShape<M>::B0 : 0, BE = H ? M * M : BulkShape<M>::B0;   // blocks [BB, BE)
+  static constexpr int NBLK = BE - BB;
+  static constexpr int R0 = NBLK > 0 ? BB / M : 0;
+  static constexpr int NR = NBLK > 0 ? (BE - 1) / M - R0 + 1 : 0;                // block rows touched
+  static constexpr int NU = (3 * NBLK + 3) / 4;                                  // 16-byte loads
+  static_assert(3 * NR <= BulkShape<M>::ZW, "at most three block rows per half");
+};
+
+// The blocks of half H of one pair: z_i rows of this half reduced over the
+// warp's 4 j lanes into swi (lane group g = lane / 8 stores values 3g..3g+2,
+// i.e. row R0 + g), z_j (16 values, this pair's contribution) returned for
+// the caller's reduction.
+template <int M, int SMODE, int H>
+__device__ __forceinline__ void z16_half(const uint32_t* rec, const float* xjs, const float* xis, bool active,
+                                         float (&zj)[16], float* swi_slot, int lane) {
+  using HF = BulkHalf<M, H>;
+  using H16 = typename std::conditional<SMODE == 1, __half, __nv_bfloat16>::type;
+  constexpr int M3P = BulkShape<M>::M3P;
+  float zi[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) zi[q] = 0.f;
+  if constexpr (HF::NBLK > 0) {
+    if (active) {
+      uint32_t w[4 * HF::NU];
+      const uint4* p = reinterpret_cast<const uint4*>(rec + 3 * HF::BB);
+#pragma unroll
+      for (int u = 0; u < HF::NU; ++u) {
+        const uint4 v = p[u];
+        w[4 * u] = v.x; w[4 * u + 1] = v.y; w[4 * u + 2] = v.z; w[4 * u + 3] = v.w;
+      }
+      float xj[M3P], xi[12];
+      load_xrow<float, M3P>(xjs, xj);
+#pragma unroll
+      for (int q = 0; q < 3 * HF::NR; ++q) xi[q] = xis[3 * HF::R0 + q];
+#pragma unroll
+      for (int b = 0; b < HF::NBLK; ++b) {
+        const int blk = HF::BB + b, kI = blk / M, kJ = blk % M;
+        float tv[6];
+#pragma unroll
+        for (int h = 0; h < 3; ++h) {
+          const float2 f = unpack16<H16>(w[3 * b + h]);
+          tv[2 * h] = f.x;
+          tv[2 * h + 1] = f.y;
+        }
+        sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * (kI - HF::R0));
+        sym_mv_acc(tv, xi + 3 * (kI - HF::R0), zj + 3 * kJ);
+      }
+    }
+  }
+  // z_i (12 values, rows R0.. padded) summed over the 4 j lanes of the warp
+  // (lane bits 4, 3) by two halving exchanges: lane group g keeps 3g..3g+2
+  const bool b4 = lane & 16, b3 = lane & 8;
+  float u[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float send = b4 ? zi[k] : zi[k + 6], keep = b4 ? zi[k + 6] : zi[k];
+    u[k] = keep + shfl_xor(send, 16);
+  }
+  const int g = lane >> 3;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float send = b3 ? u[k] : u[k + 3], keep = b3 ? u[k + 3] : u[k];
+    swi_slot[3 * g + k] = keep + shfl_xor(send, 8);
+  }
+}
+
+// v[16] summed over the 8 lanes that differ in lane bits 0..2; lane l keeps
+// the sums of v[2l] and v[2l+1] (three halving exchanges instead of 16 x 3).
+__device__ __forceinline__ float2 reduce_scatter8(const float (&v)[16], int lane) {
+  const bool b2 = lane & 4, b1 = lane & 2, b0 = lane & 1;
+  float u[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float send = b2 ? v[k] : v[k + 8], keep = b2 ? v[k + 8] : v[k];
+    u[k] = keep + shfl_xor(send, 4);
+  }
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = b1 ? u[k] : u[k + 4], keep = b1 ? u[k + 4] : u[k];
+    w[k] = keep + shfl_xor(send, 2);
+  }
+  float y[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = b0 ? w[k] : w[k + 2], keep = b0 ? w[k + 2] : w[k];
+    y[k] = keep + shfl_xor(send, 1);
+  }
+  return make_float2(y[0], y[1]);
+}
+
+// (I, J) of storage tile L (L = J (J + 1) / 2 + I, I <= J) without FP64
+__device__ __forceinline__ void tile_pair16f(int64_t L, int& I, int& J) {
+  int64_t j = (int64_t)((sqrtf(8.f * (float)L + 1.f) - 1.f) * 0.5f);
+  while ((j + 1) * (j + 2) / 2 <= L) ++j;
+  while (j * (j + 1) / 2 > L) --j;
+  J = (int)j;
+  I = (int)(L - j * (j + 1) / 2);
+}
+
+// Thread t: half h = t / 256 takes blocks [BB, BE) of pair tt = t % 256
+// (TileMap).  z_i of a block row comes from one or both halves (4 warp
+// slots each), z_j from both halves (2 warp slots each).  Partial rows go to
+// zpart slot J (i side of tile (I, J)) and I (j side); the j side of a
+// diagonal tile goes to slot ceil(N/16), so every slot has one writer.
 template <int M, int SMODE>
 __global__ void __launch_bounds__(512, 1)
 k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restrict__ x, float* __restrict__ zpart,
                   const int* __restrict__ skip, int* __restrict__ err, uint32_t wait_polls) {
   constexpr int TI = 8, M3 = 3 * M;
   using B = BulkShape<M>;
-  using RL = RowLoader<M, TI, SMODE>;
-  constexpr int XS = B::XS;
+  using H0 = BulkHalf<M, 0>;
+  using H1 = BulkHalf<M, 1>;
+  constexpr int XS = B::XS, ZW = B::ZW;
   if (skip != nullptr && *skip) return;
   extern __shared__ __align__(128) unsigned char bsm[];
-  uint32_t* stage[2] = {reinterpret_cast<uint32_t*>(bsm), reinterpret_cast<uint32_t*>(bsm + B::kTileBytes)};
+  auto stage = [&](int s) { return reinterpret_cast<uint32_t*>(bsm + (size_t)s * B::kTileBytes); };
   float (*sx)[2][kStoreTile][XS] = reinterpret_cast<float (*)[2][kStoreTile][XS]>(bsm + 2 * B::kTileBytes);
-  float (*swi)[4][M3] = reinterpret_cast<float (*)[4][M3]>(bsm + 2 * B::kTileBytes + B::kX);
-  float (*swj)[4][M3] = reinterpret_cast<float (*)[4][M3]>(bsm + 2 * B::kTileBytes + B::kX + B::kWI);
+  float (*swi)[kStoreTile][4][ZW] = reinterpret_cast<float (*)[kStoreTile][4][ZW]>(bsm + 2 * B::kTileBytes + B::kX);
+  float (*swj)[4][16] = reinterpret_cast<float (*)[4][16]>(bsm + 2 * B::kTileBytes + B::kX + B::kWI);
   __shared__ __align__(8) uint64_t bar[2];
   const int64_t ntiles = struct_store_tiles_dev(N);
   const int t = threadIdx.x, lane = t & 31;
   const int half = t >> 8, tt = t & 255, hw = tt >> 5;   // warp index within the half
-  const int kbeg = half ? B::KSPLIT : 0, kend = half ? M : B::KSPLIT;
   const int64_t R = (int64_t)M3 * N;
   const TileMap<TI> mp(tt);
   if (t == 0) {
@@ -352,13 +463,11 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
   }
   auto issue = [&](int64_t L, int s) {
     mbar_expect_tx(&bar[s], B::kTileBytes);
-    bulk_g2s(stage[s], S16 + L * (int64_t)(B::kTileBytes / 4), B::kTileBytes, &bar[s]);
+    bulk_g2s(stage(s), S16 + L * (int64_t)(B::kTileBytes / 4), B::kTileBytes, &bar[s]);
   };
   // x rows of a tile: thread t < 2*16*M3 owns one value
-  auto xval = [&](int64_t L) -> float {
-    if (t >= 2 * kStoreTile * M3 || L >= ntiles) return 0.f;
-    int I16, J16;
-    tile_pair16(L, I16, J16);
+  auto xval = [&](bool valid, int I16, int J16) -> float {
+    if (t >= 2 * kStoreTile * M3 || !valid) return 0.f;
     const int side = t / (kStoreTile * M3), rem = t % (kStoreTile * M3);
     const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
     return f < N ? x[(int64_t)f * M3 + rem % M3] : 0.f;
@@ -369,7 +478,9 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
       sx[buf][side][rem / M3][rem % M3] = v;
     }
   };
-  xstore(0, xval(blockIdx.x));
+  int cI = 0, cJ = 0;
+  tile_pair16f(blockIdx.x, cI, cJ);
+  xstore(0, xval(true, cI, cJ));
   __syncthreads();
   if (t == 0) {
     for (int s = 0; s < 2; ++s) {
@@ -382,10 +493,11 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
   for (int64_t L = blockIdx.x; L < ntiles; L += gridDim.x, ++k) {
     const int s = k & 1, xb = k & 1;
     const uint32_t parity = (k >> 1) & 1;
-    int I16, J16;
-    tile_pair16(L, I16, J16);
+    const int I16 = cI, J16 = cJ;
     const bool diag = I16 == J16;
-    const float xnext = xval(L + gridDim.x);   // in flight while this tile is computed
+    const bool more = L + gridDim.x < ntiles;
+    if (more) tile_pair16f(L + gridDim.x, cI, cJ);
+    const float xnext = xval(more, cI, cJ);   // in flight while this tile is computed
     const bool ok_wait = mbar_wait_bounded(&bar[s], parity, wait_polls);
     if (__syncthreads_or(!ok_wait)) {
       failed = true;
@@ -393,51 +505,17 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     }
     const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
     const bool active = i < j && j < N;
-    const uint32_t* pw = stage[s] + ((mp.sub * TI + mp.jl) * B::NQ16) * TI + mp.tl;
-    float zj[M3];
+    const uint32_t* rec = stage(s) + ((mp.sub * TI + mp.jl) * TI + mp.tl) * B::NW;
+    const float* xjs = sx[xb][1][mp.j16()];
+    const float* xis = sx[xb][0][mp.i16()];
+    float zj[16];
 #pragma unroll
-    for (int q = 0; q < M3; ++q) zj[q] = 0.f;
-    constexpr int M3P = (M3 + 3) / 4 * 4;
-    float xjr[M3P];
-    load_xrow<float, M3P>(sx[xb][1][mp.j16()], xjr);
-    const float* xi = sx[xb][0][mp.i16()];
-#pragma unroll
-    for (int kI = 0; kI < M; ++kI) {
-      if (kI < kbeg || kI >= kend) continue;   // uniform per warp
-      float ziv[3] = {0.f, 0.f, 0.f};
-      if (active) {
-        uint32_t w[3 * M];
-#pragma unroll
-        for (int q = 0; q < 3 * M; ++q) w[q] = pw[(kI * 3 * M + q) * TI];
-        const float xik[3] = {xi[3 * kI], xi[3 * kI + 1], xi[3 * kI + 2]};
-#pragma unroll
-        for (int kJ = 0; kJ < M; ++kJ) {
-          float tv[6];
-          RL::values(w, kJ, tv);
-          sym_mv_acc(tv, xjr + 3 * kJ, ziv);
-          sym_mv_acc(tv, xik, zj + 3 * kJ);
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        float v = ziv[a];
-        v += shfl_xor(v, 8);
-        v += shfl_xor(v, 16);
-        if (lane < TI) swi[mp.i16()][hw & 3][3 * kI + a] = v;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < M3; ++q) {
-      float b = zj[q];
-      b += shfl_xor(b, 1);
-      b += shfl_xor(b, 2);
-      b += shfl_xor(b, 4);
-      zj[q] = b;
-    }
-    if ((lane & (TI - 1)) == 0) {
-#pragma unroll
-      for (int q = 0; q < M3; ++q) swj[mp.j16()][2 * half + (hw >> 2)][q] = zj[q];
-    }
+    for (int q = 0; q < 16; ++q) zj[q] = 0.f;
+    if (half == 0) z16_half<M, SMODE, 0>(rec, xjs, xis, active, zj, swi[0][mp.i16()][hw & 3], lane);
+    else z16_half<M, SMODE, 1>(rec, xjs, xis, active, zj, swi[1][mp.i16()][hw & 3], lane);
+    // z_j over the 8 i lanes (lane bits 0..2): lane tl keeps values 2 tl, 2 tl + 1
+    const float2 zs = reduce_scatter8(zj, lane);
+    *reinterpret_cast<float2*>(&swj[mp.j16()][2 * half + (hw >> 2)][2 * (lane & 7)]) = zs;
     xstore(xb ^ 1, xnext);
     __syncthreads();
     // stage s is free again: refill it with the tile two steps ahead
@@ -445,16 +523,24 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
       const int64_t Ln = L + 2 * (int64_t)gridDim.x;
       if (Ln < ntiles) issue(Ln, s);
     }
-    for (int task = t; task < kStoreTile * M3; task += blockDim.x) {
-      const int rf = task / M3, rv = task % M3;
-      const float si = ((swi[rf][0][rv] + swi[rf][1][rv]) + swi[rf][2][rv]) + swi[rf][3][rv];
-      const float sj = ((swj[rf][0][rv] + swj[rf][1][rv]) + swj[rf][2][rv]) + swj[rf][3][rv];
-      const int fi = I16 * kStoreTile + rf, fj = J16 * kStoreTile + rf;
-      if (diag) {
-        if (fi < N) zpart[(int64_t)I16 * R + (int64_t)fi * M3 + rv] = si + sj;
-      } else {
+    // half 0 writes the i side, half 1 the j side (fixed-order slot sums)
+    if (tt < kStoreTile * M3) {
+      const int rf = tt / M3, rv = tt % M3;
+      if (half == 0) {
+        const int kI = rv / 3;
+        const bool in0 = H0::NR > 0 && kI >= H0::R0 && kI < H0::R0 + H0::NR;
+        const bool in1 = H1::NR > 0 && kI >= H1::R0 && kI < H1::R0 + H1::NR;
+        const int q0 = in0 ? rv - 3 * H0::R0 : 0, q1 = in1 ? rv - 3 * H1::R0 : 0;
+        const float s0 = ((swi[0][rf][0][q0] + swi[0][rf][1][q0]) + swi[0][rf][2][q0]) + swi[0][rf][3][q0];
+        const float s1 = ((swi[1][rf][0][q1] + swi[1][rf][1][q1]) + swi[1][rf][2][q1]) + swi[1][rf][3][q1];
+        const float si = in0 ? (in1 ? s0 + s1 : s0) : s1;
+        const int fi = I16 * kStoreTile + rf;
         if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si;
-        if (fj < N) zpart[(int64_t)I16 * R + (int64_t)fj * M3 + rv] = sj;
+      } else {
+        const float sj = ((swj[rf][0][rv] + swj[rf][1][rv]) + swj[rf][2][rv]) + swj[rf][3][rv];
+        const int fj = J16 * kStoreTile + rf;
+        const int64_t slot = diag ? (int64_t)((N + kStoreTile - 1) / kStoreTile) : (int64_t)I16;
+        if (fj < N) zpart[slot * R + (int64_t)fj * M3 + rv] = sj;
       }
     }
   }
@@ -476,8 +562,8 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
 // p loop unrolled so that 8 loads per thread are in flight.
 template <typename ACC>
 __global__ void __launch_bounds__(256)
-k_sum_parts(const ACC* __restrict__ part, int nparts, int64_t R, ACC* __restrict__ out,
-            const int* __restrict__ skip) {
+k_sum_parts(const ACC* part, int nparts, int64_t R, ACC* out, const int* __restrict__ skip) {
+  // out may be the last partial row (read by this block before it is written)
   if (skip != nullptr && *skip) return;
   __shared__ ACC red[4][64];
   const int rr = threadIdx.x & 63, g = threadIdx.x >> 6;
@@ -682,7 +768,8 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
                          cudaStream_t st, int variant) {
   int rc = RF_E_UNSUPPORTED;
-  if (variant != 2 && tab.Q == 24 && smode != 0 && err != nullptr && tab.M <= 5) {
+  const bool bulk = variant != 2 && tab.Q == 24 && smode != 0 && err != nullptr && tab.M <= 5;
+  if (bulk) {
     // tiles staged by TMA bulk copies (two 3072*M-byte tiles per SM fit in shared memory for M <= 5)
     switch (tab.M) {
       case 1: rc = smode == 1 ? launch_z16_bulk<1, 1>(N, S16, x, zpart, skip, err, st) : launch_z16_bulk<1, 2>(N, S16, x, zpart, skip, err, st); break;
@@ -701,8 +788,10 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
   const int64_t n = (int64_t)N * tab.M;
   const int64_t R = 3 * n;
   const int nparts = (int)ceil_div(N, kStoreTile);
-  // the summed rows go to partial slot 0 (read by nothing else afterwards)
-  k_sum_parts<float><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart, nparts, R, zpart + (int64_t)nparts * R, skip);
+  // the summed rows go to partial slot nparts, which the TMA-staged kernel
+  // also fills (diagonal tiles' j side): each row is read before it is written
+  k_sum_parts<float><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart, bulk ? nparts + 1 : nparts, R,
+                                                                zpart + (int64_t)nparts * R, skip);
   RF_LAUNCH_CHECK();
   k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(
       tab, N, ori, x, zpart + (int64_t)nparts * R, 1, nullptr, y, skip);
