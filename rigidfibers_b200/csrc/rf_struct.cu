@@ -725,7 +725,7 @@ static unsigned fin_blocks(int64_t n) { return (unsigned)std::min<int64_t>(ceil_
 template <int M, int TI, int SMODE, typename XT, typename ACC>
 static int launch_z_one(int N, const float* S32, const uint32_t* S16, const XT* x, ACC* zpart, const int* skip,
                         cudaStream_t st) {
-  constexpr bool kPrefetch = SMODE != 0;   // 16-bit rows are small enough to double-buffer
+  constexpr bool kPrefetch = true;   // the next block row in flight while this one is computed
   constexpr size_t smem = ZSmem<M, sizeof(ACC)>::kBytes;
   static const cudaError_t attr = cudaFuncSetAttribute(k_struct_z<M, TI, SMODE, XT, ACC, kPrefetch>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
