@@ -103,7 +103,7 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   float* const sTbase = smem_dyn + NC * S::GS;                                               // 2 x [TI][TP]
   __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
   __shared__ float sfJ[TI][FF];
-  __shared__ short sMap16[S::NQ16 * 2];   // 16-bit value q' -> offset of its T entry within a pair
+  __shared__ short sMapS[S::NQ32];   // stored value q (s32_block order) -> offset of its T entry within a pair
 
   // numerical: unordered tile pairs (I <= J), both blocks of a pair from one
   // evaluation of K; analytical: ordered tile pairs, direct blocks only
@@ -136,9 +136,18 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   }
   for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
   if constexpr (MODE != kAsmDense) {
-    for (int q = tid; q < S::NQ16 * 2; q += blockDim.x) {
+    for (int q = tid; q < S::NQ32; q += blockDim.x) {
       const int c = q % 6, blk = q / 6;
-      sMap16[q] = (short)(((blk / M + 1) * K1 + (blk % M + 1)) * 6 + c);
+      int row = 0, col = 0;
+      if (blk < M * M) {
+        row = blk / M + 1;
+        col = blk % M + 1;
+      } else if (blk < M * M + K1) {
+        col = blk - M * M;
+      } else {
+        row = blk - M * M - M;
+      }
+      sMapS[q] = (short)((row * K1 + col) * 6 + c);
     }
   }
 
@@ -306,11 +315,14 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
       const int sub = (I % S::SUB) * S::SUB + (J % S::SUB);
       const int64_t L16 = (int64_t)J16 * (J16 + 1) / 2 + I16;
       const int64_t rec = (L16 * S::SUB * S::SUB + sub) * TI + jl;
-      // T is already in the record order [q][tl]; pairs that do not exist
-      // (i >= N, i >= j on a diagonal tile) came out of phases 1-2 as exact zeros
+      // T is [q][tl] with q in (row, col) order; stored in s32_block order.
+      // Pairs that do not exist (i >= N, i >= j on a diagonal tile) came out
+      // of phases 1-2 as exact zeros
       float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
-      for (int v = tid; v < S::NQ32 * TI / 4; v += blockDim.x)
-        reinterpret_cast<float4*>(d32)[v] = reinterpret_cast<const float4*>(sTflat)[v];
+      for (int v = tid; v < S::NQ32 * TI / 4; v += blockDim.x) {
+        const int q = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
+        reinterpret_cast<float4*>(d32)[v] = *reinterpret_cast<const float4*>(&sTflat[sMapS[q] * TI + g4]);
+      }
       // 16-bit records [tl][NW]: pair tl's words are contiguous; a warp stores
       // 64-byte runs of 8 records
       constexpr int NW = s16_record_words(M);
@@ -321,8 +333,8 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int q2 = 4 * w4 + u;
-          const float lo = q2 < S::NQ16 ? sTflat[sMap16[2 * q2] * TI + tl] : 0.f;
-          const float hi = q2 < S::NQ16 ? sTflat[sMap16[2 * q2 + 1] * TI + tl] : 0.f;
+          const float lo = q2 < S::NQ16 ? sTflat[sMapS[2 * q2] * TI + tl] : 0.f;
+          const float hi = q2 < S::NQ16 ? sTflat[sMapS[2 * q2 + 1] * TI + tl] : 0.f;
           if constexpr (MODE == kAsmStructF16) {
             __half2 hv = __floats2half2_rn(lo, hi);
             w[u] = *reinterpret_cast<uint32_t*>(&hv);

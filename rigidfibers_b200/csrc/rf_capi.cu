@@ -632,7 +632,7 @@ int rf_solve(rf_handle* h) {
   if (h->mixed) {
     ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
       return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
-                                      h->b, r, skip, st);
+                                      h->b, r, skip, &h->ctl->timeout, st);
     };
     h->refinements = 0;
     rc = gmres_solve_ex(s, mv, resid, h->b, h->x64, true, h->st, &res);

@@ -15,6 +15,13 @@ constexpr int kStoreTile = 16;
 // block kI*M + kJ, values (0,1), (2,3), (4,5) of its symmetric 3x3) padded to a
 // multiple of 4 words so that every record starts on a 16-byte boundary.
 __host__ __device__ constexpr int s16_record_words(int M) { return (3 * M * M + 3) / 4 * 4; }
+// FP32 storage: block (row, col) of a pair (Legendre indices 0..M, 0 = P_0) is
+// stored at block position s32_block(M, row, col) of its (M+1)^2 blocks of 6
+// values: the M^2 operator blocks (row, col >= 1) first, row-major, so that
+// they are one contiguous run per pair; then row 0; then column 0.
+__host__ __device__ constexpr int s32_block(int M, int row, int col) {
+  return (row >= 1 && col >= 1) ? (row - 1) * M + (col - 1) : row == 0 ? M * M + col : M * M + M + row;
+}
 
 bool mq_supported(int M, int Q);
 // out[r] = sum_p part[p*R + r], fixed order
@@ -45,8 +52,9 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
                          const float4* ori, const float* x, float* zpart, float* y, const int* skip, int* err,
                          cudaStream_t st, int variant = 0);
 // r = b - A x with the FP32 blocks, x and accumulation in FP64; zpart64: (ceil(N/16) + 1) x R doubles.
+// err as for launch_struct_matvec (null: the register-staged kernel).
 int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
-                             double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st);
+                             double* zpart64, const float* b, float* r, const int* skip, int* err, cudaStream_t st);
 // y = A x with the FP32 blocks, x and accumulation in FP64.
 int launch_struct_apply64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
                           double* zpart64, float* y, cudaStream_t st);

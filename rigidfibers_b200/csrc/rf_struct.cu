@@ -11,8 +11,9 @@
 //
 // Storage (written by k_assemble_numerical in structured mode): 16x16 fiber
 // storage tiles over the upper triangle; inside, (16/TI)^2 assembly
-// sub-tiles of TI x TI pairs.  FP32 blocks as [j][value][i], so a warp reads
-// whole 32-byte sectors; 16-bit blocks as [j][i][record], one 16-byte aligned
+// sub-tiles of TI x TI pairs.  FP32 blocks as [j][value][i] (values in
+// s32_block order: the operator blocks lead), so a warp reads whole 32-byte
+// sectors; 16-bit blocks as [j][i][record], one 16-byte aligned
 // record of s16_record_words(M) words per pair (copied whole into shared
 // memory and read there with 16-byte loads).  One CTA = one storage tile =
 // 256 pairs.
@@ -114,7 +115,7 @@ struct RowLoader {
       for (int kJ = 0; kJ < M; ++kJ)
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-          w[kJ * 6 + c] = __float_as_uint(__ldcs(p + (((kI + 1) * K1 + (kJ + 1)) * 6 + c) * TI));
+          w[kJ * 6 + c] = __float_as_uint(__ldcs(p + ((kI * M + kJ) * 6 + c) * TI));
     } else {
       const uint32_t* p = static_cast<const uint32_t*>(base);   // this pair's record (L1 keeps its sectors)
 #pragma unroll
@@ -338,6 +339,52 @@ struct BulkHalf {
   static_assert(3 * NR <= BulkShape<M>::ZW, "at most three block rows per half");
 };
 
+// v[16] summed over the 8 lanes that differ in lane bits 0..2; lane l keeps
+// the sums of v[2l] and v[2l+1] (three halving exchanges instead of 16 x 3).
+template <typename T>
+__device__ __forceinline__ void reduce_scatter8(const T (&v)[16], int lane, T& y0, T& y1) {
+  const bool b2 = lane & 4, b1 = lane & 2, b0 = lane & 1;
+  T u[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const T send = b2 ? v[k] : v[k + 8], keep = b2 ? v[k + 8] : v[k];
+    u[k] = keep + shfl_xor(send, 4);
+  }
+  T w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const T send = b1 ? u[k] : u[k + 4], keep = b1 ? u[k + 4] : u[k];
+    w[k] = keep + shfl_xor(send, 2);
+  }
+  T y[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const T send = b0 ? w[k] : w[k + 2], keep = b0 ? w[k + 2] : w[k];
+    y[k] = keep + shfl_xor(send, 1);
+  }
+  y0 = y[0];
+  y1 = y[1];
+}
+
+// v[12] summed over the 4 lanes that differ in lane bits 3, 4 (two halving
+// exchanges); lane group g = lane / 8 stores the sums of v[3g..3g+2] to dst.
+template <typename T>
+__device__ __forceinline__ void reduce_scatter4x3(const T (&v)[12], int lane, T* dst) {
+  const bool b4 = lane & 16, b3 = lane & 8;
+  T u[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const T send = b4 ? v[k] : v[k + 6], keep = b4 ? v[k + 6] : v[k];
+    u[k] = keep + shfl_xor(send, 16);
+  }
+  const int g = lane >> 3;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const T send = b3 ? u[k] : u[k + 3], keep = b3 ? u[k + 3] : u[k];
+    dst[3 * g + k] = keep + shfl_xor(send, 8);
+  }
+}
+
 // The blocks of half H of one pair: z_i rows of this half reduced over the
 // warp's 4 j lanes into swi (lane group g = lane / 8 stores values 3g..3g+2,
 // i.e. row R0 + g), z_j (16 values, this pair's contribution) returned for
@@ -380,45 +427,7 @@ __device__ __forceinline__ void z16_half(const uint32_t* rec, const float* xjs, 
     }
   }
   // z_i (12 values, rows R0.. padded) summed over the 4 j lanes of the warp
-  // (lane bits 4, 3) by two halving exchanges: lane group g keeps 3g..3g+2
-  const bool b4 = lane & 16, b3 = lane & 8;
-  float u[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const float send = b4 ? zi[k] : zi[k + 6], keep = b4 ? zi[k + 6] : zi[k];
-    u[k] = keep + shfl_xor(send, 16);
-  }
-  const int g = lane >> 3;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float send = b3 ? u[k] : u[k + 3], keep = b3 ? u[k + 3] : u[k];
-    swi_slot[3 * g + k] = keep + shfl_xor(send, 8);
-  }
-}
-
-// v[16] summed over the 8 lanes that differ in lane bits 0..2; lane l keeps
-// the sums of v[2l] and v[2l+1] (three halving exchanges instead of 16 x 3).
-__device__ __forceinline__ float2 reduce_scatter8(const float (&v)[16], int lane) {
-  const bool b2 = lane & 4, b1 = lane & 2, b0 = lane & 1;
-  float u[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const float send = b2 ? v[k] : v[k + 8], keep = b2 ? v[k + 8] : v[k];
-    u[k] = keep + shfl_xor(send, 4);
-  }
-  float w[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float send = b1 ? u[k] : u[k + 4], keep = b1 ? u[k + 4] : u[k];
-    w[k] = keep + shfl_xor(send, 2);
-  }
-  float y[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float send = b0 ? w[k] : w[k + 2], keep = b0 ? w[k + 2] : w[k];
-    y[k] = keep + shfl_xor(send, 1);
-  }
-  return make_float2(y[0], y[1]);
+  reduce_scatter4x3(zi, lane, swi_slot);
 }
 
 // (I, J) of storage tile L (L = J (J + 1) / 2 + I, I <= J) without FP64
@@ -514,7 +523,8 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
     if (half == 0) z16_half<M, SMODE, 0>(rec, xjs, xis, active, zj, swi[0][mp.i16()][hw & 3], lane);
     else z16_half<M, SMODE, 1>(rec, xjs, xis, active, zj, swi[1][mp.i16()][hw & 3], lane);
     // z_j over the 8 i lanes (lane bits 0..2): lane tl keeps values 2 tl, 2 tl + 1
-    const float2 zs = reduce_scatter8(zj, lane);
+    float2 zs;
+    reduce_scatter8(zj, lane, zs.x, zs.y);
     *reinterpret_cast<float2*>(&swj[mp.j16()][2 * half + (hw >> 2)][2 * (lane & 7)]) = zs;
     xstore(xb ^ 1, xnext);
     __syncthreads();
@@ -552,6 +562,206 @@ k_struct_z16_bulk(int N, const uint32_t* __restrict__ S16, const float* __restri
         const int64_t L = blockIdx.x + (int64_t)kk * gridDim.x;
         if (L < ntiles) (void)mbar_wait_bounded(&bar[kk & 1], (kk >> 1) & 1);
       }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// A x with the FP32 blocks, x and accumulation in FP64 (the refinement
+// residual), staged by TMA bulk copies.  A storage tile comes in as two
+// halves (assembly sub-tile row a = 0, 1: 16 records of 8 pairs), and of
+// every record only its M^2 operator blocks, which lead the record
+// (s32_block order: 6 M^2 values x 8 pairs, one copy per record; the P_0 row
+// and column stay in HBM).  Persistent CTAs, one per SM; while one half is
+// computed the other is in flight.
+// ---------------------------------------------------------------------------
+template <int M>
+struct R64Shape {
+  static constexpr int M3 = 3 * M, K1 = M + 1;
+  static constexpr int NQ32 = K1 * K1 * 6;                 // FP32 values per pair in storage
+  static constexpr int CHF = 6 * M * 8;                    // floats of one block row of a record
+  static constexpr uint32_t kRecBytes = M * CHF * 4;       // operator blocks of one record
+  static constexpr int RECF = M * CHF + 8;                 // record stride in shared memory: 4
+                                                           // consecutive records start on distinct banks
+  static constexpr int kRecs = 16;                         // records per half tile
+  static constexpr uint32_t kStageBytes = kRecs * RECF * 4;
+  static constexpr uint32_t kTxBytes = kRecs * kRecBytes;
+  static constexpr int XS = 18;                            // x row stride (doubles, 16-byte aligned rows)
+  static constexpr size_t kX = (size_t)2 * 2 * kStoreTile * XS * 8;     // [buf][side][16][XS]
+  static constexpr size_t kWI = (size_t)2 * 2 * 8 * 4 * 12 * 8;        // [h][split][8][warp][12]
+  static constexpr size_t kWJ = (size_t)kStoreTile * 4 * 16 * 8;        // [16][h*2+split][16]
+  static constexpr size_t kBytes = 2 * (size_t)kStageBytes + kX + kWI + kWJ;
+  static constexpr int kThreads = 256;                     // two threads per pair of a half tile
+  static_assert(M3 <= 15, "z_j is reduced as 16 values");
+  static_assert(kRecs == 2 * (kThreads / 32), "lanes 0 and 1 of every warp copy one record each");
+};
+
+// Blocks [BB, BE) of split S (the 16-bit kernel's split) of one pair:
+// rec points at this pair's column (tl) of its record in shared memory.
+template <int M, int S>
+__device__ __forceinline__ void r64_half(const float* rec, const double* xjs, const double* xis, bool active,
+                                         double (&zj)[16], double* swi_slot, int lane) {
+  using HF = BulkHalf<M, S>;
+  using RS = R64Shape<M>;
+  double zi[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) zi[q] = 0.0;
+  if constexpr (HF::NBLK > 0) {
+    if (active) {
+      double xj[16], xi[12];
+      load_xrow<double, 16>(xjs, xj);
+#pragma unroll
+      for (int q = 0; q < 3 * HF::NR; ++q) xi[q] = xis[3 * HF::R0 + q];
+#pragma unroll
+      for (int b = 0; b < HF::NBLK; ++b) {
+        const int blk = HF::BB + b, kI = blk / M, kJ = blk % M;
+        double tv[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tv[c] = (double)rec[kI * RS::CHF + (kJ * 6 + c) * 8];
+        sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * (kI - HF::R0));
+        sym_mv_acc(tv, xi + 3 * (kI - HF::R0), zj + 3 * kJ);
+      }
+    }
+  }
+  reduce_scatter4x3(zi, lane, swi_slot);
+}
+
+template <int M>
+__global__ void __launch_bounds__(256, 1)
+k_struct_r64_bulk(int N, const float* __restrict__ S32, const double* __restrict__ x, double* __restrict__ zpart,
+                  const int* __restrict__ skip, int* __restrict__ err, uint32_t wait_polls) {
+  constexpr int M3 = 3 * M;
+  using RS = R64Shape<M>;
+  using H0 = BulkHalf<M, 0>;
+  using H1 = BulkHalf<M, 1>;
+  constexpr int XS = RS::XS;
+  if (skip != nullptr && *skip) return;
+  extern __shared__ __align__(128) unsigned char rsm[];
+  auto stage = [&](int s) { return reinterpret_cast<float*>(rsm + (size_t)s * RS::kStageBytes); };
+  double (*sx)[2][kStoreTile][XS] = reinterpret_cast<double (*)[2][kStoreTile][XS]>(rsm + 2 * RS::kStageBytes);
+  double (*swi)[2][8][4][12] =
+      reinterpret_cast<double (*)[2][8][4][12]>(rsm + 2 * RS::kStageBytes + RS::kX);
+  double (*swj)[4][16] = reinterpret_cast<double (*)[4][16]>(rsm + 2 * RS::kStageBytes + RS::kX + RS::kWI);
+  __shared__ __align__(8) uint64_t bar[2];
+  const int64_t ntiles = struct_store_tiles_dev(N);
+  const int64_t T16 = (N + kStoreTile - 1) / kStoreTile;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int split = t >> 7, p = t & 127, wq = (t >> 5) & 3;
+  const int subj = p >> 6, jl = (p >> 3) & 7, tl = p & 7;   // j side 8-group, j and i within it
+  const int j16 = subj * 8 + jl;
+  const int64_t R = (int64_t)M3 * N;
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(&bar[0], RS::kTxBytes);
+    mbar_expect_tx(&bar[1], RS::kTxBytes);
+  }
+  // half h of tile L into stage h: record r = 2 warp + lane (lanes 0, 1 of
+  // every warp), after thread 0 registered the bytes (expect) and a barrier
+  auto expect = [&](int h) {
+    if (t == 0) mbar_expect_tx(&bar[h], RS::kTxBytes);
+  };
+  auto issue = [&](int64_t L, int h) {
+    if (lane < 2) {
+      const int r = 2 * warp + lane;
+      const float* src = S32 + (L * 32 + 16 * h + r) * (int64_t)RS::NQ32 * 8;
+      bulk_g2s(stage(h) + r * RS::RECF, src, RS::kRecBytes, &bar[h]);
+    }
+  };
+  // x rows of a tile: element e < 2*16*M3 (thread t owns e = t and t + 256)
+  auto xval = [&](int e, bool valid, int I16, int J16) -> double {
+    if (e >= 2 * kStoreTile * M3 || !valid) return 0.0;
+    const int side = e / (kStoreTile * M3), rem = e % (kStoreTile * M3);
+    const int f = (side == 0 ? I16 : J16) * kStoreTile + rem / M3;
+    return f < N ? x[(int64_t)f * M3 + rem % M3] : 0.0;
+  };
+  auto xstore = [&](int buf, int e, double v) {
+    if (e < 2 * kStoreTile * M3) {
+      const int side = e / (kStoreTile * M3), rem = e % (kStoreTile * M3);
+      sx[buf][side][rem / M3][rem % M3] = v;
+    }
+  };
+  int cI = 0, cJ = 0;
+  tile_pair16f(blockIdx.x, cI, cJ);
+  xstore(0, t, xval(t, true, cI, cJ));
+  xstore(0, t + 256, xval(t + 256, true, cI, cJ));
+  __syncthreads();
+  issue(blockIdx.x, 0);
+  issue(blockIdx.x, 1);
+  bool failed = false, fail_more = false;
+  int k = 0, fail_h = 0;
+  for (int64_t L = blockIdx.x; L < ntiles; L += gridDim.x, ++k) {
+    const int xb = k & 1;
+    const uint32_t parity = k & 1;
+    const int I16 = cI, J16 = cJ;
+    const bool diag = I16 == J16;
+    const bool more = L + gridDim.x < ntiles;
+    if (more) tile_pair16f(L + gridDim.x, cI, cJ);
+    const double xn0 = xval(t, more, cI, cJ), xn1 = xval(t + 256, more, cI, cJ);
+    const int j = J16 * kStoreTile + j16;
+    const double* xjs = sx[xb][1][j16];
+    for (int h = 0; h < 2; ++h) {
+      const bool ok_wait = mbar_wait_bounded(&bar[h], parity, wait_polls);
+      if (__syncthreads_or(!ok_wait)) {
+        failed = true;
+        fail_h = h;
+        fail_more = more;
+        break;
+      }
+      const int i = I16 * kStoreTile + 8 * h + tl;
+      const bool active = i < j && j < N;
+      const float* rec = stage(h) + (subj * 8 + jl) * RS::RECF + tl;
+      const double* xis = sx[xb][0][8 * h + tl];
+      double zj[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) zj[q] = 0.0;
+      if (split == 0) r64_half<M, 0>(rec, xjs, xis, active, zj, swi[h][0][tl][wq], lane);
+      else r64_half<M, 1>(rec, xjs, xis, active, zj, swi[h][1][tl][wq], lane);
+      double y0, y1;
+      reduce_scatter8(zj, lane, y0, y1);
+      swj[j16][2 * h + split][2 * tl] = y0;
+      swj[j16][2 * h + split][2 * tl + 1] = y1;
+      if (h == 1) {
+        xstore(xb ^ 1, t, xn0);
+        xstore(xb ^ 1, t + 256, xn1);
+      }
+      if (more) expect(h);
+      __syncthreads();
+      // stage h is free again: the same half of the next tile
+      if (more) issue(L + gridDim.x, h);
+    }
+    if (failed) break;
+    // partial rows of this tile: i side to slot J, j side to slot I (diagonal: slot T16)
+    for (int task = t; task < 2 * kStoreTile * M3; task += blockDim.x) {
+      const int side = task / (kStoreTile * M3), rem = task % (kStoreTile * M3);
+      const int rf = rem / M3, rv = rem % M3;
+      if (side == 0) {
+        const int h = rf >> 3, il = rf & 7, kI = rv / 3;
+        const bool in0 = H0::NR > 0 && kI >= H0::R0 && kI < H0::R0 + H0::NR;
+        const bool in1 = H1::NR > 0 && kI >= H1::R0 && kI < H1::R0 + H1::NR;
+        const int q0 = in0 ? rv - 3 * H0::R0 : 0, q1 = in1 ? rv - 3 * H1::R0 : 0;
+        const double s0 = ((swi[h][0][il][0][q0] + swi[h][0][il][1][q0]) + swi[h][0][il][2][q0]) + swi[h][0][il][3][q0];
+        const double s1 = ((swi[h][1][il][0][q1] + swi[h][1][il][1][q1]) + swi[h][1][il][2][q1]) + swi[h][1][il][3][q1];
+        const double si = in0 ? (in1 ? s0 + s1 : s0) : s1;
+        const int fi = I16 * kStoreTile + rf;
+        if (fi < N) zpart[(int64_t)J16 * R + (int64_t)fi * M3 + rv] = si;
+      } else {
+        const double sj = ((swj[rf][0][rv] + swj[rf][1][rv]) + swj[rf][2][rv]) + swj[rf][3][rv];
+        const int fj = J16 * kStoreTile + rf;
+        if (fj < N) zpart[(diag ? T16 : (int64_t)I16) * R + (int64_t)fj * M3 + rv] = sj;
+      }
+    }
+  }
+  if (failed) {
+    if (t == 0) {
+      atomicExch(err, 1);
+      // drain (bounded): the copies this CTA still has in flight
+      const uint32_t ph = k & 1;
+      (void)mbar_wait_bounded(&bar[fail_h], ph);                       // the half that timed out
+      if (fail_h == 0) (void)mbar_wait_bounded(&bar[1], ph);           // this tile's second half
+      else if (fail_more) (void)mbar_wait_bounded(&bar[0], ph ^ 1u);   // the next tile's first half
     }
     __syncthreads();
   }
@@ -650,7 +860,7 @@ k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict_
       // receiving side i: rows P0 and P1 against x_j
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
-        const int q0 = (r * K1 + (kk + 1)) * 6;
+        const int q0 = s32_block(M, r, kk + 1) * 6;
 #pragma unroll
         for (int c = 0; c < 6; ++c) tv[c] = __ldcs(p + (q0 + c) * TI);
         sym_mv_acc(tv, xj + 3 * kk, vi + 3 * r);
@@ -658,7 +868,7 @@ k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict_
       // receiving side j: columns P0 and P1 against x_i
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
-        const int q0 = ((kk + 1) * K1 + r) * 6;
+        const int q0 = s32_block(M, kk + 1, r) * 6;
 #pragma unroll
         for (int c = 0; c < 6; ++c) tv[c] = __ldcs(p + (q0 + c) * TI);
         sym_mv_acc(tv, xi + 3 * kk, vj + 3 * r);
@@ -799,19 +1009,51 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
   return RF_OK;
 }
 
+template <int M>
+static int launch_r64_bulk(int N, const float* S32, const double* x, double* zpart, const int* skip, int* err,
+                           cudaStream_t st) {
+  using RS = R64Shape<M>;
+  static const cudaError_t attr = cudaFuncSetAttribute(k_struct_r64_bulk<M>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS::kBytes);
+  RF_CUDA_TRY(attr);
+  int dev = 0, nsm = 0;
+  RF_CUDA_TRY(cudaGetDevice(&dev));
+  RF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t ntiles = struct_store_tiles(N);
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
+  const int64_t lim = device_wait_limit();
+  const uint32_t polls = lim < 0 ? (1u << 24) : (uint32_t)std::min<int64_t>(lim, 1 << 24);
+  k_struct_r64_bulk<M><<<grid, RS::kThreads, RS::kBytes, st>>>(N, S32, x, zpart, skip, err, polls);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
 int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
-                             double* zpart64, const float* b, float* r, const int* skip, cudaStream_t st) {
+                             double* zpart64, const float* b, float* r, const int* skip, int* err, cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
+  // FP32 blocks staged by TMA bulk copies where that kernel is built (M <= 5, Q = 24, err given)
+  const bool bulk = err != nullptr && tab.Q == 24 && tab.M <= 5;
+  if (bulk) {
+    switch (tab.M) {
+      case 1: rc = launch_r64_bulk<1>(N, S32, x, zpart64, skip, err, st); break;
+      case 2: rc = launch_r64_bulk<2>(N, S32, x, zpart64, skip, err, st); break;
+      case 3: rc = launch_r64_bulk<3>(N, S32, x, zpart64, skip, err, st); break;
+      case 4: rc = launch_r64_bulk<4>(N, S32, x, zpart64, skip, err, st); break;
+      case 5: rc = launch_r64_bulk<5>(N, S32, x, zpart64, skip, err, st); break;
+    }
+  } else {
 #define RF_Z_CASE(MM, QQ) \
   if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(0, true, N, S32, nullptr, x, zpart64, skip, st);
-  RF_FOR_EACH_MQ(RF_Z_CASE)
+    RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
+  }
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
   const int64_t R = 3 * n;
   const int nparts = (int)ceil_div(N, kStoreTile);
-  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, nparts, R, zpart64 + (int64_t)nparts * R,
-                                                                 skip);
+  // the bulk kernel also fills slot nparts (diagonal tiles' j side), which is the output row
+  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, bulk ? nparts + 1 : nparts, R,
+                                                                 zpart64 + (int64_t)nparts * R, skip);
   RF_LAUNCH_CHECK();
   k_struct_finalize<double, double, true><<<fin_blocks(n), 256, 0, st>>>(
       tab, N, ori, x, zpart64 + (int64_t)nparts * R, 1, b, r, skip);
