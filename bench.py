@@ -512,11 +512,11 @@ def run_ours(args, dist):
         bytes_per_matvec = 2.0 * 150 * N * (N - 1) / 2
     achieved = bytes_per_matvec / (mv_avg_ms / 1000.0) / 1e9 if head["mv_launches"] else None
     # DRAM traffic per launch from one ncu capture of the same kernel at N=1500
-    # (dram__bytes_read.sum 347.6 MB + dram__bytes_write.sum 9.4 MB for 1124250
+    # (dram__bytes_read.sum 347.6 MB + dram__bytes_write.sum 9.8 MB for 1124250
     # unordered pairs: 304-byte records for 300 algorithmic bytes, x, partial
     # rows; profiles/struct_z16_bulk_N1500.md), scaled by the pairs one launch
     # processes; not captured for the dense FP32 kernel
-    traffic = 357.0e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision != "fp32" else None
+    traffic = 357.4e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision != "fp32" else None
     roof = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
             "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
