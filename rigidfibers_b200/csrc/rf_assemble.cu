@@ -58,12 +58,16 @@ struct AsmShape {
   // that phase 2, where consecutive threads read consecutive columns, is free
   // of bank conflicts), then the T blocks (6 floats each)
   static constexpr int GS = U + 1;
-  static constexpr size_t kGBytes = sizeof(float) * NC * GS;
+  // the T blocks start on a 16-byte boundary (they are copied out as float4);
+  // NC * GS is odd for odd M + 1
+  static constexpr int GOFF = (NC * GS + 3) / 4 * 4;
+  static constexpr size_t kGBytes = sizeof(float) * GOFF;
   // T pair stride padded so that 8 consecutive pairs start on distinct banks
   // that are multiples of 4 (stride = 4 * odd mod 32)
   static constexpr int TP = (K1 * K1 * 6 + 7) / 8 * 8 + 4;
   static constexpr size_t kTBytes = sizeof(float) * TI * TP;
   static constexpr size_t kSmem = kGBytes + 2 * kTBytes;   // T double-buffered across j
+  static_assert(GOFF % 4 == 0 && TP % 4 == 0, "T buffers must be 16-byte aligned");
   // structured storage
   static constexpr int SUB = kStoreTile / TI;      // assembly tiles per storage-tile side
   static constexpr int NQ32 = K1 * K1 * 6;         // FP32 values per pair
@@ -100,7 +104,7 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
   extern __shared__ __align__(16) float smem_dyn[];
   float (*sG)[S::GS] = reinterpret_cast<float (*)[S::GS]>(smem_dyn);                          // [NC][GS]
-  float* const sTbase = smem_dyn + NC * S::GS;                                               // 2 x [TI][TP]
+  float* const sTbase = smem_dyn + S::GOFF;                                                  // 2 x [TI][TP]
   __shared__ float sCoef[kMaxTerms], sEig[kMaxTerms];
   __shared__ float sfJ[TI][FF];
   __shared__ short sMapS[S::NQ32];   // stored value q (s32_block order) -> offset of its T entry within a pair

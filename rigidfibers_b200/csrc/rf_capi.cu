@@ -852,7 +852,14 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
                                 &h->ctl->timeout, h->st));
   } else {
     RF_CUDA_TRY(cudaMemcpyAsync(h->x64, hx.data(), R * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    RF_TRY(launch_struct_apply64(h->tab, h->N, h->S32, h->ori32, h->x64, h->zpart64, dy, h->st));
+    RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
+    RF_TRY(launch_struct_apply64(h->tab, h->N, h->S32, h->ori32, h->x64, h->zpart64, dy, &h->ctl->timeout, h->st));
+  }
+  if (h->mixed) {
+    int timed_out = 0;
+    RF_CUDA_TRY(cudaMemcpyAsync(&timed_out, &h->ctl->timeout, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    if (timed_out) { set_last_error_str("a bounded device-side wait timed out"); return RF_E_TIMEOUT; }
   }
   RF_CUDA_TRY(cudaMemcpyAsync(hy.data(), dy, R * sizeof(float), cudaMemcpyDeviceToHost, h->st));
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));

@@ -55,9 +55,9 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
 // err as for launch_struct_matvec (null: the register-staged kernel).
 int launch_struct_residual64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
                              double* zpart64, const float* b, float* r, const int* skip, int* err, cudaStream_t st);
-// y = A x with the FP32 blocks, x and accumulation in FP64.
+// y = A x with the FP32 blocks, x and accumulation in FP64 (err as for the residual).
 int launch_struct_apply64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
-                          double* zpart64, float* y, cudaStream_t st);
+                          double* zpart64, float* y, int* err, cudaStream_t st);
 // velocities from the FP32 blocks; vpart: ceil(N/16) x N x 6 floats.
 int launch_struct_velocity(const Tables& tab, int N, const float* S32, const float4* ori, const float* F,
                            const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);

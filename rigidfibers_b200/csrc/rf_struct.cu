@@ -1062,18 +1062,29 @@ int launch_struct_residual64(const Tables& tab, int N, const float* S32, const f
 }
 
 int launch_struct_apply64(const Tables& tab, int N, const float* S32, const float4* ori, const double* x,
-                          double* zpart64, float* y, cudaStream_t st) {
+                          double* zpart64, float* y, int* err, cudaStream_t st) {
   int rc = RF_E_UNSUPPORTED;
+  const bool bulk = err != nullptr && tab.Q == 24 && tab.M <= 5;
+  if (bulk) {
+    switch (tab.M) {
+      case 1: rc = launch_r64_bulk<1>(N, S32, x, zpart64, nullptr, err, st); break;
+      case 2: rc = launch_r64_bulk<2>(N, S32, x, zpart64, nullptr, err, st); break;
+      case 3: rc = launch_r64_bulk<3>(N, S32, x, zpart64, nullptr, err, st); break;
+      case 4: rc = launch_r64_bulk<4>(N, S32, x, zpart64, nullptr, err, st); break;
+      case 5: rc = launch_r64_bulk<5>(N, S32, x, zpart64, nullptr, err, st); break;
+    }
+  } else {
 #define RF_Z_CASE(MM, QQ) \
   if (tab.M == MM && tab.Q == QQ && QQ == 24) rc = launch_z<MM, 8>(0, true, N, S32, nullptr, x, zpart64, nullptr, st);
-  RF_FOR_EACH_MQ(RF_Z_CASE)
+    RF_FOR_EACH_MQ(RF_Z_CASE)
 #undef RF_Z_CASE
+  }
   if (rc != RF_OK) return rc;
   const int64_t n = (int64_t)N * tab.M;
   const int64_t R = 3 * n;
   const int nparts = (int)ceil_div(N, kStoreTile);
-  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, nparts, R, zpart64 + (int64_t)nparts * R,
-                                                                 nullptr);
+  k_sum_parts<double><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart64, bulk ? nparts + 1 : nparts, R,
+                                                                 zpart64 + (int64_t)nparts * R, nullptr);
   RF_LAUNCH_CHECK();
   k_struct_finalize<double, double, false><<<fin_blocks(n), 256, 0, st>>>(
       tab, N, ori, x, zpart64 + (int64_t)nparts * R, 1, nullptr, y, nullptr);

@@ -48,6 +48,25 @@ def test_structured_operator_matches_dense(n, prec):
         assert _rel(b, b64) <= max(2e-6, 2 * _rel(b32, b64))
 
 
+@pytest.mark.parametrize("m", [1, 2, 3, 4, 6])
+@pytest.mark.parametrize("n", [17, 40])
+def test_structured_operator_other_force_terms(m, n):
+    """The TMA-staged kernels split a pair's M^2 blocks between two threads at
+    a 16-byte boundary of its record (M <= 5); M > 5 uses the register-staged
+    kernels.  Same bounds as the M = 5 test."""
+    pos, ori = sphere_layout(n, radius=max(1.5, 0.8 * n ** (1 / 3)), seed=31 + n + m)
+    sim = _sim(pos, ori, precision="mixed_fp16", number_of_terms_in_force_expansion=m)
+    sim.assembleSystem()
+    p = O.Params(M=m)
+    A64, _ = O.assemble(pos, ori, p, False, np.float64)
+    A32, _ = O.assemble(pos, ori, p, False, np.float32)
+    x = np.random.default_rng(n + m).standard_normal(3 * m * n)
+    yref = A64 @ x
+    y32ref = A32.astype(np.float64) @ x
+    assert _rel(sim.apply_operator(x, 0), yref) <= max(2e-6, 2 * _rel(y32ref, yref))
+    assert _rel(sim.apply_operator(x, 1), yref) <= 2e-3
+
+
 def _run(sim, nsteps):
     out = []
     for t in range(nsteps):
