@@ -136,6 +136,21 @@ int rf_step(rf_handle* h, int current_timestep);
 /* rf_step over `nsteps` steps starting at `first_timestep`. */
 int rf_run(rf_handle* h, int first_timestep, int nsteps);
 
+/* Packed solves of many small suspensions (no reference counterpart: the
+ * ensemble path of the serving loop).  One launch solves the assembled
+ * systems of n handles, one CTA each, with the algorithm rf_solve runs in the
+ * mixed modes (GMRES-IR, FP64 residual).  Members: mixed precision, GMRES,
+ * 5 force terms, 8x3 quadrature, at most 128 fibers, one restart length.  A
+ * member's result depends only on its own data, so it is the same alone and
+ * in any pack (it may differ from rf_solve's in the last bits: the sums run
+ * in another order).  Returns RF_E_NAN / RF_E_NOCONV if a member ended so;
+ * rf_last_stats has each member's counts. */
+int rf_solve_packed(rf_handle** handles, int n);
+/* One time step of n suspensions with a packed solve: rf_assemble on each,
+ * rf_solve_packed, rf_update_velocities and rf_update_fibers on each.
+ * status[i] receives each member's result (RF_OK, RF_E_NOCONV, RF_E_NAN, ...). */
+int rf_step_packed(rf_handle** handles, const int* timesteps, int n, int* status);
+
 /* State and dumps (src/simulation.cu:530-822 write these to files). */
 int rf_get_state(rf_handle* h, double* pos, double* ori);
 int rf_set_state(rf_handle* h, const double* pos, const double* ori);
@@ -240,9 +255,13 @@ enum rf_request_status { RF_REQ_QUEUED = 0, RF_REQ_RUNNING = 1, RF_REQ_DONE = 2,
 typedef struct rf_server rf_server;
 
 typedef struct rf_server_config {
-  int max_active;            /* requests running at once */
+  int max_active;            /* requests running at once on their own handles */
   int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
   int use_cuda_graphs;       /* rf_set_cuda_graphs for every request's handle */
+  int pack_max_fibers;       /* requests of at most this many fibers (<= 128, mixed
+                                precision, GMRES, 5 terms, 8x3 quadrature) step together
+                                with packed solves (rf_step_packed); 0: off */
+  int pack_max_members;      /* suspensions per pack */
 } rf_server_config;
 
 typedef struct rf_request_stats {

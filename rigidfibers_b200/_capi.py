@@ -76,7 +76,8 @@ RF_REQ_QUEUED, RF_REQ_RUNNING, RF_REQ_DONE, RF_REQ_FAILED, RF_REQ_CANCELLED = ra
 
 
 class rf_server_config(ctypes.Structure):
-    _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64), ("use_cuda_graphs", ctypes.c_int)]
+    _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64), ("use_cuda_graphs", ctypes.c_int),
+                ("pack_max_fibers", ctypes.c_int), ("pack_max_members", ctypes.c_int)]
 
 
 class rf_request_stats(ctypes.Structure):
@@ -119,6 +120,9 @@ SIGNATURES = {
     "rf_update_fibers": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_step": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_run": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int]),
+    "rf_solve_packed": (ctypes.c_int, [ctypes.POINTER(_H), ctypes.c_int]),
+    "rf_step_packed": (ctypes.c_int, [ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int)]),
     "rf_get_state": (ctypes.c_int, [_H, _P, _P]),
     "rf_set_state": (ctypes.c_int, [_H, _P, _P]),
     "rf_get_velocities": (ctypes.c_int, [_H, _P, _P]),

@@ -169,6 +169,8 @@ struct rf_handle {
   float4* fw = nullptr;
   float* vpart = nullptr;
   cudaEvent_t ev[8];
+  cudaEvent_t order_ev = nullptr;   // orders this handle's stream before a packed solve
+  int pack_status = RF_OK;          // this handle's result in the last packed solve
   rf_stats stats;
   // optional per-launch timing of the solve's matvec kernels
   bool profile = false;
@@ -226,6 +228,7 @@ struct rf_handle {
     if (lu.host_perm) cudaFreeHost(lu.host_perm);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    if (order_ev) cudaEventDestroy(order_ev);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -746,6 +749,152 @@ int rf_step(rf_handle* h, int t) {
   h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
   h->stats.kernel_launches = h->launches;
   return rc;
+}
+
+// ---- packed solves of many small suspensions ------------------------------
+// One launch solves every handle's assembled system (k_pack_gmres_ir: one CTA
+// per suspension, the rf_solve algorithm for the mixed modes); each handle's
+// result depends only on its own data.
+int rf_solve_packed(rf_handle** hs, int n) {
+  if (!hs || n < 1) return RF_E_INPUT;
+  int m = -1, Rmax = 0;
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    if (!h) return RF_E_INPUT;
+    if (!h->assembled) { set_last_error_str("rf_solve_packed before rf_assemble"); return RF_E_STATE; }
+    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers) {
+      set_last_error_str("rf_solve_packed: mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 128 fibers");
+      return RF_E_UNSUPPORTED;
+    }
+    if (m >= 0 && h->restart != m) { set_last_error_str("rf_solve_packed: one restart length per pack"); return RF_E_INPUT; }
+    m = h->restart;
+    Rmax = std::max<int>(Rmax, (int)h->R);
+  }
+  rf_handle* h0 = hs[0];
+  cudaStream_t st = h0->st;
+  // every member's assembly (on its own stream) before the packed launch
+  for (int i = 1; i < n; ++i) {
+    rf_handle* h = hs[i];
+    if (!h->order_ev) RF_CUDA_TRY(cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming));
+    RF_CUDA_TRY(cudaEventRecord(h->order_ev, h->st));
+    RF_CUDA_TRY(cudaStreamWaitEvent(st, h->order_ev, 0));
+  }
+  const size_t bm = (size_t)n * sizeof(PackMember), bo = (size_t)n * 4 * sizeof(int), br = (size_t)n * sizeof(double);
+  unsigned char* dbuf = nullptr;
+  RF_CUDA_TRY(cudaMallocAsync((void**)&dbuf, bm + bo + br, st));
+  PackMember* dm = reinterpret_cast<PackMember*>(dbuf);
+  double* drel = reinterpret_cast<double*>(dbuf + bm);
+  int* dout = reinterpret_cast<int*>(dbuf + bm + br);
+  std::vector<PackMember> pm((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    PackMember& q = pm[(size_t)i];
+    std::memset(&q, 0, sizeof(q));
+    q.N = h->N;
+    q.smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+    q.maxit = h->cfg.gmres_max_iterations;
+    q.tol = h->cfg.refinement_tolerance;
+    q.S16 = h->S16;
+    q.S32 = h->S32;
+    q.ori = h->ori32;
+    q.b = h->b;
+    q.x64 = h->x64;
+    q.x = h->x;
+    q.V = h->V;
+    q.ldv = ceil_div(h->R, 32) * 32;
+    q.out = dout + 4 * i;
+    q.relres = drel + i;
+    for (int k = 0; k < 5; ++k) {
+      q.coef[k] = h->tab.gamma[k];
+      q.eig[k] = h->tab.eigen[k];
+    }
+    RF_CUDA_TRY(cudaEventRecord(h->ev[2], st));
+  }
+  RF_CUDA_TRY(cudaMemcpyAsync(dm, pm.data(), bm, cudaMemcpyHostToDevice, st));
+  int rc = launch_pack_gmres_ir(dm, n, Rmax, m, st);
+  std::vector<int> out((size_t)n * 4, 0);
+  std::vector<double> rel((size_t)n, 0.0);
+  if (rc == RF_OK) {
+    RF_CUDA_TRY(cudaMemcpyAsync(out.data(), dout, bo, cudaMemcpyDeviceToHost, st));
+    RF_CUDA_TRY(cudaMemcpyAsync(rel.data(), drel, br, cudaMemcpyDeviceToHost, st));
+  }
+  for (int i = 0; i < n; ++i) RF_CUDA_TRY(cudaEventRecord(hs[i]->ev[3], st));
+  RF_CUDA_TRY(cudaFreeAsync(dbuf, st));
+  // the members' next work is enqueued after this returns, so after the solve
+  RF_CUDA_TRY(cudaStreamSynchronize(st));
+  if (rc != RF_OK) return rc;
+  int worst = RF_OK;
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    const int* o = &out[(size_t)i * 4];
+    h->launches += (i == 0) ? 1 : 0;
+    h->matvecs_done = o[0];
+    h->refinements = o[2];
+    h->stats.iterations = o[0];
+    h->stats.restarts = o[1];
+    h->stats.refinement_steps = o[2];
+    h->stats.relative_residual = rel[(size_t)i];
+    h->stats.graph_replays = 0;
+    h->pack_status = o[3] == 0 ? RF_OK : (o[3] == 1 ? RF_E_NOCONV : RF_E_NAN);
+    if (h->pack_status != RF_E_NAN) h->solved = true;
+    if (h->pack_status == RF_E_NAN) worst = RF_E_NAN;
+    else if (h->pack_status == RF_E_NOCONV && worst == RF_OK) worst = RF_E_NOCONV;
+  }
+  return worst;
+}
+
+int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
+  if (!hs || !timesteps || !status || n < 1) return RF_E_INPUT;
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i]) return RF_E_INPUT;
+    hs[i]->launches = 0;
+    status[i] = RF_OK;
+  }
+  nvtxRangePushA("rf_step_packed");
+  struct Pop {
+    ~Pop() { nvtxRangePop(); }
+  } pop;
+  // members whose assembly fails keep that status and sit out this step
+  std::vector<rf_handle*> ok;
+  for (int i = 0; i < n; ++i) {
+    status[i] = rf_assemble(hs[i]);
+    if (status[i] == RF_OK) ok.push_back(hs[i]);
+  }
+  if (!ok.empty()) {
+    const int rc = rf_solve_packed(ok.data(), (int)ok.size());
+    if (rc != RF_OK && rc != RF_E_NOCONV && rc != RF_E_NAN) {
+      for (int i = 0; i < n; ++i)
+        if (status[i] == RF_OK) status[i] = rc;
+      return rc;
+    }
+  }
+  std::vector<int> vbad((size_t)n, 0), stepped((size_t)n, 0);
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    if (status[i] != RF_OK) continue;
+    status[i] = h->pack_status;
+    if (status[i] == RF_E_NAN) continue;
+    int r2 = rf_update_velocities(h);
+    if (r2 == RF_OK) r2 = rf_update_fibers(h, timesteps[i] == 0);
+    if (r2 != RF_OK) { status[i] = r2; continue; }
+    RF_CUDA_TRY(cudaMemcpyAsync(&vbad[(size_t)i], h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    stepped[(size_t)i] = 1;
+  }
+  int worst = RF_OK;
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    if (stepped[(size_t)i]) {
+      if (vbad[(size_t)i]) status[i] = RF_E_NAN;
+      h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
+      h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
+      h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
+      h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
+      h->stats.kernel_launches = h->launches;
+    }
+    if (status[i] != RF_OK && status[i] != RF_E_NOCONV && worst == RF_OK) worst = status[i];
+  }
+  return worst;
 }
 
 int rf_run(rf_handle* h, int first_timestep, int nsteps) {

@@ -63,6 +63,27 @@ int launch_struct_velocity(const Tables& tab, int N, const float* S32, const flo
                            const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t st);
 
+// Packed mixed-precision solves (csrc/rf_pack.cu): one CTA per suspension of
+// at most kPackMaxFibers fibers, M = 5, Q = 24 storage.
+constexpr int kPackMaxFibers = 128;
+struct PackMember {
+  int N, smode, maxit, pad;      // smode 1 FP16, 2 BF16 blocks; maxit: Arnoldi steps in total
+  double tol;                    // relative to ||b||
+  const uint32_t* S16;
+  const float* S32;
+  const float4* ori;
+  const float* b;
+  double* x64;                   // solution (FP64)
+  float* x;                      // solution (FP32 copy)
+  float* V;                      // Krylov basis, m + 1 columns of ldv floats
+  int64_t ldv;
+  int* out;                      // iterations, restarts, refinements, status (0 ok, 1 no convergence, 2 non-finite)
+  double* relres;                // ||b - A x|| / ||b|| at the last check
+  float coef[5], eig[5];         // C_k = coef_k (I - E_k t t^T), k >= 1; coef_0 t t^T
+};
+size_t pack_smem_bytes(int Rmax, int m);
+int launch_pack_gmres_ir(const PackMember* members, int n, int Rmax, int m, cudaStream_t st);
+
 }  // namespace rf
 
 namespace rf {

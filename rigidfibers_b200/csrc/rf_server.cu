@@ -7,8 +7,12 @@
 // and memory free up.  Each admitted request gets its own handle (device-
 // resident fibers, Krylov state, previous-step velocities) and stream, driven
 // by a worker thread; the streams of all running requests overlap on the
-// device.  Every kernel is deterministic (fixed-order reductions, no
-// atomics), so a request's result does not depend on what runs beside it.
+// device.  Small requests (at most pack_max_fibers fibers, mixed precision)
+// instead join a pack: one worker thread steps all of them together, their
+// systems solved by one launch per step (rf_step_packed, one CTA per
+// suspension); they join and leave the pack between steps.  Every kernel is
+// deterministic (fixed-order reductions, no atomics), so a request's result
+// does not depend on what runs beside it.
 // The reference has no serving layer; this is the ensemble workload of the
 // thesis' parameter studies run as a service.
 #include <algorithm>
@@ -45,8 +49,17 @@ struct Request {
   bool cancel = false;
   double t_submit = 0, t_start = 0, t_end = 0;
   std::vector<double> step_ms;
+  bool packed = false;                // stepped by the pack worker
   std::thread worker;
 };
+
+// a configuration the packed solve takes (rf_solve_packed's conditions)
+bool packable(const rf_config& c, int N, int max_fibers) {
+  return max_fibers > 0 && N <= std::min(max_fibers, rf::kPackMaxFibers) &&
+         (c.precision == RF_PREC_MIXED_FP16 || c.precision == RF_PREC_MIXED_BF16) &&
+         c.solver == RF_SOLVER_GMRES && c.number_of_terms_in_force_expansion == 5 &&
+         c.number_of_quadrature_intervals == 8 && c.number_of_quadrature_points_per_interval == 3;
+}
 
 }  // namespace
 
@@ -66,6 +79,11 @@ struct rf_server {
   int peak_active = 0;
   bool stopping = false;
   std::thread dispatcher;
+  // pack of small requests
+  std::condition_variable pack_cv;
+  std::vector<Request*> pack_pending;   // admitted, not yet in the pack
+  int packed_active = 0;
+  std::thread pack_worker;
   std::vector<double> all_step_ms;
   int64_t fiber_steps = 0;
   double t0 = 0, t_last = 0;
@@ -74,6 +92,8 @@ struct rf_server {
 static double now_s() {
   return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
 }
+
+static void finish_locked(rf_server* s, Request* r, int rc, const std::vector<double>& lat);
 
 static void run_request(rf_server* s, Request* r) {
   cudaSetDevice(s->device);
@@ -106,6 +126,13 @@ static void run_request(rf_server* s, Request* r) {
     rf_destroy(h);
   }
   std::lock_guard<std::mutex> lk(s->mu);
+  s->active -= 1;
+  s->finished_workers.push_back(std::move(r->worker));
+  finish_locked(s, r, rc, lat);
+}
+
+// record the end of a request (lock held)
+static void finish_locked(rf_server* s, Request* r, int rc, const std::vector<double>& lat) {
   r->t_end = now_s();
   r->step_ms = lat;
   r->error = rc;
@@ -115,11 +142,102 @@ static void run_request(rf_server* s, Request* r) {
     s->fiber_steps += (int64_t)r->N * (int64_t)lat.size();
   }
   s->t_last = r->t_end;
-  s->active -= 1;
   s->bytes_in_use -= r->bytes;
-  s->finished_workers.push_back(std::move(r->worker));
   s->cv.notify_all();
   s->done_cv.notify_all();
+}
+
+// The pack: every small request admitted steps once per round; the
+// suspensions of one restart length share an rf_step_packed call.
+static void pack_loop(rf_server* s) {
+  cudaSetDevice(s->device);
+  struct Member {
+    Request* r;
+    rf_handle* h;
+    int t;
+    std::vector<double> lat;
+  };
+  std::vector<Member> mem;
+  for (;;) {
+    std::vector<Request*> joining;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (mem.empty() && s->pack_pending.empty()) {
+        if (s->stopping) return;
+        s->pack_cv.wait_for(lk, std::chrono::milliseconds(50));
+        continue;
+      }
+      joining.swap(s->pack_pending);
+    }
+    for (Request* r : joining) {
+      rf_handle* h = nullptr;
+      const int rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
+      if (rc != RF_OK) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        finish_locked(s, r, rc, {});
+        s->packed_active -= 1;
+        continue;
+      }
+      mem.push_back({r, h, 0, {}});
+    }
+    // members that are done or cancelled leave before the step
+    auto leave = [&](size_t k, int rc) {
+      Member& q = mem[k];
+      if (rc == RF_OK) {
+        rf_get_state(q.h, q.r->pos.data(), q.r->ori.data());
+        if (q.t > 0) rf_get_velocities(q.h, q.r->tvel.data(), q.r->rvel.data());
+      }
+      rf_destroy(q.h);
+      std::lock_guard<std::mutex> lk(s->mu);
+      finish_locked(s, q.r, rc, q.lat);
+      s->packed_active -= 1;
+      mem.erase(mem.begin() + (std::ptrdiff_t)k);
+    };
+    for (size_t k = mem.size(); k-- > 0;) {
+      bool cancel;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        cancel = mem[k].r->cancel;
+      }
+      if (cancel || mem[k].t >= mem[k].r->nsteps) leave(k, RF_OK);
+    }
+    if (mem.empty()) continue;
+    // one packed step per restart length
+    std::map<int, std::vector<size_t>> groups;
+    for (size_t k = 0; k < mem.size(); ++k) {
+      const rf_config& c = mem[k].r->cfg;
+      groups[c.refinement_restart > 0 ? c.refinement_restart : c.gmres_restart].push_back(k);
+    }
+    std::vector<int> failed(mem.size(), RF_OK);
+    for (auto& g : groups) {
+      const size_t n = g.second.size();
+      for (size_t a = 0; a < n; a += (size_t)s->cfg.pack_max_members) {
+        const size_t nb = std::min(n - a, (size_t)s->cfg.pack_max_members);
+        std::vector<rf_handle*> hs(nb);
+        std::vector<int> ts(nb), st(nb, RF_OK);
+        for (size_t q = 0; q < nb; ++q) {
+          hs[q] = mem[g.second[a + q]].h;
+          ts[q] = mem[g.second[a + q]].t;
+        }
+        const auto t0 = Clock::now();
+        rf_step_packed(hs.data(), ts.data(), (int)nb, st.data());
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        for (size_t q = 0; q < nb; ++q) {
+          Member& mm = mem[g.second[a + q]];
+          if (st[q] == RF_OK || st[q] == RF_E_NOCONV) {
+            mm.t += 1;
+            mm.lat.push_back(ms);
+            std::lock_guard<std::mutex> lk(s->mu);
+            mm.r->steps_done = mm.t;
+          } else {
+            failed[g.second[a + q]] = st[q];
+          }
+        }
+      }
+    }
+    for (size_t k = mem.size(); k-- > 0;)
+      if (failed[k] != RF_OK) leave(k, failed[k]);
+  }
 }
 
 static void dispatch_loop(rf_server* s) {
@@ -133,7 +251,7 @@ static void dispatch_loop(rf_server* s) {
       if (t.joinable()) t.join();
       lk.lock();
     }
-    if (s->stopping && s->active == 0) return;
+    if (s->stopping && s->active == 0 && s->packed_active == 0) return;
     bool admitted = false;
     while (!s->stopping && !s->queue.empty()) {
       Request* r = s->reqs[s->queue.front()].get();
@@ -143,15 +261,30 @@ static void dispatch_loop(rf_server* s) {
         s->done_cv.notify_all();
         continue;
       }
+      const int running = s->active + s->packed_active;
+      if (r->packed) {
+        if (running > 0 && s->bytes_in_use + r->bytes > s->cfg.hbm_budget_bytes) break;   // wait for memory
+        s->queue.pop_front();
+        r->status = RF_REQ_RUNNING;
+        r->t_start = now_s();
+        s->packed_active += 1;
+        s->bytes_in_use += r->bytes;
+        s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
+        s->peak_active = std::max(s->peak_active, s->active + s->packed_active);
+        s->pack_pending.push_back(r);
+        s->pack_cv.notify_all();
+        admitted = true;
+        continue;
+      }
       if (s->active >= s->cfg.max_active) break;
-      if (s->active > 0 && s->bytes_in_use + r->bytes > s->cfg.hbm_budget_bytes) break;   // wait for memory
+      if (running > 0 && s->bytes_in_use + r->bytes > s->cfg.hbm_budget_bytes) break;   // wait for memory
       s->queue.pop_front();
       r->status = RF_REQ_RUNNING;
       r->t_start = now_s();
       s->active += 1;
       s->bytes_in_use += r->bytes;
       s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
-      s->peak_active = std::max(s->peak_active, s->active);
+      s->peak_active = std::max(s->peak_active, s->active + s->packed_active);
       r->worker = std::thread(run_request, s, r);
       admitted = true;
     }
@@ -166,6 +299,8 @@ int rf_server_config_default(rf_server_config* c) {
   std::memset(c, 0, sizeof(*c));
   c->max_active = 16;
   c->use_cuda_graphs = 1;
+  c->pack_max_fibers = 0;
+  c->pack_max_members = 148;
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c->hbm_budget_bytes = (int64_t)(0.8 * (double)fr);
   else c->hbm_budget_bytes = (int64_t)64 << 30;
@@ -173,8 +308,9 @@ int rf_server_config_default(rf_server_config* c) {
 }
 
 int rf_server_create(const rf_server_config* cfg, rf_server** out) {
-  if (!cfg || !out || cfg->max_active < 1 || cfg->hbm_budget_bytes <= 0) {
-    rf::set_last_error_str("rf_server_create: max_active >= 1 and a positive memory budget");
+  if (!cfg || !out || cfg->max_active < 1 || cfg->hbm_budget_bytes <= 0 || cfg->pack_max_fibers < 0 ||
+      (cfg->pack_max_fibers > 0 && cfg->pack_max_members < 1)) {
+    rf::set_last_error_str("rf_server_create: max_active >= 1, a positive memory budget, pack_max_members >= 1");
     return RF_E_INPUT;
   }
   rf_server* s = new rf_server();
@@ -182,6 +318,7 @@ int rf_server_create(const rf_server_config* cfg, rf_server** out) {
   cudaGetDevice(&s->device);
   s->t0 = now_s();
   s->dispatcher = std::thread(dispatch_loop, s);
+  if (cfg->pack_max_fibers > 0) s->pack_worker = std::thread(pack_loop, s);
   *out = s;
   return RF_OK;
 }
@@ -199,6 +336,7 @@ int rf_server_submit(rf_server* s, const rf_config* cfg, int N, const double* po
   r->rvel.assign(3 * (size_t)N, 0.0);
   r->bytes = rf_device_bytes_estimate(cfg, N);   // also validates the configuration
   if (r->bytes < 0) return RF_E_INPUT;
+  r->packed = packable(*cfg, N, s->cfg.pack_max_fibers);
   r->t_submit = now_s();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stopping) return RF_E_STATE;
@@ -250,7 +388,7 @@ int rf_server_drain(rf_server* s, double timeout_s) {
   if (!s) return RF_E_INPUT;
   std::unique_lock<std::mutex> lk(s->mu);
   const bool ok = s->done_cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                                      [&] { return s->queue.empty() && s->active == 0; });
+                                      [&] { return s->queue.empty() && s->active == 0 && s->packed_active == 0; });
   return ok ? RF_OK : RF_E_TIMEOUT;
 }
 
@@ -308,7 +446,7 @@ int rf_server_get_stats(rf_server* s, rf_server_stats* out) {
   out->completed = done;
   out->failed = failed;
   out->queued = queued;
-  out->active = s->active;
+  out->active = s->active + s->packed_active;
   return RF_OK;
 }
 
@@ -321,6 +459,11 @@ int rf_server_destroy(rf_server* s) {
     s->cv.notify_all();
   }
   if (s->dispatcher.joinable()) s->dispatcher.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->pack_cv.notify_all();
+  }
+  if (s->pack_worker.joinable()) s->pack_worker.join();
   for (auto& kv : s->reqs)
     if (kv.second->worker.joinable()) kv.second->worker.join();
   for (auto& t : s->finished_workers)

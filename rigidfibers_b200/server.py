@@ -9,7 +9,9 @@
 
 The reference runs one suspension per process (fibers_runner.py:17-162);
 here many suspensions share one GPU: admission in arrival order by free slot
-and device-memory budget, one handle and stream per running suspension.
+and device-memory budget, one handle and stream per running suspension; with
+pack_max_fibers > 0 the small ones step together, their systems solved by
+one launch per step (rf_step_packed).
 """
 import ctypes
 
@@ -33,7 +35,8 @@ def device_bytes(config, number_of_fibers):
 
 
 class Server:
-    def __init__(self, max_active=None, hbm_budget_bytes=None, use_cuda_graphs=None):
+    def __init__(self, max_active=None, hbm_budget_bytes=None, use_cuda_graphs=None, pack_max_fibers=None,
+                 pack_max_members=None):
         self._lib = C.load()
         sc = C.rf_server_config()
         C.check(self._lib.rf_server_config_default(ctypes.byref(sc)), "rf_server_config_default")
@@ -43,6 +46,11 @@ class Server:
             sc.hbm_budget_bytes = int(hbm_budget_bytes)
         if use_cuda_graphs is not None:
             sc.use_cuda_graphs = int(bool(use_cuda_graphs))
+        if pack_max_fibers is not None:
+            sc.pack_max_fibers = int(pack_max_fibers)
+        if pack_max_members is not None:
+            sc.pack_max_members = int(pack_max_members)
+        self.pack_max_fibers = sc.pack_max_fibers
         self.max_active = sc.max_active
         self.hbm_budget_bytes = sc.hbm_budget_bytes
         s = ctypes.c_void_p()

@@ -214,3 +214,32 @@ class Simulation:
         s = C.rf_stats()
         C.check(self._lib.rf_last_stats(self._h, ctypes.byref(s)), "rf_last_stats")
         return {k: getattr(s, k) for k, _ in C.rf_stats._fields_}
+
+
+# -- packed solves of many small suspensions --------------------------------
+def _handles(sims):
+    arr = (ctypes.c_void_p * len(sims))()
+    for k, s in enumerate(sims):
+        arr[k] = s._h
+    return arr
+
+
+def solve_packed(sims, allow_noconv=False):
+    """Solve the assembled systems of several small mixed-precision
+    suspensions with one launch (rf_solve_packed)."""
+    lib = C.load()
+    allow = (C.RF_E_NOCONV,) if allow_noconv else ()
+    return C.check(lib.rf_solve_packed(_handles(sims), len(sims)), "rf_solve_packed", allow)
+
+
+def step_packed(sims, timesteps):
+    """One time step of several small suspensions with a packed solve
+    (rf_step_packed); returns the per-suspension status codes."""
+    lib = C.load()
+    ts = (ctypes.c_int * len(sims))(*[int(t) for t in timesteps])
+    st = (ctypes.c_int * len(sims))()
+    rc = lib.rf_step_packed(_handles(sims), ts, len(sims), st)
+    codes = list(st)
+    if rc not in (C.RF_OK, C.RF_E_NOCONV) and all(c == C.RF_OK for c in codes):
+        C.check(rc, "rf_step_packed")
+    return codes

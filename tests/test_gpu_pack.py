@@ -1,0 +1,146 @@
+"""Packed solves of many small suspensions: rf_solve_packed / rf_step_packed
+(one CTA per suspension) and the server's pack.
+
+Bounds (written here): the packed solution within 1e-5 relative of rf_solve's
+(both run GMRES-IR to a relative residual of 1e-6; only the summation order
+differs) and within 1e-4 of the FP64 oracle's direct solve; a suspension's
+result bit for bit the same alone and in a pack.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rigidfibers_b200.generate import sphere_layout
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _layout(n, seed):
+    # the serving workload's density: circumscribed-sphere volume fraction 1 %
+    return sphere_layout(n, max(1.5, (100.0 * n) ** (1.0 / 3.0)), 0.2, seed=seed)
+
+
+def _sim(pos, ori, **kw):
+    from rigidfibers_b200 import Config, Simulation
+    return Simulation(Config(**kw), pos, ori)
+
+
+@pytest.mark.parametrize("prec", ["mixed_fp16", "mixed_bf16"])
+@pytest.mark.parametrize("n", [1, 7, 16, 33, 100, 128])
+def test_packed_solve_matches_rf_solve_and_fp64(prec, n):
+    from rigidfibers_b200.simulation import solve_packed
+    pos, ori = _layout(n, 100 + n)
+    a = _sim(pos, ori, precision=prec)
+    a.assembleSystem()
+    a.solveSystem()
+    xa = a.solution()
+    b = _sim(pos, ori, precision=prec)
+    b.assembleSystem()
+    solve_packed([b])
+    xb = b.solution()
+    st = b.stats()
+    assert st["relative_residual"] <= 1e-6
+    assert _rel(xb, xa) <= 1e-5
+    A64, b64 = O.assemble(pos, ori, O.Params(), False, np.float64)
+    x64 = np.linalg.solve(A64, b64) if n > 1 else np.zeros_like(b64)
+    assert _rel(xb, x64) <= 1e-4
+    if n > 1:
+        assert st["iterations"] >= 1 and st["refinement_steps"] >= 1
+
+
+def test_member_is_the_same_alone_and_in_a_pack():
+    from rigidfibers_b200.simulation import solve_packed, step_packed
+    lays = {"a": (_layout(40, 1), dict(precision="mixed_bf16")),
+            "b": (_layout(100, 2), dict(precision="mixed_bf16", slenderness=0.005)),
+            "c": (_layout(7, 3), dict(precision="mixed_bf16"))}
+    alone = _sim(*lays["a"][0], **lays["a"][1])
+    alone.assembleSystem()
+    solve_packed([alone])
+    x_alone = alone.solution()
+    mix = {k: _sim(*v[0], **v[1]) for k, v in lays.items()}
+    for s in mix.values():
+        s.assembleSystem()
+    solve_packed([mix["b"], mix["a"], mix["c"]])
+    assert np.array_equal(mix["a"].solution(), x_alone)
+    # whole steps: three of them, alone and beside two others
+    one = _sim(*lays["a"][0], **lays["a"][1])
+    many = [_sim(*lays[k][0], **lays[k][1]) for k in ("c", "a", "b")]
+    for t in range(3):
+        assert step_packed([one], [t]) == [0]
+        assert step_packed(many, [t, t, t]) == [0, 0, 0]
+    p1, o1 = one.state()
+    p2, o2 = many[1].state()
+    assert np.array_equal(p1, p2) and np.array_equal(o1, o2)
+
+
+def test_packed_steps_follow_rf_step():
+    from rigidfibers_b200.simulation import step_packed
+    pos, ori = _layout(60, 9)
+    ref = _sim(pos, ori, precision="mixed_fp16")
+    pk = _sim(pos, ori, precision="mixed_fp16")
+    for t in range(2):
+        ref.step(t)
+        assert step_packed([pk], [t]) == [0]
+    for a, b in zip(pk.state(), ref.state()):
+        assert _rel(a, b) <= 1e-6
+    for a, b in zip(pk.velocities(), ref.velocities()):
+        assert _rel(a, b) <= 1e-5
+    st = pk.stats()
+    assert st["ms_solve_system"] > 0 and st["ms_assemble_system"] > 0
+
+
+def test_packed_solve_refuses_what_it_does_not_take():
+    from rigidfibers_b200 import _capi as C
+    from rigidfibers_b200.simulation import solve_packed
+    pos, ori = _layout(20, 5)
+    fp32 = _sim(pos, ori)
+    fp32.assembleSystem()
+    with pytest.raises(C.RigidFibersError) as e:
+        solve_packed([fp32])
+    assert e.value.status == C.RF_E_UNSUPPORTED
+    big = _sim(*_layout(129, 6), precision="mixed_bf16")
+    big.assembleSystem()
+    with pytest.raises(C.RigidFibersError) as e:
+        solve_packed([big])
+    assert e.value.status == C.RF_E_UNSUPPORTED
+    fresh = _sim(pos, ori, precision="mixed_bf16")
+    with pytest.raises(C.RigidFibersError) as e:
+        solve_packed([fresh])
+    assert e.value.status == C.RF_E_STATE
+    m10 = _sim(pos, ori, precision="mixed_bf16")
+    m20 = _sim(pos, ori, precision="mixed_bf16", refinement_restart=20)
+    m10.assembleSystem()
+    m20.assembleSystem()
+    with pytest.raises(C.RigidFibersError) as e:
+        solve_packed([m10, m20])
+    assert e.value.status == C.RF_E_INPUT
+
+
+def test_server_pack_result_alone_equals_result_in_the_mix():
+    from rigidfibers_b200 import Config
+    from rigidfibers_b200.server import Server
+    small = _layout(24, 11)
+    cfg = Config(precision="mixed_bf16")
+    with Server(max_active=4, pack_max_fibers=64) as srv:
+        rid = srv.submit(cfg, *small, nsteps=4)
+        srv.drain(timeout=300)
+        ref = srv.result(rid)
+    with Server(max_active=4, pack_max_fibers=64) as srv:
+        ids = [srv.submit(Config(precision="mixed_bf16", slenderness=0.005), *_layout(50, 12), nsteps=6),
+               srv.submit(cfg, *small, nsteps=4),
+               srv.submit(Config(precision="mixed_bf16"), *_layout(300, 13), nsteps=3),   # its own handle
+               srv.submit(cfg, *_layout(9, 14), nsteps=2)]
+        srv.drain(timeout=300)
+        assert [srv.poll(i)[0] for i in ids] == ["done"] * 4
+        got = srv.result(ids[1])
+        st = srv.stats()
+    for a, b in zip(ref[:4], got[:4]):
+        assert np.array_equal(a, b)
+    assert got[4]["steps_done"] == 4
+    assert st["completed"] == 4 and st["steps"] == 6 + 4 + 3 + 2

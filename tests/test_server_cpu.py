@@ -79,3 +79,37 @@ def test_requests_fail_cleanly_without_a_device():
             srv.result(ids[0])
         st = srv.stats()
         assert st["failed"] == 5 and st["active"] == 0
+
+
+def test_pack_config_and_validation():
+    lib = C.load()
+    sc = C.rf_server_config()
+    assert lib.rf_server_config_default(ctypes.byref(sc)) == C.RF_OK
+    assert sc.pack_max_fibers == 0 and sc.pack_max_members >= 1
+    sc.pack_max_fibers = 64
+    sc.pack_max_members = 0
+    s = ctypes.c_void_p()
+    assert lib.rf_server_create(ctypes.byref(sc), ctypes.byref(s)) == C.RF_E_INPUT
+    # packed entry points check their arguments before touching a device
+    assert lib.rf_solve_packed(None, 1) == C.RF_E_INPUT
+    hs = (ctypes.c_void_p * 1)()
+    assert lib.rf_solve_packed(hs, 0) == C.RF_E_INPUT
+    assert lib.rf_solve_packed(hs, 1) == C.RF_E_INPUT          # a null handle
+    ts = (ctypes.c_int * 1)()
+    st = (ctypes.c_int * 1)()
+    assert lib.rf_step_packed(hs, ts, 1, st) == C.RF_E_INPUT
+
+
+def test_packed_requests_fail_cleanly_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present; the GPU tests cover execution")
+    from rigidfibers_b200.server import Server
+    pos = np.random.default_rng(1).uniform(-3, 3, (12, 3))
+    ori = np.tile([0.0, 0.0, 1.0], (12, 1))
+    with Server(max_active=2, hbm_budget_bytes=1 << 34, pack_max_fibers=64) as srv:
+        ids = [srv.submit(_cfg(precision="mixed_bf16"), pos, ori, 2) for _ in range(4)]
+        ids.append(srv.submit(_cfg(), pos, ori, 2))                 # FP32: not packed
+        srv.drain(timeout=60)
+        assert [srv.poll(i)[0] for i in ids] == ["failed"] * 5
+        assert srv.stats()["active"] == 0
