@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--serve-max-active", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-graphs", type=int, default=1, help="replay GMRES cycles from CUDA graphs (1) or not (0)")
+    ap.add_argument("--serve-pack-fibers", type=int, default=0,
+                    help="requests of at most this many fibers step together with packed solves (0: off)")
+    ap.add_argument("--serve-pack-compare", type=int, default=64,
+                    help="also run the ensemble with packed solves for requests of at most this many fibers, "
+                         "reported as serving_packed (0: skip)")
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
     ap.add_argument("--legs", default="headline,serving,direct",
@@ -397,7 +402,7 @@ def error_vs_fp64(precision, n=300):
     return err
 
 
-def serve_ensemble(args, dist):
+def serve_ensemble(args, dist, pack_fibers=None):
     """The served ensemble: independent suspensions (N log-uniform in
     [16, 1000], eps in {0.01, 0.005}, 5-50 steps, BF16 pair blocks) arriving
     as a Poisson stream into one rf_server; per-step latency percentiles and
@@ -413,7 +418,8 @@ def serve_ensemble(args, dist):
     rng = np.random.default_rng(5 + dist.rank)
     gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
     dist.barrier()
-    with Server(max_active=args.serve_max_active, use_cuda_graphs=args.serve_graphs) as srv:
+    pack = args.serve_pack_fibers if pack_fibers is None else pack_fibers
+    with Server(max_active=args.serve_max_active, use_cuda_graphs=args.serve_graphs, pack_max_fibers=pack) as srv:
         t0 = time.perf_counter()
         due = t0
         for r, (p, o), c, g in zip(reqs, layouts, cfgs, gaps):
@@ -433,7 +439,7 @@ def serve_ensemble(args, dist):
             "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"],
             "fiber_steps_per_s": fiber_steps / wall_max, "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
             "max_active": args.serve_max_active, "peak_active": st["peak_active"],
-            "cuda_graphs": bool(args.serve_graphs),
+            "cuda_graphs": bool(args.serve_graphs), "pack_max_fibers": pack,
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps in {0.01, 0.005}, 5-50 steps, volume fraction 1%, "
                         "M=5, 8x3 quadrature, Poisson arrivals; latency = host wall time of one rf_step "
@@ -550,6 +556,8 @@ def run_ours(args, dist):
     }
     if args.serve_requests > 0:
         out["serving"] = serve_ensemble(args, dist)
+        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
+            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
     if args.direct_fibers > 0 and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
     if comparison:
@@ -573,6 +581,8 @@ def run_legs(args, dist):
     out = {"legs": sorted(legs)}
     if "serving" in legs:
         out["serving"] = serve_ensemble(args, dist)
+        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
+            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
     if "direct" in legs and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
     if dist.rank == 0:

@@ -854,6 +854,8 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   struct Pop {
     ~Pop() { nvtxRangePop(); }
   } pop;
+  // each member's assembly, velocities and update run on its own stream (so
+  // they overlap on the device); the solve is the one shared launch
   // members whose assembly fails keep that status and sit out this step
   std::vector<rf_handle*> ok;
   for (int i = 0; i < n; ++i) {
