@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
+#include <thread>
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
@@ -843,6 +844,25 @@ int rf_solve_packed(rf_handle** hs, int n) {
   return worst;
 }
 
+// fn(i) for i < n from up to 8 host threads (members of a pack are
+// independent: each one's launches go to its own stream)
+static void for_members(int n, const std::function<void(int)>& fn) {
+  const int nt = std::min(8, std::max(1, n / 8));
+  if (nt == 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::vector<std::thread> th;
+  for (int k = 0; k < nt; ++k)
+    th.emplace_back([&, k] {
+      cudaSetDevice(dev);
+      for (int i = k; i < n; i += nt) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
+
 int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   if (!hs || !timesteps || !status || n < 1) return RF_E_INPUT;
   for (int i = 0; i < n; ++i) {
@@ -855,13 +875,13 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
     ~Pop() { nvtxRangePop(); }
   } pop;
   // each member's assembly, velocities and update run on its own stream (so
-  // they overlap on the device); the solve is the one shared launch
-  // members whose assembly fails keep that status and sit out this step
+  // they overlap on the device), issued from several host threads; the solve
+  // is the one shared launch.  Members whose assembly fails keep that status
+  // and sit out this step.
+  for_members(n, [&](int i) { status[i] = rf_assemble(hs[i]); });
   std::vector<rf_handle*> ok;
-  for (int i = 0; i < n; ++i) {
-    status[i] = rf_assemble(hs[i]);
+  for (int i = 0; i < n; ++i)
     if (status[i] == RF_OK) ok.push_back(hs[i]);
-  }
   if (!ok.empty()) {
     const int rc = rf_solve_packed(ok.data(), (int)ok.size());
     if (rc != RF_OK && rc != RF_E_NOCONV && rc != RF_E_NAN) {
@@ -870,32 +890,30 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
       return rc;
     }
   }
-  std::vector<int> vbad((size_t)n, 0), stepped((size_t)n, 0);
-  for (int i = 0; i < n; ++i) {
+  auto finish = [&](int i) -> int {
     rf_handle* h = hs[i];
-    if (status[i] != RF_OK) continue;
-    status[i] = h->pack_status;
-    if (status[i] == RF_E_NAN) continue;
-    int r2 = rf_update_velocities(h);
-    if (r2 == RF_OK) r2 = rf_update_fibers(h, timesteps[i] == 0);
-    if (r2 != RF_OK) { status[i] = r2; continue; }
-    RF_CUDA_TRY(cudaMemcpyAsync(&vbad[(size_t)i], h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    stepped[(size_t)i] = 1;
-  }
-  int worst = RF_OK;
-  for (int i = 0; i < n; ++i) {
-    rf_handle* h = hs[i];
+    if (status[i] != RF_OK) return status[i];
+    if (h->pack_status == RF_E_NAN) return RF_E_NAN;
+    RF_TRY(rf_update_velocities(h));
+    RF_TRY(rf_update_fibers(h, timesteps[i] == 0));
+    int vbad = 0;
+    RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     RF_CUDA_TRY(cudaStreamSynchronize(h->st));
-    if (stepped[(size_t)i]) {
-      if (vbad[(size_t)i]) status[i] = RF_E_NAN;
-      h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
-      h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
-      h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
-      h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
-      h->stats.kernel_launches = h->launches;
+    if (vbad) {
+      set_last_error_str("non-finite velocity");
+      return RF_E_NAN;
     }
+    h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
+    h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
+    h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
+    h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
+    h->stats.kernel_launches = h->launches;
+    return h->pack_status;
+  };
+  for_members(n, [&](int i) { status[i] = finish(i); });
+  int worst = RF_OK;
+  for (int i = 0; i < n; ++i)
     if (status[i] != RF_OK && status[i] != RF_E_NOCONV && worst == RF_OK) worst = status[i];
-  }
   return worst;
 }
 
