@@ -1,7 +1,7 @@
 """Mixed-precision path: structured operator (FP32 + 16-bit pair blocks),
 GMRES with FP64-residual refinement, velocities from the stored blocks.
 
-Bounds (written here, from the north star): forces, velocities and fiber
+Bounds (written here): forces, velocities and fiber
 state within 1e-4 relative of the FP64 oracle; the structured FP32 operator
 within twice the REAL*4 oracle's own error; the 16-bit operators within
 their storage precision (FP16 2e-3, BF16 1.5e-2 of the largest |y|).

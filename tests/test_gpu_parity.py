@@ -1,6 +1,6 @@
 """CUDA path against the oracle and the reference's golden vectors.
 
-Tolerances (FP32 plain path; north star: 1e-5 relative):
+Tolerances (FP32 plain path: 1e-5 relative):
   * assembled A and b vs the FP64 oracle: 2e-6 of the largest |entry|
   * golden fields: relative to the field's largest magnitude, 1e-5
 """
