@@ -169,16 +169,30 @@ static void pack_loop(rf_server* s) {
       }
       joining.swap(s->pack_pending);
     }
-    for (Request* r : joining) {
-      rf_handle* h = nullptr;
-      const int rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
-      if (rc != RF_OK) {
+    // new members' handles, created from several host threads
+    std::vector<rf_handle*> made(joining.size(), nullptr);
+    std::vector<int> mrc(joining.size(), RF_OK);
+    {
+      const size_t nt = std::min<size_t>(8, joining.size());
+      std::vector<std::thread> th;
+      for (size_t k = 0; k < nt; ++k)
+        th.emplace_back([&, k] {
+          cudaSetDevice(s->device);
+          for (size_t q = k; q < joining.size(); q += nt)
+            mrc[q] = rf_create(&joining[q]->cfg, joining[q]->N, joining[q]->pos.data(), joining[q]->ori.data(),
+                               &made[q]);
+        });
+      for (auto& x : th) x.join();
+    }
+    for (size_t q = 0; q < joining.size(); ++q) {
+      Request* r = joining[q];
+      if (mrc[q] != RF_OK) {
         std::lock_guard<std::mutex> lk(s->mu);
-        finish_locked(s, r, rc, {});
+        finish_locked(s, r, mrc[q], {});
         s->packed_active -= 1;
         continue;
       }
-      mem.push_back({r, h, 0, {}});
+      mem.push_back({r, made[q], 0, {}});
     }
     // members that are done or cancelled leave before the step
     auto leave = [&](size_t k, int rc) {
