@@ -830,6 +830,7 @@ int rf_solve_packed(rf_handle** hs, int n) {
     const int* o = &out[(size_t)i * 4];
     h->launches += (i == 0) ? 1 : 0;
     h->matvecs_done = o[0];
+    h->mv_used = 0;   // no per-launch matvec windows: the matvecs ran inside the packed kernel
     h->refinements = o[2];
     h->stats.iterations = o[0];
     h->stats.restarts = o[1];
