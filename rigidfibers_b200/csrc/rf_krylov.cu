@@ -388,7 +388,7 @@ void set_coop_block_cap(int cap) { t_coop_cap = cap; }
 int coop_blocks_per_sm_capped(int num_sms) { return t_coop_cap > 0 ? std::min(num_sms, t_coop_cap) : num_sms; }
 
 void GmresGraphCache::release() {
-  for (int v = 0; v < 2; ++v) {
+  for (int v = 0; v < kGmresGraphVariants; ++v) {
     if (exec[v]) cudaGraphExecDestroy(exec[v]);
     exec[v] = nullptr;
     state[v] = 0;
@@ -453,45 +453,54 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   res->launches = 2;
   GmresCtl h{};
   int cycles_run = 0;
-  // one restart cycle: [residual of x], residual kernel, m x (matvec + Arnoldi step), update
-  auto enqueue_cycle = [&](bool first) -> int {
+  // Pieces of the restart cycles, each launched directly or replayed from a
+  // CUDA graph: variant 0 the first cycle whole (residual kernel, m x (matvec
+  // + Arnoldi step), update); variant 1 the head of a later cycle (residual of
+  // x, residual kernel); variant 2 + c the c-th chunk of kGmresChunk (matvec +
+  // Arnoldi step) of a later cycle.  The host reads the control block after a
+  // head and after every chunk, so a cycle whose residual has converged, or
+  // whose Arnoldi steps have, launches nothing more.
+  auto chunk_end = [&](int c) { return std::min(m, (c + 1) * kGmresChunk); };
+  auto own_kernels = [&](int v) { return v == 0 ? 2 + m : v == 1 ? 1 : chunk_end(v - 2) - (v - 2) * kGmresChunk; };
+  auto enqueue = [&](int v) -> int {
     int mode = 0;
-    if (!first) {
+    if (v == 1) {
       const int rc = residual ? residual(x, s.V, &s.ctl->converged, st)
                               : matvec(static_cast<const float*>(x), &s.ctl->converged, st);
       if (rc) return rc;
       mode = residual ? 2 : 1;
     }
-    {
+    if (v <= 1) {
       void* args[] = {&a, &mode};
       const int rc = coop_launch((const void*)k_gmres_residual, nblk, 256, args, st);
       if (rc) return rc;
     }
-    for (int j = 0; j < m; ++j) {
+    if (v == 1) return RF_OK;
+    const int j0 = v == 0 ? 0 : (v - 2) * kGmresChunk, j1 = v == 0 ? m : chunk_end(v - 2);
+    for (int j = j0; j < j1; ++j) {
       int rc = matvec(s.V + (int64_t)j * s.ldv, &s.ctl->cycle_done, st);
       if (rc) return rc;
       void* args[] = {&a, &j};
       rc = coop_launch((const void*)k_gmres_arnoldi, nblk, 256, args, st);
       if (rc) return rc;
     }
-    k_gmres_update<<<nblk, 256, 0, st>>>(a);
-    RF_LAUNCH_CHECK();
+    if (v == 0) {
+      k_gmres_update<<<nblk, 256, 0, st>>>(a);
+      RF_LAUNCH_CHECK();
+    }
     return RF_OK;
   };
-  for (int cycle = 0;; ++cycle) {
-    ++cycles_run;
-    const bool first = cycle == 0;
-    const int v = first ? 0 : 1;
-    bool from_graph = false;
+  auto run = [&](int v) -> int {
     GmresGraphCache* gc = s.graphs;
+    bool from_graph = false;
     if (gc && gc->state[v] == 2) {
-      // capture this cycle once (the capture does not run it; the replay below
+      // capture this piece once (the capture does not run it; the replay below
       // does).  A variant is captured on its second use, so the kernels' one-time
       // set-up (function attributes) has run outside any capture.
       cudaGraph_t graph = nullptr;
       int rc = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess ? RF_OK : RF_E_CUDA;
       if (rc == RF_OK) {
-        rc = enqueue_cycle(first);
+        rc = enqueue(v);
         const cudaError_t ec = cudaStreamEndCapture(st, &graph);
         if (rc == RF_OK && ec == cudaSuccess && graph &&
             cudaGraphInstantiate(&gc->exec[v], graph, 0) == cudaSuccess) {
@@ -516,8 +525,8 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
       }
       cudaGetLastError();   // a refused capture leaves no sticky error; clear the non-sticky one
       if (gc->state[v] == 1) {
-        // the callbacks counted their kernels while capturing; count ours as a direct cycle does
-        res->launches += 2 + m + (first ? 0 : 1);
+        // the callbacks counted their kernels while capturing; count ours as a direct launch does
+        res->launches += own_kernels(v);
         RF_CUDA_TRY(cudaGraphLaunch(gc->exec[v], st));
         from_graph = true;
       }
@@ -529,16 +538,40 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
     if (from_graph) {
       ++res->graph_replays;
     } else {
-      const int rc = enqueue_cycle(first);
+      const int rc = enqueue(v);
       if (rc) return rc;
-      res->launches += 2 + m + (first ? 0 : 1);
+      res->launches += own_kernels(v);
       if (gc && gc->state[v] == 0) gc->state[v] = 2;
     }
+    return RF_OK;
+  };
+  auto read_ctl = [&]() -> int {
     RF_CUDA_TRY(cudaMemcpyAsync(s.host_ctl, s.ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, st));
     RF_CUDA_TRY(cudaStreamSynchronize(st));
     h = *s.host_ctl;
-    if (h.converged || h.nan || h.timeout) break;
-    if (h.total_iters >= s.maxit && cycle > 0 && h.jconv == 0) break;
+    return RF_OK;
+  };
+  for (int cycle = 0;; ++cycle) {
+    ++cycles_run;
+    if (cycle == 0) {
+      if (int rc = run(0)) return rc;
+      if (int rc = read_ctl()) return rc;
+      if (h.converged || h.nan || h.timeout) break;
+      continue;
+    }
+    if (int rc = run(1)) return rc;
+    if (int rc = read_ctl()) return rc;
+    // converged, failed, or out of iterations (the residual kernel then ends the cycle)
+    if (h.converged || h.nan || h.timeout || h.cycle_done) break;
+    for (int c = 0; c * kGmresChunk < m; ++c) {
+      if (int rc = run(2 + c)) return rc;
+      if (int rc = read_ctl()) return rc;
+      if (h.cycle_done || h.nan || h.timeout) break;
+    }
+    if (h.nan || h.timeout) break;
+    k_gmres_update<<<nblk, 256, 0, st>>>(a);
+    RF_LAUNCH_CHECK();
+    res->launches += 1;
     if (cycle > s.maxit + 2) break;
   }
   res->residual_calls = residual ? cycles_run - 1 : 0;

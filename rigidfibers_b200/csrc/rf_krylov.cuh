@@ -31,17 +31,22 @@ using MatvecFn = std::function<int(const float* x, const int* skip, cudaStream_t
 // operator / accumulation than the matvec's.
 using ResidualFn = std::function<int(const void* x, float* r, const int* skip, cudaStream_t st)>;
 
-// A restart cycle of GMRES captured as a CUDA graph: [0] the first cycle
-// (x = 0), [1] the later ones (residual of the current x first).  Kernel
+// Pieces of the GMRES restart cycles captured as CUDA graphs: [0] the first
+// cycle (x = 0), [1] the head of a later one (residual of the current x),
+// [2 + c] its c-th chunk of kGmresChunk Arnoldi steps.  Kernel
 // arguments and buffers are fixed per handle and the tolerance / iteration
 // limit live in the device control block, so a replay is exactly the launch
 // sequence it was captured from.  state: 0 not run yet, 2 run once directly
 // (captured on the next use), 1 ready, -1 capture not possible here (the cycle
 // is then launched directly).
+// Arnoldi steps between host checks in the cycles after the first
+constexpr int kGmresChunk = 4;
+// graph variants: the first cycle, a later cycle's head, its chunks
+constexpr int kGmresGraphVariants = 2 + (kMaxRestart + kGmresChunk - 1) / kGmresChunk;
 struct GmresGraphCache {
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  int state[2] = {0, 0};
-  int kernels[2] = {0, 0};   // kernel nodes per replay
+  cudaGraphExec_t exec[kGmresGraphVariants] = {};
+  int state[kGmresGraphVariants] = {};
+  int kernels[kGmresGraphVariants] = {};   // kernel nodes per replay
   void release();
 };
 
