@@ -40,7 +40,10 @@ def parse():
     ap.add_argument("--radius", type=float, default=18.0)
     ap.add_argument("--precision", default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-error-leg", action="store_true",
+                    help="skip the step errors against the FP64 reference at the benchmark configurations")
+    ap.add_argument("--reference-cap-s", type=float, default=1500.0,
+                    help="reference arm: stop timing CPU steps when the next one would end past this many seconds")
     ap.add_argument("--mixed-restart", type=int, default=20,
                     help="Arnoldi steps between FP64 residual corrections in mixed precision (0: GMRES restart)")
     ap.add_argument("--serve-requests", type=int, default=512,
@@ -56,15 +59,22 @@ def parse():
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
     ap.add_argument("--legs", default="headline,serving,direct",
-                    help="comma-separated subset of headline,serving,direct; a subset other than the default "
-                         "prints the requested legs only (for profiling one part)")
+                    help="comma-separated subset of headline,serving,direct,error,cpu; without headline only the "
+                         "requested legs are run and printed (for profiling one part)")
     return ap.parse_args()
 
 
-def workload(args):
+def workload_layout(fibers, radius=None):
+    """The seeded layout of the precision configuration: N fibers, centres in
+    a ball of radius 18 (N=4000; scaled as N^(1/3) by default for other N)."""
     from rigidfibers_b200.generate import layout_seed, sphere_layout
-    pos, ori = sphere_layout(args.fibers, args.radius, 0.2, seed=layout_seed(3, args.fibers))
-    return pos, ori
+    if radius is None:
+        radius = 18.0 * (fibers / 4000.0) ** (1.0 / 3.0)
+    return sphere_layout(fibers, radius, 0.2, seed=layout_seed(3, fibers))
+
+
+def workload(args):
+    return workload_layout(args.fibers, args.radius)
 
 
 def workload_name(args):
@@ -195,6 +205,15 @@ def peaks():
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 NOMINAL_TF32_TFLOPS = 1100.0
 
+# Flops the structured assembly kernel k_assemble_pairs<5,24,FP16,numerical>
+# executes per unordered fiber pair, from one ncu capture of that kernel at
+# N=1000 (499,500 pairs): thread instructions FFMA 295 M x 2 + FMUL 77 M +
+# FADD 68 M warp-instructions x 32 lanes = 23.5 GFLOP.  The kernel evaluates
+# the Stokeslet once per unordered pair and folds mirror quadrature points,
+# so this is what its FP32 pipes actually do; the reference algorithm counts
+# 2 x 67,923 for the same pair.
+ASM_EXEC_FLOPS_PER_PAIR = (295e6 * 2 + 77e6 + 68e6) * 32 / 499500.0
+
 
 def asm_flops_per_ordered_pair(M=5, Q=24):
     """The reference algorithm's assembly work per ordered fiber pair (K at
@@ -206,21 +225,21 @@ def asm_flops_per_ordered_pair(M=5, Q=24):
 
 def kernel_rooflines(N, head, hbm, mixed, direct=None):
     """Per-stage figures of the timed step (stage times from the timed pass):
-    the assembly as reference-algorithm FLOP/s against nominal FP32 and as
-    store bandwidth, the velocities from the stored blocks as read bandwidth,
-    the LU as 2/3 R^3 against nominal TF32, and the step as the sum of its
-    stages' bound times over the measured time."""
+    the assembly as executed FLOP/s (ncu instruction mix per unordered pair)
+    against nominal FP32 SIMT and as store bandwidth, the velocities from the
+    stored blocks as read bandwidth, the LU as 2/3 R^3 per second against
+    nominal TF32, and the step as the sum of its stages' bound times over the
+    measured time."""
     steps = max(head["steps"], 1)
     st = {k: v / steps for k, v in head["stage"].items()}
     pairs = N * (N - 1) / 2.0
-    asm_flops = asm_flops_per_ordered_pair() * N * (N - 1)
+    exec_flops = ASM_EXEC_FLOPS_PER_PAIR * pairs
     t_asm = st["assemble_system"] / 1e3
-    out = {"assembly": {"flops_per_ordered_pair": asm_flops_per_ordered_pair(),
-                        "achieved_tflops_equivalent": asm_flops / t_asm / 1e12 if t_asm else None,
+    out = {"assembly": {"executed_flops_per_unordered_pair": ASM_EXEC_FLOPS_PER_PAIR,
+                        "achieved_tflops": exec_flops / t_asm / 1e12 if t_asm else None,
                         "peak_tflops": NOMINAL_FP32_TFLOPS, "peak_kind": "nominal FP32 SIMT",
-                        "frac": asm_flops / t_asm / 1e12 / NOMINAL_FP32_TFLOPS if t_asm else None,
-                        "note": "above 1: K is evaluated once per unordered pair and mirror quadrature points "
-                                "are folded, so fewer flops run than the reference algorithm counts"}}
+                        "frac": exec_flops / t_asm / 1e12 / NOMINAL_FP32_TFLOPS if t_asm else None,
+                        "reference_flops_per_ordered_pair": asm_flops_per_ordered_pair()}}
     iters = head["iters"] / steps
     if mixed:
         store = pairs * (216 * 4 + 152 * 2)      # FP32 blocks + 16-bit records per unordered pair
@@ -239,11 +258,11 @@ def kernel_rooflines(N, head, hbm, mixed, direct=None):
     if vel_bytes:
         out["velocities"] = {"bytes": vel_bytes, "achieved_gbs": vel_bytes / t_vel / 1e9 if t_vel else None,
                              "peak_gbs": hbm, "frac": vel_bytes / t_vel / 1e9 / hbm if t_vel else None}
-    bound_ms = 1e3 * (asm_flops / (NOMINAL_FP32_TFLOPS * 1e12) + (iters * mv_bytes + refs * res_bytes) / (hbm * 1e9) +
+    bound_ms = 1e3 * (exec_flops / (NOMINAL_FP32_TFLOPS * 1e12) + (iters * mv_bytes + refs * res_bytes) / (hbm * 1e9) +
                       (vel_bytes or 0.0) / (hbm * 1e9))
     step_ms = head["ms"] / steps
     out["step"] = {"bound_ms": bound_ms, "measured_ms": step_ms, "frac": bound_ms / step_ms if step_ms else None,
-                   "bound": "assembly at nominal FP32 (reference flops) + matvecs and residuals at measured HBM"}
+                   "bound": "assembly's executed flops at nominal FP32 + matvecs and residuals at measured HBM"}
     if direct and "direct" in direct:
         tf = direct["direct"].get("tflops")
         out["lu"] = {"fibers": direct["fibers"], "achieved_tflops": tf, "peak_tflops": NOMINAL_TF32_TFLOPS,
@@ -252,77 +271,115 @@ def kernel_rooflines(N, head, hbm, mixed, direct=None):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (a C++ restatement of the reference's Fortran
-# path; the Fortran itself cannot be built here) on a bounded sample
+# CPU: the oracle (a C++ restatement of the reference's Fortran/OpenMP path;
+# the Fortran itself cannot be built here), full time steps on the host cores
 # ---------------------------------------------------------------------------
-def cpu_sample(pos, ori, iterations, cycles, target_s):
+def cpu_steps(pos, ori, timed, untimed=1, cap_s=None, analytical=False):
+    """The reference's time loop (fortran/fibers.f95:182-349) run by the oracle
+    in FP32 on all host cores: per step the full dense assembly (R x R FP32),
+    GMRES(10) to 1e-5 with its own iteration count (sgmres semantics), the
+    velocities and the fiber update.  `untimed` steps run first (the
+    reference's own timers exclude step 0); then up to `timed` timed steps, or
+    fewer when the next one would end past cap_s seconds of timed work."""
     from oracle import oracle as O
     p = O.Params()
-    N = pos.shape[0]
-    R = 15 * N
-    threads = O.lib().rfo_num_threads()
-    rng = np.random.default_rng(0)
-    coeff = (1e-3 * rng.standard_normal(R)).astype(np.float32)
-
-    def rows_cost(ns):
+    f32 = np.float32
+    cur_pos = np.array(pos, f32).reshape(-1, 3)
+    cur_ori = np.array(ori, f32).reshape(-1, 3)
+    prev_pos, prev_ori = cur_pos.copy(), cur_ori.copy()
+    prev_tv = np.zeros_like(cur_pos)
+    prev_rv = np.zeros_like(cur_pos)
+    recs = []
+    spent = 0.0
+    for t in range(untimed + timed):
         t0 = time.perf_counter()
-        slab, _ = O.assemble_rows(pos, ori, p, 0, ns, dtype=np.float32)
+        A, b = O.assemble(cur_pos, cur_ori, p, analytical, f32)
         t1 = time.perf_counter()
-        O.update_velocities(pos, ori, coeff, p, 0, ns, dtype=np.float32)
+        x, it, rel = O.solve(A, b, p, "gmres")
         t2 = time.perf_counter()
-        xg = rng.standard_normal(R).astype(np.float32)
-        reps = 3
+        del A
+        tv, rv = O.update_velocities(cur_pos, cur_ori, x, p, dtype=f32, analytical=analytical)
         t3 = time.perf_counter()
-        for _ in range(reps):
-            O.gemv(slab, xg)
+        npos, nori = O.update_fibers(t == 0, p.dt, prev_pos, cur_pos, prev_ori, cur_ori, prev_tv, tv, prev_rv, rv)
         t4 = time.perf_counter()
-        return t1 - t0, t2 - t1, (t4 - t3) / reps
+        if t >= untimed:
+            recs.append({"assemble_system": t1 - t0, "solve_system": t2 - t1, "update_velocities": t3 - t2,
+                         "update_fibers": t4 - t3, "total": t4 - t0, "iterations": it, "relres": rel})
+            spent += t4 - t0
+            if cap_s is not None and spent + (t4 - t0) > cap_s:
+                break
+        prev_pos, cur_pos = cur_pos, npos
+        prev_ori, cur_ori = cur_ori, nori
+        prev_tv, prev_rv = tv, rv
+    n = len(recs)
+    N = len(cur_pos)
+    total = sum(r["total"] for r in recs)
+    return {"value": N * n / total, "steps": n, "seconds_per_step": total / n, "cores": O.lib().rfo_num_threads(),
+            "stage_s_per_step": {k: sum(r[k] for r in recs) / n
+                                 for k in ("assemble_system", "solve_system", "update_velocities", "update_fibers")},
+            "gmres_iterations_per_step": sum(r["iterations"] for r in recs) / n,
+            "max_relative_residual": max(r["relres"] for r in recs)}
 
-    ns = max(1, min(N, threads))
-    ta, tv, tg = rows_cost(ns)
-    per = (ta + tv + (iterations + cycles) * tg) / ns
-    ns2 = int(min(N, max(ns, target_s / max(per, 1e-9))))
-    if ns2 > ns:
-        ns = ns2
-        ta, tv, tg = rows_cost(ns)
-    scale = N / ns
-    step_s = scale * (ta + tv + (iterations + cycles) * tg)
-    t0 = time.perf_counter()
-    z = np.zeros((N, 3), np.float32)
-    O.update_fibers(False, 0.1, pos.astype(np.float32), pos.astype(np.float32), ori.astype(np.float32),
-                    ori.astype(np.float32), z, z, z, z)
-    step_s += time.perf_counter() - t0
-    return {
-        "value": N / step_s, "unit": "fiber-steps/s", "cores": threads, "kind": "port",
-        "sample": ("C++ restatement of the reference's Fortran/OpenMP step (FP32, OpenMP over fibers): assembly and "
-                   "velocity rows of %d of %d fibers and a dense FP32 gemv over that row slab, scaled by N/%d; "
-                   "%d GMRES matvecs per step (iterations + restart residuals, from the GPU run)"
-                   % (ns, N, ns, iterations + cycles)),
-        "seconds_per_step": step_s,
-        "breakdown_s": {"assemble_system": scale * ta, "update_velocities": scale * tv,
-                        "solve_system": scale * (iterations + cycles) * tg},
-    }
+
+CPU_KIND = "port"
+CPU_WHAT = ("the oracle, a C++ restatement of the reference's Fortran/OpenMP time step (FP32, OpenMP over fibers, "
+            "full dense assembly, GMRES(10) to 1e-5 with sgmres semantics, velocities, fiber update)")
+
+
+def one_thread_sample(N, radius, fibers=32):
+    """Seconds per step on one host thread, from a bounded sample run in a
+    child process with OMP_NUM_THREADS=1: the assembly and velocity rows of
+    `fibers` fibers of the N-fiber workload and a GEMV over that row slab,
+    scaled by N / fibers (the rest of a step is O(N) or O(R) work)."""
+    code = ("import sys, time, json, numpy as np; sys.path.insert(0, %r)\n"
+            "from bench import workload_layout\n"
+            "from oracle import oracle as O\n"
+            "pos, ori = workload_layout(%d, %r)\n"
+            "p = O.Params(); ns = %d\n"
+            "t0 = time.perf_counter(); slab, _ = O.assemble_rows(pos, ori, p, 0, ns, dtype=np.float32)\n"
+            "t1 = time.perf_counter(); O.update_velocities(pos, ori, np.zeros(15 * len(pos), np.float32), p, 0, ns,"
+            " dtype=np.float32)\n"
+            "t2 = time.perf_counter(); O.gemv(slab, np.ones(slab.shape[1], np.float32)); t3 = time.perf_counter()\n"
+            "print(json.dumps({'asm': t1 - t0, 'vel': t2 - t1, 'gemv': t3 - t2, "
+            "'threads': O.lib().rfo_num_threads()}))\n") % (ROOT, N, radius, fibers)
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    try:
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+    except (subprocess.SubprocessError, ValueError, IndexError) as e:
+        return {"unavailable": str(e)[:200]}
+    return d
 
 
 def run_reference(args):
     pos, ori = workload(args)
-    iters = 20
-    cycles = 3
-    for _ in range(args.warmup):
-        cpu_sample(pos, ori, iters, cycles, 2.0)
-    vals = []
-    for _ in range(args.steps):
-        vals.append(cpu_sample(pos, ori, iters, cycles, max(1.0, args.cpu_seconds / 2)))
-    v = statistics.median(r["value"] for r in vals)
-    last = vals[-1]
+    res = cpu_steps(pos, ori, args.steps, untimed=1, cap_s=args.reference_cap_s)
+    v = res["value"]
+    one = one_thread_sample(args.fibers, args.radius)
+    if "asm" in one:
+        scale = args.fibers / 32.0
+        s1 = scale * (one["asm"] + one["vel"] + one["gemv"] * (res["gmres_iterations_per_step"] + 3))
+        one_thread = {"value": args.fibers / s1, "unit": "fiber-steps/s", "threads": one["threads"],
+                      "sample": "assembly and velocity rows of 32 of %d fibers and a GEMV over that slab "
+                                "(x %.1f GMRES matvecs per step), scaled by N/32" %
+                                (args.fibers, res["gmres_iterations_per_step"] + 3)}
+    else:
+        one_thread = one
+    sample = ("%s; %d full time steps of the N=%d workload timed (step 0, first-order, run untimed first as the "
+              "reference's timers exclude it)" % (CPU_WHAT, res["steps"], args.fibers))
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "fiber-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.fibers / v,
+        "steps": res["steps"], "warmup": 1, "ms_per_step": 1000.0 * res["seconds_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_name(args), "fibers": args.fibers, "radius": args.radius,
-                   "assumed_gmres_matvecs_per_step": iters + cycles},
-        "cpu_baseline": {k: last[k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "fiber-steps/s"},
+                   "precision": "fp32", "requested_steps": args.steps, "requested_warmup": args.warmup},
+        "cpu_baseline": {"kind": CPU_KIND, "cores": res["cores"], "sample": sample, "value": v,
+                         "unit": "fiber-steps/s"},
         "e2e": {"value": v, "unit": "fiber-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "stage_s_per_step": res["stage_s_per_step"],
+        "gmres_iterations_per_step": res["gmres_iterations_per_step"],
+        "max_relative_residual": res["max_relative_residual"],
+        "one_thread": one_thread,
     }
     print(json.dumps(out), flush=True)
 
@@ -330,12 +387,22 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def time_path(args, dist, cfg, pos, ori, clocks=None):
-    """Warm-up, K profiled steps (CUDA events around every matvec launch: the
-    roofline figures), then the same K steps again from a checkpoint taken
-    after the warm-up, device-timed with the library's defaults (no per-launch
-    events, GMRES cycles replayed as CUDA graphs; CUDA events on the handle's
-    stream)."""
+def _stream_of(lib, sim):
+    import ctypes
+
+    import torch
+    sp = ctypes.c_void_p()
+    lib.rf_get_stream(sim._h, ctypes.byref(sp))
+    return torch.cuda.ExternalStream(sp.value)
+
+
+def time_path(args, dist, cfg, pos, ori, clocks=None, profile=True):
+    """W warm-up steps and the autotuner, a checkpoint C, two steps that
+    capture the GMRES graphs (discarded: C is restored), then K steps from C
+    device-timed with the library's defaults (graph replay, no per-launch
+    events; CUDA events on the handle's stream), then the same K steps from C
+    again with CUDA events around every matvec launch (the roofline's
+    per-launch figures; those events rule out graph replay)."""
     import ctypes
 
     import torch
@@ -344,27 +411,19 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
     from rigidfibers_b200 import _capi as C
     lib = C.load()
     sim = Simulation(cfg, pos, ori)
-    sp = ctypes.c_void_p()
-    lib.rf_get_stream(sim._h, ctypes.byref(sp))
-    stream = torch.cuda.ExternalStream(sp.value)
+    stream = _stream_of(lib, sim)
     for t in range(args.warmup):
         sim.step(t)
-    tuned = sim.autotune()          # matvec launch choice, timed on this operator
-    after_warmup = sim.checkpoint()
-    acc = {"stage": {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0},
-           "iters": 0, "restarts": 0, "refinements": 0, "launches": 0, "mv_launches": 0, "mv_ms": 0.0, "relres": 0.0,
-           "graph_replays": 0}
+    tuned = sim.autotune()          # launch choices, timed on this operator
+    ckpt = sim.checkpoint()
     t = args.warmup
-    lib.rf_set_profiling(sim._h, 1)
-    for _ in range(args.steps):
+    for _ in range(2):
         sim.step(t)
         t += 1
-        nl, tm = ctypes.c_int(), ctypes.c_double()
-        lib.rf_matvec_profile(sim._h, ctypes.byref(nl), ctypes.byref(tm))
-        acc["mv_launches"] += nl.value
-        acc["mv_ms"] += tm.value
-    lib.rf_set_profiling(sim._h, 0)
-    t = sim.restore(after_warmup)
+    acc = {"stage": {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0},
+           "iters": 0, "restarts": 0, "refinements": 0, "launches": 0, "mv_launches": 0, "mv_ms": 0.0, "relres": 0.0,
+           "graph_replays": 0, "iters_per_step": []}
+    t = sim.restore(ckpt)
     dist.barrier()
     torch.cuda.synchronize()
     if clocks:
@@ -379,6 +438,7 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
         for k in acc["stage"]:
             acc["stage"][k] += st["ms_" + k]
         acc["iters"] += st["iterations"]
+        acc["iters_per_step"].append(st["iterations"])
         acc["restarts"] += st["restarts"]
         acc["refinements"] += st["refinement_steps"]
         acc["launches"] += st["kernel_launches"]
@@ -389,6 +449,17 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
     acc["clocks"] = clocks.stop() if clocks else None
     dist.barrier()
     acc["ms"] = e0.elapsed_time(e1)
+    if profile:
+        t = sim.restore(ckpt)
+        lib.rf_set_profiling(sim._h, 1)
+        for _ in range(args.steps):
+            sim.step(t)
+            t += 1
+            nl, tm = ctypes.c_int(), ctypes.c_double()
+            lib.rf_matvec_profile(sim._h, ctypes.byref(nl), ctypes.byref(tm))
+            acc["mv_launches"] += nl.value
+            acc["mv_ms"] += tm.value
+        lib.rf_set_profiling(sim._h, 0)
     acc["device_bytes"] = sim.stats()["device_bytes"]
     acc["autotune"] = tuned
     sim.close()
@@ -396,11 +467,13 @@ def time_path(args, dist, cfg, pos, ori, clocks=None):
 
 
 def e2e_path(args, dist, cfg, pos, ori):
-    """Through the C ABI with host buffers: every step uploads the fiber state
-    from pinned host memory and reads the new state back (W untimed rounds of
-    the same loop first, so the timed steps replay captured graphs as the
-    device-timed ones do).  Returns (max seconds over ranks, GMRES iterations
-    per step)."""
+    """The same K steps (from the state after the W warm-up steps) through the
+    C ABI with the run's state in host memory between steps: every step loads
+    the state it needs (positions and orientations of the current and previous
+    step, in FP64 and FP32, and the previous velocities: rf_checkpoint_load)
+    from pinned host memory, runs rf_step, and reads the next state back
+    (rf_checkpoint_save).  Host wall clock, max over ranks.  Returns (seconds,
+    GMRES iterations per step, bytes per copy)."""
     import ctypes
 
     import torch
@@ -408,60 +481,133 @@ def e2e_path(args, dist, cfg, pos, ori):
     from rigidfibers_b200 import Simulation
     from rigidfibers_b200 import _capi as C
     lib = C.load()
-    hpos = torch.from_numpy(np.ascontiguousarray(pos, np.float64)).pin_memory()
-    hori = torch.from_numpy(np.ascontiguousarray(ori, np.float64)).pin_memory()
-    out_pos = torch.empty_like(hpos).pin_memory()
-    out_ori = torch.empty_like(hori).pin_memory()
     sim = Simulation(cfg, pos, ori)
-    sim.step(0)
-
-    def one(t):
-        C.check(lib.rf_set_state(sim._h, ctypes.c_void_p(hpos.data_ptr()), ctypes.c_void_p(hori.data_ptr())),
-                "rf_set_state")
+    for t in range(args.warmup):
         sim.step(t)
-        C.check(lib.rf_get_state(sim._h, ctypes.c_void_p(out_pos.data_ptr()), ctypes.c_void_p(out_ori.data_ptr())),
-                "rf_get_state")
+    sim.autotune()                  # the cached choice of the device-timed pass
+    nbytes = lib.rf_checkpoint_bytes(sim._h)
+    host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    start = torch.empty_like(host).pin_memory()
+    hp = ctypes.c_void_p(host.data_ptr())
+    C.check(lib.rf_checkpoint_save(sim._h, ctypes.c_void_p(start.data_ptr()), nbytes), "rf_checkpoint_save")
+    taken = ctypes.c_int64()
+
+    def one():
+        C.check(lib.rf_checkpoint_load(sim._h, hp, nbytes, ctypes.byref(taken)), "rf_checkpoint_load")
+        sim.step(taken.value)
+        C.check(lib.rf_checkpoint_save(sim._h, hp, nbytes), "rf_checkpoint_save")
         return sim.stats()["iterations"]
 
-    for t in range(1, 1 + args.warmup):
-        one(t)
+    host.copy_(start)
+    for _ in range(2):              # captures the GMRES graphs; discarded
+        one()
+    host.copy_(start)
     dist.barrier()
     torch.cuda.synchronize()
     iters = 0
     t0 = time.perf_counter()
-    for t in range(1 + args.warmup, 1 + args.warmup + args.steps):
-        iters += one(t)
+    for _ in range(args.steps):
+        iters += one()
     torch.cuda.synchronize()
     s = dist.max(time.perf_counter() - t0)
     sim.close()
-    return s, iters / args.steps
+    return s, iters / args.steps, int(nbytes)
 
 
-def error_vs_fp64(precision, n=300):
-    """Relative error of the given path against the FP64 oracle (direct
-    solve) on a seeded layout of n fibers at the workload's density, 2 steps."""
+def fp64_reference_step(pos, ori, analytical=False):
+    """One time step (step 0: Euler update) of the reference method in FP64:
+    the oracle's FP64 assembly and velocities on the host cores, and the dense
+    FP64 system solved on the GPU by LU (torch.linalg.solve) as the checker.
+    Returns b, x, tvel, rvel and the next positions / orientations."""
+    import torch
+
     from oracle import oracle as O
-    from rigidfibers_b200 import Config, Simulation
-    from rigidfibers_b200.generate import layout_seed, sphere_layout
-    radius = 18.0 * (n / 4000.0) ** (1.0 / 3.0)
-    pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(3, n))
-    ref = O.run_steps(pos, ori, O.Params(), 2, solver="direct", dtype=np.float64)
-    sim = Simulation(Config(precision=precision), pos, ori)
-    err = {"fibers": n, "steps": 2}
-    for t in range(2):
-        sim.assembleSystem()
-        sim.solveSystem()
-        x = sim.solution()
-        sim.updateVelocities()
-        tv, rv = sim.velocities()
-        sim.updateFibers(t == 0)
-        p1, o1 = sim.state()
-        for k, v in (("forces", x), ("tvel", tv), ("rvel", rv), ("pos", p1), ("ori", o1)):
-            r = np.asarray(ref[t][{"forces": "x"}.get(k, k)]).reshape(-1)
-            e = float(np.abs(np.asarray(v).reshape(-1) - r).max() / np.abs(r).max())
-            err[k] = max(err.get(k, 0.0), e)
+    p = O.Params()
+    f64 = np.float64
+    A, b = O.assemble(pos, ori, p, analytical, f64)
+    Ad = torch.from_numpy(A).to("cuda")          # column-major host array -> a transposed-stride tensor
+    del A
+    x = torch.linalg.solve(Ad, torch.from_numpy(b).to("cuda")).cpu().numpy()
+    del Ad
+    torch.cuda.empty_cache()
+    tv, rv = O.update_velocities(pos, ori, x, p, dtype=f64, analytical=analytical)
+    z = np.zeros_like(np.asarray(pos, f64))
+    npos, nori = O.update_fibers(True, p.dt, pos, pos, ori, ori, z, tv, z, rv)
+    return {"b": b, "x": x, "tvel": tv, "rvel": rv, "pos": npos, "ori": nori}
+
+
+def _gpu_step0(cfg, pos, ori):
+    from rigidfibers_b200 import Simulation
+    sim = Simulation(cfg, pos, ori)
+    sim.assembleSystem()
+    sim.solveSystem()
+    x = sim.solution()
+    sim.updateVelocities()
+    tv, rv = sim.velocities()
+    sim.updateFibers(True)
+    p1, o1 = sim.state()
+    st = sim.stats()
     sim.close()
-    return err
+    return {"x": x, "tvel": tv, "rvel": rv, "pos": p1, "ori": o1, "iterations": st["iterations"],
+            "relres": st["relative_residual"]}
+
+
+def _rel_errors(got, ref):
+    out = {}
+    for k, name in (("x", "forces"), ("tvel", "tvel"), ("rvel", "rvel"), ("pos", "pos"), ("ori", "ori")):
+        a = np.asarray(got[k], np.float64).reshape(-1)
+        r = np.asarray(ref[k], np.float64).reshape(-1)
+        out[name] = float(np.abs(a - r).max() / max(np.abs(r).max(), 1e-30))
+    out["max"] = max(out.values())
+    return out
+
+
+def _mem_available_gb():
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def error_vs_fp64(args, precision):
+    """Errors of whole time steps against the FP64 reference at the benchmark
+    configurations (max |ours - FP64| / max |FP64| per field, step 0 from the
+    seeded layout): N fibers of the headline workload for the mixed and the
+    plain FP32 path, and N=direct_fibers analytical fibers for GMRES and the
+    direct solver."""
+    from rigidfibers_b200 import Config
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    out = {"method": "step 0 from the seeded layout; FP64 reference = the oracle's FP64 assembly and velocities on "
+                     "the host cores, FP64 LU solve on the GPU (torch.linalg.solve) as the checker; "
+                     "max |ours - FP64| / max |FP64| per field"}
+    N = args.fibers
+    need = 2.2 * (15 * N) ** 2 * 8 / 1e9
+    if _mem_available_gb() < need:
+        out["headline"] = {"unavailable": "host memory: %.0f GB available, %.0f GB needed" %
+                                          (_mem_available_gb(), need)}
+    else:
+        pos, ori = workload(args)
+        ours = {precision: _gpu_step0(Config(precision=precision, refinement_restart=args.mixed_restart), pos, ori),
+                "fp32": _gpu_step0(Config(precision="fp32"), pos, ori)}
+        ref = fp64_reference_step(pos, ori)
+        out["headline"] = {"fibers": N, "integration": "numerical"}
+        for k, g in ours.items():
+            out["headline"][k] = _rel_errors(g, ref)
+            out["headline"][k]["gmres_iterations"] = g["iterations"]
+    if args.direct_fibers > 0:
+        n = args.direct_fibers
+        radius = 14.0 * (n / 2000.0) ** (1.0 / 3.0)
+        pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(2, n))
+        ours = {s: _gpu_step0(Config(solver=s, integration="analytical"), pos, ori) for s in ("gmres", "direct")}
+        ref = fp64_reference_step(pos, ori, analytical=True)
+        out["thesis_scale"] = {"fibers": n, "integration": "analytical"}
+        for k, g in ours.items():
+            out["thesis_scale"][k] = _rel_errors(g, ref)
+    return out
 
 
 def serve_ensemble(args, dist, pack_fibers=None):
@@ -496,16 +642,15 @@ def serve_ensemble(args, dist, pack_fibers=None):
     dist.barrier()
     wall_max = dist.max(wall)
     fiber_steps = dist.sum(st["fiber_steps"])
-    return {"requests": len(reqs) * dist.world, "completed": int(dist.sum(st["completed"])),
-            "failed": int(dist.sum(st["failed"])), "steps": int(dist.sum(st["steps"])),
-            "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"],
-            "fiber_steps_per_s": fiber_steps / wall_max, "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
+    return {"p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"],
+            "fiber_steps_per_s": fiber_steps / wall_max, "requests": len(reqs) * dist.world,
+            "completed": int(dist.sum(st["completed"])), "failed": int(dist.sum(st["failed"])),
+            "steps": int(dist.sum(st["steps"])), "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
             "max_active": args.serve_max_active, "peak_active": st["peak_active"],
             "cuda_graphs": bool(args.serve_graphs), "pack_max_fibers": pack,
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
-            "workload": "N log-uniform in [16, 1000], eps in {0.01, 0.005}, 5-50 steps, volume fraction 1%, "
-                        "M=5, 8x3 quadrature, Poisson arrivals; latency = host wall time of one rf_step "
-                        "while the others run (rank 0's percentiles)"}
+            "workload": "N log-uniform in [16, 1000], eps 0.01 or 0.005, 5-50 steps, Poisson arrivals; latency = "
+                        "host wall time of one step while others run"}
 
 
 def direct_leg(args):
@@ -530,11 +675,21 @@ def direct_leg(args):
         R = 15 * n
         leg = {"ms_solve": st["ms_solve_system"], "ms_assemble": st["ms_assemble_system"],
                "relative_residual": st["relative_residual"], "iterations": st["iterations"],
-               "refinements": st["refinement_steps"], "autotune": tuned}
+               "refinements": st["refinement_steps"]}
         if solver == "direct":
             leg["tflops"] = (2.0 / 3.0) * R ** 3 / (st["ms_solve_system"] / 1e3) / 1e12
+            leg["panel_blocks"] = tuned["panel_blocks"]
         out[solver] = leg
     return out
+
+
+def _plain(args, dist, total_fiber_steps, cfg):
+    r = time_path(args, dist, cfg, *workload(args), profile=False)
+    ms = dist.max(r["ms"])
+    return {"value": total_fiber_steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
+            "gmres_restart": cfg.gmres_restart,
+            "stage_ms_per_step": {k: v / args.steps for k, v in r["stage"].items()},
+            "gmres_iterations_per_step": r["iters"] / args.steps}, r
 
 
 def run_ours(args, dist):
@@ -550,23 +705,16 @@ def run_ours(args, dist):
     cfg = Config(precision=precision, refinement_restart=args.mixed_restart)
     head = time_path(args, dist, cfg, pos, ori, clocks=Clocks(dist.local))
     ms_max, total_fiber_steps, value = whole_job_rate(dist, head["ms"], N * args.steps)
-    e2e_s, e2e_iters = e2e_path(args, dist, cfg, pos, ori)
+    e2e_s, e2e_iters, ck_bytes = e2e_path(args, dist, cfg, pos, ori)
     e2e_value = total_fiber_steps / e2e_s
-    # bytes the C ABI moves per step: rf_set_state uploads double4 prev+cur
-    # position/orientation and their float4 copies; rf_get_state reads double4 pos/ori
-    h2d = N * (2 * 2 * 32 + 2 * 16)
-    d2h = N * 2 * 32
 
-    comparison = None
+    comparison = matched = None
     if precision != "fp32":
-        plain = time_path(args, dist, Config(precision="fp32"), pos, ori)
-        plain_ms = dist.max(plain["ms"])
-        comparison = {"precision": "fp32", "value": total_fiber_steps / (plain_ms / 1000.0),
-                      "ms_per_step": plain_ms / args.steps,
-                      "stage_ms_per_step": {k: v / args.steps for k, v in plain["stage"].items()},
-                      "gmres_iterations_per_step": plain["iters"] / args.steps,
-                      "matvec_ms": plain["mv_ms"] / max(plain["mv_launches"], 1),
-                      "autotune": plain["autotune"]}
+        comparison, plain = _plain(args, dist, total_fiber_steps, Config(precision="fp32"))
+        # the mixed path runs mixed_restart Arnoldi steps between corrections;
+        # FP32 GMRES with the same restart length separates precision from restart
+        matched, _ = _plain(args, dist, total_fiber_steps,
+                            Config(precision="fp32", gmres_restart=args.mixed_restart or 10))
 
     hbm, peak_kind = peaks()
     mvn = max(head["mv_launches"], 1)
@@ -582,16 +730,16 @@ def run_ours(args, dist):
     # DRAM traffic per launch from one ncu capture of the same kernel at N=1500
     # (dram__bytes_read.sum 347.6 MB + dram__bytes_write.sum 9.8 MB for 1124250
     # unordered pairs: 304-byte records for 300 algorithmic bytes, x, partial
-    # rows; profiles/struct_z16_bulk_N1500.md), scaled by the pairs one launch
-    # processes; not captured for the dense FP32 kernel
+    # rows), scaled by the pairs one launch processes; not captured for the
+    # dense FP32 kernel
     traffic = 357.4e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision != "fp32" else None
-    roof = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-            "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
+            "kernel": kernel, "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
             "algorithmic_bytes_per_launch": bytes_per_matvec, "avg_launch_ms": mv_avg_ms,
             "launches": head["mv_launches"], "share_of_step_time": head["mv_ms"] / head["ms"] if head["ms"] else None,
-            "measured_in": "a profiled pass of the same K steps just before the timed ones (CUDA events around "
-                           "each matvec launch on the handle's stream; per-launch events rule out graph replay)"}
+            "measured_in": "a profiled pass of the same K steps after the timed ones (CUDA events around each matvec "
+                           "launch on the handle's stream; per-launch events rule out graph replay)"}
     out = {
         "metric": METRIC, "value": value, "unit": "fiber-steps/s", "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -602,37 +750,54 @@ def run_ours(args, dist):
                    "parallelism": "replicas x%d" % dist.world,
                    "l2": "inputs larger than L2: the operator (%.1f GB) is re-assembled and re-read every step"
                          % (head["device_bytes"] / 1e9)},
+        "roofline": roof, "clocks": head["clocks"],
+        "e2e": {"value": e2e_value, "unit": "fiber-steps/s", "h2d_bytes_per_step": ck_bytes,
+                "d2h_bytes_per_step": ck_bytes, "gmres_iterations_per_step": e2e_iters,
+                "timing": "host wall clock, max over ranks; the same K steps as the device-timed pass, with the "
+                          "state in pinned host memory between steps (rf_checkpoint_load, rf_step, "
+                          "rf_checkpoint_save)"},
+        "gpu_launches": head["launches"],
         "stage_ms_per_step": {k: v / args.steps for k, v in head["stage"].items()},
         "gmres_iterations_per_step": head["iters"] / args.steps,
-        "gmres_restarts_per_step": head["restarts"] / args.steps,
         "refinements_per_step": head["refinements"] / args.steps,
         "graph_replays_per_step": head["graph_replays"] / args.steps,
         "max_relative_residual": head["relres"],
-        "roofline": roof, "clocks": head["clocks"],
-        "e2e": {"value": e2e_value, "unit": "fiber-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "gmres_iterations_per_step": e2e_iters,
-                "timing": "host wall clock, max over ranks; every step uploads the initial layout from pinned host "
-                          "memory (rf_set_state) and reads the new state back (rf_get_state)"},
-        "gpu_launches": head["launches"],
-        "autotune": head["autotune"],
+        "matvec_variant": head["autotune"]["matvec_variant"],
     }
-    if args.serve_requests > 0:
-        out["serving"] = serve_ensemble(args, dist)
-        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
-            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
     if args.direct_fibers > 0 and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
-    if comparison:
-        out["fp32_path"] = comparison
-        out["speedup_vs_fp32"] = value / comparison["value"]
     head["steps"] = args.steps
     out["kernels"] = kernel_rooflines(N, head, hbm, precision != "fp32", out.get("direct_solver"))
     if dist.rank == 0 and not args.no_cpu_baseline:
-        out["error_vs_fp64"] = error_vs_fp64(precision)
-        # the CPU port runs the reference's FP32 GMRES: its matvec count is the FP32 path's
-        src = plain if comparison else head
-        out["cpu_baseline"] = cpu_sample(pos, ori, max(1, src["iters"] // args.steps),
-                                         max(1, src["restarts"] // args.steps), args.cpu_seconds)
+        res = cpu_steps(pos, ori, 1, untimed=0)
+        out["cpu_baseline"] = {"value": res["value"], "unit": "fiber-steps/s", "cores": res["cores"],
+                               "kind": CPU_KIND, "seconds_per_step": res["seconds_per_step"],
+                               "gmres_iterations": res["gmres_iterations_per_step"],
+                               "sample": "%s; one full time step (step 0) of the N=%d workload" % (CPU_WHAT, N)}
+    if dist.rank == 0 and not args.no_error_leg:
+        out["error_vs_fp64"] = error_vs_fp64(args, precision)
+    if comparison:
+        out["fp32_path"] = comparison
+        out["fp32_restart_matched"] = matched
+    if args.serve_requests > 0:
+        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
+            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
+        out["serving"] = serve_ensemble(args, dist)
+    # the headline figures once more, compact, at the end of the line
+    summ = {"value": value, "e2e": e2e_value}
+    if comparison:
+        summ["speedup_vs_fp32_gmres10"] = value / comparison["value"]
+        summ["speedup_vs_fp32_restart_matched"] = value / matched["value"]
+    err = (out.get("error_vs_fp64") or {}).get("headline") or {}
+    for k in (precision, "fp32"):
+        if k in err:
+            summ["error_vs_fp64_%s_N%d" % (k, N)] = err[k]["max"]
+    if "serving" in out:
+        summ.update(serving_p50_ms=out["serving"]["p50_step_ms"], serving_p99_ms=out["serving"]["p99_step_ms"],
+                    serving_fiber_steps_per_s=out["serving"]["fiber_steps_per_s"])
+    if "cpu_baseline" in out:
+        summ["cpu_baseline"] = out["cpu_baseline"]["value"]
+    out["summary"] = summ
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -649,6 +814,11 @@ def run_legs(args, dist):
             out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
     if "direct" in legs and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
+    if "error" in legs and dist.rank == 0:
+        out["error_vs_fp64"] = error_vs_fp64(args, "mixed_fp16" if args.precision == "auto" else args.precision)
+    if "cpu" in legs and dist.rank == 0:
+        pos, ori = workload(args)
+        out["cpu"] = cpu_steps(pos, ori, args.steps, untimed=1, cap_s=args.reference_cap_s)
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
 

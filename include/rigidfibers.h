@@ -5,7 +5,7 @@
  * `Simulation` of ericwolter/rigidfibers (src/simulation.h:38-97), whose
  * step() (src/simulation.cu:286-329) calls assembleSystem / solveSystem /
  * updateVelocities / updateFibers.  The reference has no FFI; this header is
- * what such an FFI binds (ctypes / cgo / JNI / N-API stubs in INTEGRATION.md).
+ * what such an FFI binds (a C or C++ program, ctypes, cgo, JNI or N-API).
  *
  * Conventions
  *  - Every function returns an int status (RF_OK == 0).  rf_last_error()
@@ -237,10 +237,13 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
  * counterpart in the reference.  Its scratch is a fixed 8 MiB array in the
  * library's device image (held on every GPU that loads the library until the
  * process exits), so R must not exceed 131072 (RF_E_INPUT otherwise).  The
- * first call on a device looks up that array's device address; make that
- * first call before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU (different streams, or different host
- * threads on the same device) race and must be serialised by the caller. */
+ * first call in a CUDA context (for the primary context: the first call on
+ * that device) looks up that array's device address; make that first call
+ * before any stream capture.  The address is cached per context, so after
+ * cudaDeviceReset the next call looks it up again in the new context.  All
+ * calls share the one array: calls that overlap on the GPU (different
+ * streams, or different host threads on the same device) race and must be
+ * serialised by the caller. */
 int rf_dense_matvec_noalloc(const float* A, const float* x, float* y, int64_t R, void* stream);
 
 /* ---- Serving: an ensemble of independent suspensions ------------------------
@@ -311,6 +314,11 @@ int rf_server_destroy(rf_server* s);
  * from now on fails (RF_E_OOM); -1 disables. */
 int rf_debug_set_device_wait_limit(int64_t limit);
 int rf_debug_fail_allocation_after(int n);
+/* The column-split plan rf_dense_matvec_noalloc uses for R rows on a GPU with
+ * `sms` multiprocessors (no device needed): the number of splits and the
+ * columns per split, capped so that splits x R partial rows fit its fixed
+ * scratch array.  RF_E_INPUT when R is outside [1, 131072] or sms < 1. */
+int rf_debug_noalloc_plan(int64_t R, int sms, int* splits, int64_t* cols_per_split);
 
 const char* rf_status_string(int status);
 const char* rf_last_error(void);

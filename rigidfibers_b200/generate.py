@@ -16,6 +16,10 @@ orientations uniform on the unit sphere (normalised standard normal).  This
 stands in for the thesis' concentration-controlled scenes; the reference's
 own generator (tools/gen2.f95) enforces a segment-segment distance instead.
 
+`box_layout`: the same centre-distance rule with centres uniform in a cube,
+the kind of layout of the reference's 2000-fiber benchmark file
+tests/XcT_ref2000.in.
+
 `serving_radius`: sphere radius for a circumscribed-sphere volume fraction
 phi = N (L/2)^3 / R^3 (L = 2), i.e. R = (N / phi)^(1/3).
 """
@@ -26,16 +30,19 @@ def layout_seed(config_id, n):
     return 1000003 * config_id + n
 
 
-def sphere_layout(n, radius, min_distance=0.2, seed=0, max_tries=200):
-    rng = np.random.Generator(np.random.PCG64(seed))
+def _centre_rejection(rng, n, half, min_distance, in_ball, max_tries):
+    """Centres drawn uniformly from the cube [-half, half]^3 (kept only inside
+    the ball of radius `half` when in_ball), each rejected when it lies closer
+    than min_distance to an accepted one (grid-bucketed neighbour search)."""
     pts = np.empty((n, 3))
     count = 0
     cell = max(min_distance, 1e-9)
     grid = {}
     tries = 0
     while count < n:
-        cand = rng.uniform(-radius, radius, size=(4 * (n - count) + 16, 3))
-        cand = cand[np.einsum("ij,ij->i", cand, cand) <= radius * radius]
+        cand = rng.uniform(-half, half, size=(4 * (n - count) + 16, 3))
+        if in_ball:
+            cand = cand[np.einsum("ij,ij->i", cand, cand) <= half * half]
         for c in cand:
             key = tuple(np.floor(c / cell).astype(int))
             ok = True
@@ -61,7 +68,27 @@ def sphere_layout(n, radius, min_distance=0.2, seed=0, max_tries=200):
                     break
         tries += 1
         if tries > max_tries:
-            raise RuntimeError("could not place %d fibers in radius %g" % (n, radius))
+            raise RuntimeError("could not place %d fibers in a domain of half-size %g" % (n, half))
+    return pts
+
+
+def sphere_layout(n, radius, min_distance=0.2, seed=0, max_tries=200):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = _centre_rejection(rng, n, radius, min_distance, True, max_tries)
+    ori = rng.standard_normal((n, 3))
+    ori /= np.linalg.norm(ori, axis=1, keepdims=True)
+    return pts, ori
+
+
+def box_layout(n, half_side, min_distance=0.2, seed=0, max_tries=200):
+    """Centres uniform in the cube [-half_side, half_side]^3 with the same
+    centre-distance rejection as sphere_layout; orientations uniform on the
+    unit sphere.  This is the kind of layout of the reference's 2000-fiber
+    benchmark file tests/XcT_ref2000.in: its centres fill a cube of half side
+    4.28 with minimum centre distance 0.2 (its segments come as close as
+    1.6e-4, so it was not made by the segment-distance generator)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pts = _centre_rejection(rng, n, half_side, min_distance, False, max_tries)
     ori = rng.standard_normal((n, 3))
     ori /= np.linalg.norm(ori, axis=1, keepdims=True)
     return pts, ori
@@ -191,6 +218,32 @@ def grown_sphere_layout(n, min_distance=0.2, seed=0, max_retries=1000, batch=64)
                 break
             radius += min_distance
     return pos, ori
+
+
+def layout_statistics(pos, ori, chunk=256):
+    """Packing statistics of a layout (fibers are segments centre +- orientation):
+    fiber count, radius of the smallest origin-centred sphere holding every
+    centre, minimum and mean nearest-neighbour centre distance, and minimum
+    and mean nearest-neighbour segment-segment distance.  All pairs are
+    compared, in row chunks (O(N^2) work, meant for N up to a few thousand)."""
+    pos = np.asarray(pos, np.float64)
+    ori = np.asarray(ori, np.float64)
+    n = len(pos)
+    nn_c = np.full(n, np.inf)
+    nn_s = np.full(n, np.inf)
+    for i0 in range(0, n, chunk):
+        i1 = min(n, i0 + chunk)
+        dc = pos[i0:i1, None, :] - pos[None, :, :]
+        d2 = np.einsum("bkj,bkj->bk", dc, dc)
+        s2 = segment_distances2(pos[i0:i1], ori[i0:i1], pos, ori)
+        rows = np.arange(i1 - i0)
+        d2[rows, rows + i0] = np.inf
+        s2[rows, rows + i0] = np.inf
+        nn_c[i0:i1] = np.sqrt(d2.min(axis=1))
+        nn_s[i0:i1] = np.sqrt(np.maximum(s2.min(axis=1), 0.0))
+    return {"fibers": int(n), "centre_radius": float(np.sqrt((pos * pos).sum(1)).max()),
+            "min_centre_distance": float(nn_c.min()), "mean_nn_centre_distance": float(nn_c.mean()),
+            "min_segment_distance": float(nn_s.min()), "mean_nn_segment_distance": float(nn_s.mean())}
 
 
 def serving_requests(count=512, seed=0, n_min=16, n_max=1000, steps_min=5, steps_max=50,

@@ -22,8 +22,13 @@ def test_kernel_rooflines_of_a_mixed_step():
             "iters": 217, "refinements": 20, "ms": 245.0, "steps": 10}
     k = bench.kernel_rooflines(N, head, hbm, True, {"fibers": 2000, "direct": {"tflops": 28.0}})
     pairs = N * (N - 1) / 2
-    flops = 67923 * N * (N - 1)
-    assert abs(k["assembly"]["achieved_tflops_equivalent"] - flops / 11.2e-3 / 1e12) < 1e-6
+    # executed flops per unordered pair from the kernel's instruction mix
+    per_pair = (295e6 * 2 + 77e6 + 68e6) * 32 / 499500
+    assert abs(bench.ASM_EXEC_FLOPS_PER_PAIR - per_pair) < 1e-9
+    flops = per_pair * pairs
+    assert abs(k["assembly"]["achieved_tflops"] - flops / 11.2e-3 / 1e12) < 1e-6
+    assert abs(k["assembly"]["frac"] - flops / 11.2e-3 / 1e12 / bench.NOMINAL_FP32_TFLOPS) < 1e-9
+    assert k["assembly"]["frac"] < 1.0
     assert abs(k["assembly"]["store_gbs"] - pairs * 1168 / 11.2e-3 / 1e9) < 1e-6
     assert abs(k["velocities"]["achieved_gbs"] - pairs * 480 / 0.77e-3 / 1e9) < 1e-6
     bound = 1e3 * (flops / (bench.NOMINAL_FP32_TFLOPS * 1e12) + (21.7 * pairs * 300 + 2 * pairs * 600) / (hbm * 1e9)

@@ -68,3 +68,36 @@ def test_null_handle_is_an_input_error():
     lib = C.load()
     assert lib.rf_assemble(None) == C.RF_E_INPUT
     assert lib.rf_destroy(None) == C.RF_E_INPUT
+
+
+@pytest.mark.parametrize("sms", [148, 1000, 4096])
+@pytest.mark.parametrize("R", [1, 64, 1500, 4099, 30000, 60000, 131072])
+def test_noalloc_plan_fits_its_scratch_and_covers_every_column(R, sms):
+    """The allocation-free matvec caps its column splits so that splits x R
+    partial rows fit the fixed 8 MiB (2^21 float) scratch array; on a GPU with
+    many more SMs than a B200 the uncapped plan would overflow it.  The capped
+    plan must still cover every column exactly once."""
+    lib = C.load()
+    splits, cps = ctypes.c_int(), ctypes.c_int64()
+    assert lib.rf_debug_noalloc_plan(R, sms, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_OK
+    s, c = splits.value, cps.value
+    assert s >= 1 and c >= 1
+    assert s * R <= 2 * 1024 * 1024
+    # split k covers [k*c, min(R, (k+1)*c)): all R columns, none empty
+    assert (s - 1) * c < R <= s * c
+
+
+def test_noalloc_plan_caps_splits_on_large_gpus():
+    lib = C.load()
+    splits, cps = ctypes.c_int(), ctypes.c_int64()
+    lib.rf_debug_noalloc_plan(60000, 148, ctypes.byref(splits), ctypes.byref(cps))
+    b200 = splits.value
+    lib.rf_debug_noalloc_plan(60000, 4096, ctypes.byref(splits), ctypes.byref(cps))
+    assert splits.value * 60000 <= 2 * 1024 * 1024 and splits.value >= b200
+
+
+def test_noalloc_plan_rejects_sizes_beyond_its_scratch():
+    lib = C.load()
+    splits, cps = ctypes.c_int(), ctypes.c_int64()
+    assert lib.rf_debug_noalloc_plan(131073, 148, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_E_INPUT
+    assert lib.rf_debug_noalloc_plan(0, 148, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_E_INPUT
