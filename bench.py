@@ -58,6 +58,8 @@ def parse():
                          "reported as serving_packed (0: skip)")
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
+    ap.add_argument("--direct-large-fibers", type=int, default=4000,
+                    help="fibers of the direct solve at the precision configuration (numerical; 0: skip it)")
     ap.add_argument("--legs", default="headline,serving,direct",
                     help="comma-separated subset of headline,serving,direct,error,cpu; without headline only the "
                          "requested legs are run and printed (for profiling one part)")
@@ -592,7 +594,8 @@ def error_vs_fp64(args, precision):
     else:
         pos, ori = workload(args)
         ours = {precision: _gpu_step0(Config(precision=precision, refinement_restart=args.mixed_restart), pos, ori),
-                "fp32": _gpu_step0(Config(precision="fp32"), pos, ori)}
+                "fp32": _gpu_step0(Config(precision="fp32"), pos, ori),
+                "direct": _gpu_step0(Config(solver="direct"), pos, ori)}
         ref = fp64_reference_step(pos, ori)
         out["headline"] = {"fibers": N, "integration": "numerical"}
         for k, g in ours.items():
@@ -653,19 +656,25 @@ def serve_ensemble(args, dist, pack_fibers=None):
                         "host wall time of one step while others run"}
 
 
-def direct_leg(args):
-    """The thesis-scale configuration: N fibers (radius 14 sphere at N=2000),
-    analytical integration, one step solved by the blocked LU (in place of
-    MAGMA's sgesv) and by GMRES on the same system.  LU rate = 2/3 R^3 flops over
-    the solve time (factorisation, triangular solves and FP64 refinement)."""
+def direct_leg(args, n=None, integration="analytical", solvers=("direct", "gmres")):
+    """A direct-solver configuration: by default the thesis scale (N=2000
+    fibers in a radius-14 sphere, analytical integration), one step solved by
+    the blocked LU (in place of MAGMA's sgesv) and by GMRES on the same system;
+    with n and integration given, that layout (the precision configuration:
+    N=4000, radius 18, numerical).  LU rate = 2/3 R^3 flops over the solve time
+    (factorisation, triangular solves and FP64 refinement)."""
     from rigidfibers_b200 import Config, Simulation
     from rigidfibers_b200.generate import layout_seed, sphere_layout
-    n = args.direct_fibers
-    radius = 14.0 * (n / 2000.0) ** (1.0 / 3.0)
-    pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(2, n))
-    out = {"fibers": n, "radius": radius, "integration": "analytical"}
-    for solver in ("direct", "gmres"):
-        sim = Simulation(Config(solver=solver, integration="analytical"), pos, ori)
+    if n is None:
+        n = args.direct_fibers
+        radius = 14.0 * (n / 2000.0) ** (1.0 / 3.0)
+        pos, ori = sphere_layout(n, radius, 0.2, seed=layout_seed(2, n))
+    else:
+        radius = 18.0 * (n / 4000.0) ** (1.0 / 3.0)
+        pos, ori = workload_layout(n, radius)
+    out = {"fibers": n, "radius": radius, "integration": integration}
+    for solver in solvers:
+        sim = Simulation(Config(solver=solver, integration=integration), pos, ori)
         sim.step(0)                      # warm-up (first-touch of the kernels)
         tuned = sim.autotune()
         sim.assembleSystem()
@@ -766,6 +775,8 @@ def run_ours(args, dist):
     }
     if args.direct_fibers > 0 and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
+        if args.direct_large_fibers > 0:
+            out["direct_solver_precision_config"] = direct_leg(args, args.direct_large_fibers, "numerical", ("direct",))
     head["steps"] = args.steps
     out["kernels"] = kernel_rooflines(N, head, hbm, precision != "fp32", out.get("direct_solver"))
     if dist.rank == 0 and not args.no_cpu_baseline:

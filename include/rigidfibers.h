@@ -55,7 +55,8 @@ enum rf_integration { RF_NUMERICAL = 0, RF_ANALYTICAL = 1 };
  *  RF_PREC_MIXED_FP16 / _BF16: structured operator A = I + C T, T stored once
  *      per unordered fiber pair in FP32 and in 16 bits; the Krylov matvec runs
  *      on the 16-bit copy with FP32 accumulation inside FP64-residual
- *      iterative refinement (numerical integration only). */
+ *      iterative refinement, with GMRES or BiCGSTAB (not the direct solver;
+ *      numerical integration only). */
 enum rf_precision { RF_PREC_FP32 = 0, RF_PREC_MIXED_FP16 = 1, RF_PREC_MIXED_BF16 = 2 };
 
 /* Mirrors the reference's .ini keys (tests/config.ini:18-37, read by

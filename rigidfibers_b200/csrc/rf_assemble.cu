@@ -100,8 +100,9 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   constexpr int FF = K1 * 3;   // force-term floats per fiber
   static_assert(Q % 2 == 0, "mirror folding needs an even number of quadrature points");
 
-  __shared__ float4 sPj[TI][Q];          // x_j + s_q t_j for the J tile
+  __shared__ float4 sPj[TI][Q];          // s_q t_j for the J tile (numerical: offsets from the centre)
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
+  __shared__ float sD[TI][TI][3];        // x_i - x_j, formed in FP64 and rounded once (numerical)
   extern __shared__ __align__(16) float smem_dyn[];
   float (*sG)[S::GS] = reinterpret_cast<float (*)[S::GS]>(smem_dyn);                          // [NC][GS]
   float* const sTbase = smem_dyn + S::GOFF;                                                  // 2 x [TI][TP]
@@ -131,12 +132,24 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
     sTi[tid] = ori[i];
     sTj[tid] = ori[j];
   }
+  if (SYM && tid < TI * TI) {
+    const int a = tid / TI, c = tid % TI;
+    const double4 xi = out.pos64[min(i0 + a, N - 1)], xj = out.pos64[min(j0 + c, N - 1)];
+    sD[a][c][0] = (float)(xi.x - xj.x);
+    sD[a][c][1] = (float)(xi.y - xj.y);
+    sD[a][c][2] = (float)(xi.z - xj.z);
+  }
   if (tid < S::U) {
     const int jl = tid / Q, q = tid % Q;
     const int j = min(j0 + jl, N - 1);
-    const float4 x = pos[j], t = ori[j];
+    const float4 t = ori[j];
     const float s = tab.pts[q];
-    sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
+    if (SYM) {
+      sPj[jl][q] = make_float4(s * t.x, s * t.y, s * t.z, 0.f);
+    } else {
+      const float4 x = pos[j];
+      sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
+    }
   }
   for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
   if constexpr (MODE != kAsmDense) {
@@ -159,12 +172,12 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   const int il = tid / Q, qi = tid % Q;
   const int i = i0 + il;
   const bool unit_ok = (tid < S::U) && (i < N);
-  float pix = 0.f, piy = 0.f, piz = 0.f;
-  if (unit_ok) {
-    const float4 x = pos[i], t = ori[i];
-    const float s = tab.pts[qi];
-    pix = fmaf(s, t.x, x.x); piy = fmaf(s, t.y, x.y); piz = fmaf(s, t.z, x.z);
-  }
+  // numerical: the separation of quadrature points is formed as
+  // (x_i - x_j) + s_qi t_i - s_qj t_j with the centre difference taken in
+  // FP64 and rounded once, so its error scales with the fibers' distance
+  // rather than with their distance from the origin (FP32 points x + s t far
+  // from the origin lose ~1e-6 absolutely, which for nearly touching fibers
+  // is ~1e-4 of the kernel)
   const float e2 = tab.e2;
   const float e2x3 = -3.f * e2;
   const float fz = tab.fz_half;
@@ -200,6 +213,10 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
       analytic_G<M>(R0, tj, 2.0 * (double)tab.eps * (double)tab.eps, g);
     }
     if (SYM && pair_ok) {
+      const float4 ti = sTi[il];
+      const float pix = fmaf(tab.pts[qi], ti.x, sD[il][jl][0]);
+      const float piy = fmaf(tab.pts[qi], ti.y, sD[il][jl][1]);
+      const float piz = fmaf(tab.pts[qi], ti.z, sD[il][jl][2]);
 #pragma unroll
       for (int q = 0; q < H; ++q) {
         float Kp[6], Km[6];
@@ -491,9 +508,10 @@ static int dispatch_assemble(const Tables& tab, int N, const float4* pos, const 
   return RF_E_UNSUPPORTED;
 }
 
-int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                              int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
+int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
   AsmOut out{};
+  out.pos64 = pos64;
   out.A = A;
   out.lda = lda;
   out.ffpart = ffpart;
@@ -512,9 +530,11 @@ int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, cons
   return dispatch_assemble<kAsmDense, kAnalytical>(tab, N, pos, ori, out, F, b, st);
 }
 
-int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
-                               uint32_t* S16, bool bf16, float* ffpart, float* F, float* b, cudaStream_t st) {
+int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                               float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,
+                               cudaStream_t st) {
   AsmOut out{};
+  out.pos64 = pos64;
   out.S32 = S32;
   out.S16 = S16;
   out.ffpart = ffpart;

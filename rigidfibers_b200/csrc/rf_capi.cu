@@ -164,6 +164,8 @@ struct rf_handle {
   float* bicg_work = nullptr;     // BiCGSTAB vectors r, r0, p, v, s, t
   BicgCtl* bctl = nullptr;
   BicgCtl* host_bctl = nullptr;
+  double* ir_norm = nullptr;      // BiCGSTAB refinement (mixed): ||r||^2 on the device
+  double* host_ir_norm = nullptr; //   and its pinned host copy
   DenseGemvPlan gemv_plan;
   int coop_blocks = 1;
   // velocity scratch
@@ -225,6 +227,7 @@ struct rf_handle {
     if (st) cudaStreamSynchronize(st);
     if (host_ctl) cudaFreeHost(host_ctl);
     if (host_bctl) cudaFreeHost(host_bctl);
+    if (host_ir_norm) cudaFreeHost(host_ir_norm);
     if (lu.host_ipiv) cudaFreeHost(lu.host_ipiv);
     if (lu.host_perm) cudaFreeHost(lu.host_perm);
     for (auto& e : ev)
@@ -264,8 +267,8 @@ static int validate_config(const rf_config* c, int N) {
     set_last_error_str("mixed precision is built for 8 quadrature intervals (24 points per fiber)");
     return RF_E_UNSUPPORTED;
   }
-  if (c->precision != RF_PREC_FP32 && c->solver != RF_SOLVER_GMRES) {
-    set_last_error_str("mixed precision refines inside GMRES");
+  if (c->precision != RF_PREC_FP32 && c->solver == RF_SOLVER_DIRECT) {
+    set_last_error_str("mixed precision refines inside GMRES or BiCGSTAB (the direct solver factors the dense FP32 matrix)");
     return RF_E_UNSUPPORTED;
   }
   if (c->precision != RF_PREC_FP32 && !(c->refinement_tolerance > 0.0)) {
@@ -359,6 +362,11 @@ int rf_set_state(rf_handle* h, const double* pos, const double* ori) {
 // Every device buffer of a handle.  With h->dry set nothing is allocated and
 // h->device_bytes is the exact footprint (admission control of the server).
 constexpr int kTuneMaxCtasPerSm = 16;
+// Mixed-precision BiCGSTAB: each inner solve on the 16-bit blocks stops when
+// its residual has fallen to this fraction of the correction equation's
+// right-hand side (the 16-bit operator is accurate to about 1e-4, so going
+// further buys little before the next FP64 residual)
+constexpr double kBicgInnerTolerance = 1e-3;
 
 static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   const int64_t R = h->R;
@@ -440,6 +448,10 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     if (!rc) rc = h->alloc((void**)&h->bicg_work, (size_t)6 * (size_t)ldv * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->bctl, sizeof(BicgCtl));
     if (!rc && !h->dry && cudaMallocHost((void**)&h->host_bctl, sizeof(BicgCtl)) != cudaSuccess) rc = RF_E_OOM;
+    if (h->mixed) {
+      if (!rc) rc = h->alloc((void**)&h->ir_norm, sizeof(double));
+      if (!rc && !h->dry && cudaMallocHost((void**)&h->host_ir_norm, sizeof(double)) != cudaSuccess) rc = RF_E_OOM;
+    }
   }
   // velocities
   if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
@@ -521,13 +533,14 @@ int rf_assemble(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
   if (h->mixed)
-    RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->S32, h->S16,
+    RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
                                       h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st));
   else if (h->cfg.integration == RF_ANALYTICAL)
     RF_TRY(launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
                                       h->lda, h->ffpart, h->F, h->b, h->st));
   else
-    RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->A, h->lda, h->ffpart, h->F, h->b, h->st));
+    RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->A, h->lda, h->ffpart,
+                                     h->F, h->b, h->st));
   h->launches += 2;
   RF_CUDA_TRY(cudaEventRecord(h->ev[1], h->st));
   h->assembled = true;
@@ -619,13 +632,48 @@ int rf_solve(rf_handle* h) {
     bs.host_ctl = h->host_bctl;
     bs.coop_blocks = h->coop_blocks;
     BicgResult br;
-    int brc = bicgstab_solve(bs, mv, h->b, h->x, h->st, &br);
+    int brc;
+    if (h->mixed) {
+      // BiCGSTAB on the 16-bit blocks inside FP64-residual refinement: the
+      // residual, its correction and the FP64 solution use the Krylov basis
+      // buffers (the GMRES basis is idle under this solver)
+      RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
+      ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
+        return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin),
+                                        h->zpart64, h->b, r, skip, &h->ctl->timeout, st);
+      };
+      BicgIr ir;
+      ir.x64 = h->x64;
+      ir.r = h->V;
+      ir.d = h->V + bs.ldv;
+      ir.norm_dev = h->ir_norm;
+      ir.norm_host = h->host_ir_norm;
+      ir.tol = h->cfg.refinement_tolerance;
+      ir.inner_tol = kBicgInnerTolerance;
+      ir.max_outer = h->cfg.refinement_max_iterations;
+      brc = bicgstab_ir_solve(bs, mv, resid, h->b, ir, h->st, &br);
+      int timed_out = 0;
+      RF_CUDA_TRY(cudaMemcpyAsync(&timed_out, &h->ctl->timeout, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+      RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+      if (timed_out) {
+        set_last_error_str("a bounded device-side wait timed out");
+        return RF_E_TIMEOUT;
+      }
+      if (brc == RF_OK || brc == RF_E_NOCONV) {
+        RF_TRY(launch_cast_to_float(h->x64, h->x, h->R, h->st));
+        h->launches += 1;
+      }
+      h->launches += 3 * (br.refinements + 1);   // the FP64 residual of every outer pass
+      h->refinements = br.refinements;
+    } else {
+      brc = bicgstab_solve(bs, mv, h->b, h->x, h->st, &br);
+    }
     RF_CUDA_TRY(cudaEventRecord(h->ev[3], h->st));
     h->launches += br.launches + mv_launches;
     h->matvecs_done = br.matvecs;
     h->stats.iterations = br.iterations;
     h->stats.restarts = br.restarts;
-    h->stats.refinement_steps = 0;
+    h->stats.refinement_steps = h->mixed ? br.refinements : 0;
     h->stats.relative_residual = br.relative_residual;
     if (brc != RF_OK && brc != RF_E_NOCONV) return brc;
     h->solved = true;
@@ -677,7 +725,7 @@ int rf_update_velocities(rf_handle* h) {
                                   h->rv[h->vcur], h->st));
     h->launches += 2;
   } else {
-    RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos32, h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
+    RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos64[h->icur], h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
                                      h->rv[h->vcur], h->st));
     h->launches += 3;
   }

@@ -29,16 +29,18 @@ int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cud
 int assemble_tiles(int M, int Q, int N);
 
 // Numerical assembly.  ffpart: assemble_tiles(M,Q,N) x N x 3(M+1) floats of
-// scratch; F: N x 3(M+1) force terms sum_j T^{ij}[k][P0] F/2; b: R.
-int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, float* A,
-                              int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
+// scratch; F: N x 3(M+1) force terms sum_j T^{ij}[k][P0] F/2; b: R.  pos64:
+// the FP64 centres, from which the pair separations are formed.
+int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
 // Analytical integration (closed-form inner integral in FP64), dense A.
 int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
                                const double4* pos64, const double4* ori64, float* A, int64_t lda, float* ffpart,
                                float* F, float* b, cudaStream_t st);
 // Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
-int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, float* S32,
-                               uint32_t* S16, bool bf16, float* ffpart, float* F, float* b, cudaStream_t st);
+int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                               float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,
+                               cudaStream_t st);
 int64_t struct_store_tiles(int N);
 int64_t struct_floats32(int M, int N);
 int64_t struct_words16(int M, int N);
@@ -90,7 +92,8 @@ namespace rf {
 int velocity_chunks(int N);
 // fw: N*Q float4 scratch; vpart: velocity_chunks(N) * N * 6 floats scratch.
 int launch_check_finite(const float4* a, const float4* b, int N, int* flag, cudaStream_t st);
-int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
+// pos64: the FP64 centres, from which the pair separations are formed
+int launch_velocity_numerical(const Tables& tab, int N, const double4* pos64, const float4* ori, const float* x,
                               float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 // analytical inner integrals (FP64 moments); vpart as for the numerical kernel
 int launch_velocity_analytical(const Tables& tab, int N, const float4* ori, const double4* pos64,

@@ -16,6 +16,8 @@
 //    kernel reads first), so the host never waits per iteration.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "rf_common.cuh"
@@ -822,6 +824,81 @@ int bicgstab_solve(const BicgSetup& s, const MatvecFn& matvec, const float* b, f
   if (h.nan) return RF_E_NAN;
   if (!h.converged) return RF_E_NOCONV;
   return RF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB with iterative refinement (mixed precision): the outer loop keeps
+// x in FP64 and recomputes r = b - A x with the caller's residual (FP64
+// accumulation over the FP32 operator); the inner BiCGSTAB above solves
+// A d = r on the caller's matvec (the 16-bit operator, FP32 sums) until its
+// recursive residual falls below inner_tol relative to ||r||, and d is added
+// to x in FP64.  The correction equation has x0 = 0, as the reference's
+// solver has for the full system.
+// ---------------------------------------------------------------------------
+// ||v||^2 in FP64, one block, fixed order
+__global__ void __launch_bounds__(1024) k_norm2_f32(const float* __restrict__ v, int64_t R, double* __restrict__ out) {
+  double acc[1] = {0.0};
+  for (int64_t i = threadIdx.x; i < R; i += blockDim.x) {
+    const double t = (double)v[i];
+    acc[0] = fma(t, t, acc[0]);
+  }
+  __shared__ double tmp[1];
+  block_reduce_store<1>(acc, tmp);
+  if (threadIdx.x == 0) *out = tmp[0];
+}
+
+__global__ void k_add_correction(double* __restrict__ x, const float* __restrict__ d, int64_t R) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += (double)d[i];
+}
+
+int bicgstab_ir_solve(const BicgSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                      const BicgIr& ir, cudaStream_t st, BicgResult* res) {
+  const int64_t R = s.R;
+  const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 1024);
+  k_fill_zero<double><<<eb, 256, 0, st>>>(ir.x64, R);
+  k_norm2_f32<<<1, 1024, 0, st>>>(b, R, ir.norm_dev);
+  RF_LAUNCH_CHECK();
+  RF_CUDA_TRY(cudaMemcpyAsync(ir.norm_host, ir.norm_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+  RF_CUDA_TRY(cudaStreamSynchronize(st));
+  const double bnorm = std::sqrt(*ir.norm_host);
+  *res = BicgResult();
+  res->launches = 2;
+  double rel = 0.0;
+  int outer = 0, inner_left = s.maxit;
+  for (;;) {
+    // r = b - A x (FP64 sums); the first pass has x = 0, so r = b
+    if (int rc = residual(ir.x64, ir.r, nullptr, st)) return rc;
+    k_norm2_f32<<<1, 1024, 0, st>>>(ir.r, R, ir.norm_dev);
+    RF_LAUNCH_CHECK();
+    RF_CUDA_TRY(cudaMemcpyAsync(ir.norm_host, ir.norm_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+    RF_CUDA_TRY(cudaStreamSynchronize(st));
+    res->launches += 1;   // the norm (the residual's kernels are the caller's to count)
+    const double rnorm = std::sqrt(*ir.norm_host);
+    rel = bnorm > 0.0 ? rnorm / bnorm : 0.0;
+    if (!std::isfinite(rel)) {
+      res->relative_residual = rel;
+      return RF_E_NAN;
+    }
+    if (rel <= ir.tol || outer >= ir.max_outer || inner_left <= 0) break;
+    BicgSetup in = s;
+    in.tol = ir.inner_tol;
+    in.maxit = inner_left;
+    BicgResult br;
+    const int rc = bicgstab_solve(in, matvec, ir.r, ir.d, st, &br);
+    if (rc != RF_OK && rc != RF_E_NOCONV) return rc;
+    res->iterations += br.iterations;
+    res->restarts += br.restarts;
+    res->matvecs += br.matvecs;
+    res->launches += br.launches + 1;
+    inner_left -= std::max(1, br.iterations);
+    k_add_correction<<<eb, 256, 0, st>>>(ir.x64, ir.d, R);
+    RF_LAUNCH_CHECK();
+    ++outer;
+  }
+  res->refinements = outer;
+  res->relative_residual = rel;
+  return rel <= ir.tol ? RF_OK : RF_E_NOCONV;
 }
 
 }  // namespace rf

@@ -133,11 +133,28 @@ struct BicgResult {
   int restarts = 0;
   int matvecs = 0;
   int launches = 0;
+  int refinements = 0;    // outer corrections (bicgstab_ir_solve)
   double relative_residual = 0.0;
 };
 
 int bicgstab_solve(const BicgSetup& s, const MatvecFn& matvec, const float* b, float* x, cudaStream_t st,
                    BicgResult* res);
+
+// Buffers and targets of BiCGSTAB with FP64-residual refinement.
+struct BicgIr {
+  double* x64;         // R: the solution (FP64)
+  float* r;            // R: the residual b - A x (FP32 copy of the FP64 sums)
+  float* d;            // R: the correction
+  double* norm_dev;    // 1 (device)
+  double* norm_host;   // 1 (pinned host)
+  double tol;          // outer target on ||b - A x|| / ||b||
+  double inner_tol;    // inner BiCGSTAB target relative to ||r||
+  int max_outer;       // corrections at most
+};
+// s.maxit bounds the inner iterations in total; res->iterations counts them,
+// res->refinements the corrections.
+int bicgstab_ir_solve(const BicgSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                      const BicgIr& ir, cudaStream_t st, BicgResult* res);
 
 struct DenseGemvPlan {
   int row_blocks;

@@ -39,22 +39,30 @@ __global__ void k_source_density(const Tables tab, int N, const float* __restric
 // (fiber il, quadrature point qi) and accumulates sum_j GF_ij(qi).
 template <int Q>
 __global__ void __launch_bounds__(192, 4)
-k_velocity_numerical(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+k_velocity_numerical(const Tables tab, int N, const double4* __restrict__ pos64, const float4* __restrict__ ori,
                      const float4* __restrict__ fw, int jchunk, float* __restrict__ vpart) {
   constexpr int TI = 192 / Q;
   constexpr int U = TI * Q;
-  __shared__ float4 sP[TI][Q], sF[TI][Q];
+  // quadrature-point separations (x_i - x_j) + s_qi t_i - s_qj t_j with the
+  // centre difference in FP64, rounded once (as in the assembly): the error
+  // scales with the fibers' distance, not with their distance from the origin
+  __shared__ float4 sP[TI][Q], sF[TI][Q];    // s_q t_j, w_q f_j(s_q)
+  __shared__ double sXi[TI][3], sXj[TI][3];
   __shared__ float sGs[3][U];
   const int tid = threadIdx.x;
   const int il = tid / Q, qi = tid % Q;
   const int i0 = blockIdx.x * TI;
   const int i = i0 + il;
   const bool unit_ok = tid < U && i < N;
-  float pix = 0.f, piy = 0.f, piz = 0.f;
+  float tix = 0.f, tiy = 0.f, tiz = 0.f;
   if (unit_ok) {
-    const float4 x = pos[i], t = ori[i];
+    const float4 t = ori[i];
     const float s = tab.pts[qi];
-    pix = fmaf(s, t.x, x.x); piy = fmaf(s, t.y, x.y); piz = fmaf(s, t.z, x.z);
+    tix = s * t.x; tiy = s * t.y; tiz = s * t.z;
+  }
+  if (tid < TI) {
+    const double4 x = pos64[min(i0 + tid, N - 1)];
+    sXi[tid][0] = x.x; sXi[tid][1] = x.y; sXi[tid][2] = x.z;
   }
   const float e2 = tab.e2, e2x3 = -3.f * tab.e2;
   float g0 = 0.f, g1 = 0.f, g2 = 0.f;
@@ -64,16 +72,23 @@ k_velocity_numerical(const Tables tab, int N, const float4* __restrict__ pos, co
     if (tid < U) {
       const int jl = tid / Q, q = tid % Q;
       const int j = min(js + jl, N - 1);
-      const float4 x = pos[j], t = ori[j];
+      const float4 t = ori[j];
       const float s = tab.pts[q];
-      sP[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
+      sP[jl][q] = make_float4(s * t.x, s * t.y, s * t.z, 0.f);
       sF[jl][q] = fw[(int64_t)j * Q + q];
+      if (q == 0) {
+        const double4 x = pos64[j];
+        sXj[jl][0] = x.x; sXj[jl][1] = x.y; sXj[jl][2] = x.z;
+      }
     }
     __syncthreads();
     const int jn = min(TI, jend - js);
     if (unit_ok) {
       for (int jl = 0; jl < jn; ++jl) {
         if (js + jl == i) continue;
+        const float pix = (float)(sXi[il][0] - sXj[jl][0]) + tix;
+        const float piy = (float)(sXi[il][1] - sXj[jl][1]) + tiy;
+        const float piz = (float)(sXi[il][2] - sXj[jl][2]) + tiz;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
           const float4 pj = sP[jl][q];
@@ -240,7 +255,7 @@ int launch_check_finite(const float4* a, const float4* b, int N, int* flag, cuda
   return RF_OK;
 }
 
-int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const float* x,
+int launch_velocity_numerical(const Tables& tab, int N, const double4* pos64, const float4* ori, const float* x,
                               float4* fw, float* vpart, float4* tvel, float4* rvel, cudaStream_t st) {
   const int Q = tab.Q;
   k_source_density<<<(unsigned)std::min<int64_t>(ceil_div((int64_t)N * Q, 256), 148 * 16), 256, 0, st>>>(tab, N, x, fw);
@@ -250,9 +265,9 @@ int launch_velocity_numerical(const Tables& tab, int N, const float4* pos, const
   const int TI = 192 / Q;
   dim3 grid((unsigned)ceil_div(N, TI), (unsigned)chunks);
   switch (Q) {
-    case 12: k_velocity_numerical<12><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
-    case 24: k_velocity_numerical<24><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
-    case 48: k_velocity_numerical<48><<<grid, 192, 0, st>>>(tab, N, pos, ori, fw, jchunk, vpart); break;
+    case 12: k_velocity_numerical<12><<<grid, 192, 0, st>>>(tab, N, pos64, ori, fw, jchunk, vpart); break;
+    case 24: k_velocity_numerical<24><<<grid, 192, 0, st>>>(tab, N, pos64, ori, fw, jchunk, vpart); break;
+    case 48: k_velocity_numerical<48><<<grid, 192, 0, st>>>(tab, N, pos64, ori, fw, jchunk, vpart); break;
     default: set_last_error_str("velocity: quadrature size not instantiated"); return RF_E_UNSUPPORTED;
   }
   RF_LAUNCH_CHECK();

@@ -94,6 +94,43 @@ def test_mixed_steps_within_1e4_of_fp64(prec):
         assert st["refinement_steps"] >= 1
 
 
+@pytest.mark.parametrize("prec", ["mixed_fp16", "mixed_bf16"])
+def test_mixed_bicgstab_steps_within_1e4_of_fp64(prec):
+    """BiCGSTAB on the 16-bit pair blocks (FP32 sums) inside FP64-residual
+    refinement (the reference's BiCGSTAB call: src/simulation.cu:424-427):
+    forces, velocities and fiber state within 1e-4 of the FP64 oracle over
+    three steps, the FP64 residual at the refinement target."""
+    pos, ori = sphere_layout(200, radius=4.0, seed=7)
+    ref = O.run_steps(pos, ori, O.Params(), 3, solver="direct", dtype=np.float64)
+    res = _run(_sim(pos, ori, precision=prec, solver="bicgstab", refinement_tolerance=1e-6), 3)
+    for t in range(3):
+        for k in ("x", "tvel", "rvel", "pos", "ori"):
+            assert _rel(res[t][k], ref[t][k]) <= 1e-4, (prec, t, k, _rel(res[t][k], ref[t][k]))
+        st = res[t]["stats"]
+        assert st["relative_residual"] <= 1e-6
+        assert st["refinement_steps"] >= 1 and st["iterations"] > 0
+
+
+def test_mixed_bicgstab_matches_mixed_gmres():
+    """Both refined solves reach ||b - A x|| / ||b|| <= 1e-6 on the same FP32
+    blocks, so their forces agree far inside the 1e-4 bound."""
+    pos, ori = sphere_layout(120, radius=3.5, seed=17)
+    a = _run(_sim(pos, ori, precision="mixed_fp16", solver="bicgstab"), 2)
+    b = _run(_sim(pos, ori, precision="mixed_fp16"), 2)
+    for t in range(2):
+        for k in ("x", "tvel", "rvel", "pos"):
+            assert _rel(a[t][k], b[t][k]) <= 1e-5, (t, k, _rel(a[t][k], b[t][k]))
+
+
+def test_mixed_rejects_direct_solver():
+    from rigidfibers_b200 import RigidFibersError
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(4, radius=1.5, seed=1)
+    with pytest.raises(RigidFibersError) as e:
+        _sim(pos, ori, precision="mixed_fp16", solver="direct")
+    assert e.value.status == C.RF_E_UNSUPPORTED
+
+
 def test_mixed_golden(golden):
     """The reference's golden files (FP64 runs) through the mixed path."""
     res = _run(_sim(golden["positions"], golden["orientations"], precision="mixed_fp16"), 2)
