@@ -687,7 +687,7 @@ def direct_leg(args, n=None, integration="analytical", solvers=("direct", "gmres
                "refinements": st["refinement_steps"]}
         if solver == "direct":
             leg["tflops"] = (2.0 / 3.0) * R ** 3 / (st["ms_solve_system"] / 1e3) / 1e12
-            leg["panel_blocks"] = tuned["panel_blocks"]
+            leg["row_exchanges"] = bool(st["pivoted"])
         out[solver] = leg
     return out
 

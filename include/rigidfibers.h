@@ -108,6 +108,9 @@ typedef struct rf_stats {
                                 captured CUDA graph (0 while profiling is on) */
   int factorizations;        /* direct solver: 1 = TF32 tensor-core factors refined,
                                 2 = refactored with the 3xTF32 split update */
+  int pivoted;               /* direct solver: 1 when the factorization without row
+                                exchanges met a multiplier above 1 (or a zero pivot)
+                                and the factors were computed with row exchanges */
 } rf_stats;
 
 typedef struct rf_handle rf_handle;

@@ -57,6 +57,7 @@ class rf_stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_int),
         ("graph_replays", ctypes.c_int),
         ("factorizations", ctypes.c_int),
+        ("pivoted", ctypes.c_int),
     ]
 
 

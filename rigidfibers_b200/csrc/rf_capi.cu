@@ -440,7 +440,12 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     if (!rc) rc = h->alloc((void**)&L.d, (size_t)R * sizeof(float));
     if (!rc) rc = h->alloc((void**)&L.x64, (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&L.r64, (size_t)R * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&L.rpart, (size_t)kLuResidualSplits * R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&L.norms, 2 * sizeof(double));
+    if (!rc) rc = h->alloc((void**)&L.LT, (size_t)lu_tc_lt_floats(R) * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.inv, (size_t)lu_tc_inv_floats() * sizeof(float));
+    if (!rc) rc = h->alloc((void**)&L.flags, 2 * sizeof(int));
+    if (!rc) rc = h->alloc((void**)&L.sinv, (size_t)lu_tc_sinv_floats(R) * sizeof(float));
     if (!rc && !h->dry && cudaMallocHost((void**)&L.host_ipiv, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
     if (!rc && !h->dry && cudaMallocHost((void**)&L.host_perm, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
   }
@@ -612,6 +617,7 @@ int rf_solve(rf_handle* h) {
     h->stats.restarts = 0;
     h->stats.refinement_steps = lr.refinement_steps;
     h->stats.factorizations = lr.factorizations;
+    h->stats.pivoted = lr.pivoted ? 1 : 0;
     h->stats.relative_residual = lr.relative_residual;
     if (lrc != RF_OK && lrc != RF_E_NOCONV) return lrc;
     h->solved = true;
@@ -1370,6 +1376,8 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
   LuSetup L{};
   L.R = R;
   L.lda = R;
+  L.ldlu = ceil_div(R, 32) * 32;   // factors with 128-byte aligned columns (the tensor-core path's TMA needs
+                                   // 16-byte multiples)
   L.tol = tol;
   L.max_refine = 20;
   L.coop_blocks = std::max(krylov_coop_blocks(R, sms), coop_blocks_per_sm_capped(sms));
@@ -1388,7 +1396,11 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
     mem.push_back(*p);
     return RF_OK;
   };
-  int rc = get((void**)&L.LU, (size_t)R * R * sizeof(float));
+  int rc = get((void**)&L.LU, (size_t)L.ldlu * R * sizeof(float));
+  if (!rc) rc = get((void**)&L.LT, (size_t)lu_tc_lt_floats(R) * sizeof(float));
+  if (!rc) rc = get((void**)&L.inv, (size_t)lu_tc_inv_floats() * sizeof(float));
+  if (!rc) rc = get((void**)&L.flags, 2 * sizeof(int));
+  if (!rc) rc = get((void**)&L.sinv, (size_t)lu_tc_sinv_floats(R) * sizeof(float));
   if (!rc) rc = get((void**)&L.ipiv, R * sizeof(int));
   if (!rc) rc = get((void**)&L.perm, R * sizeof(int));
   if (!rc) rc = get((void**)&L.pmax, 2 * L.coop_blocks * sizeof(float));
@@ -1399,6 +1411,7 @@ int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, doubl
   if (!rc) rc = get((void**)&L.d, R * sizeof(float));
   if (!rc) rc = get((void**)&L.x64, R * sizeof(double));
   if (!rc) rc = get((void**)&L.r64, R * sizeof(double));
+  if (!rc) rc = get((void**)&L.rpart, (size_t)kLuResidualSplits * R * sizeof(double));
   if (!rc) rc = get((void**)&L.norms, 2 * sizeof(double));
   std::vector<int> hi(R), hp(R);
   L.host_ipiv = hi.data();

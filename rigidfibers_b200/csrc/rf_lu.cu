@@ -602,14 +602,15 @@ __global__ void k_permute(const float* __restrict__ in, const int* __restrict__ 
     out[i] = in[perm[i]];
 }
 
-constexpr int kSB = 64;   // substitution block
+constexpr int kSB = 128;   // substitution block
 
 // Diagonal block [j0, j0+n): the block in shared memory, one column of the
 // substitution per step, all threads update the entries below (or above).
 template <bool LOWER>
 __global__ void __launch_bounds__(kSB) k_trsv_diag(const float* __restrict__ A, int64_t lda, int64_t R, int64_t j0,
                                                    float* __restrict__ x) {
-  __shared__ float Ls[kSB][kSB + 1];
+  extern __shared__ float trsv_sm[];
+  float (*Ls)[kSB + 1] = reinterpret_cast<float (*)[kSB + 1]>(trsv_sm);
   __shared__ float xs[kSB];
   const int n = (int)std::min<int64_t>(kSB, R - j0);
   const int t = threadIdx.x;
@@ -649,34 +650,70 @@ __global__ void k_trsv_update(const float* __restrict__ A, int64_t lda, int64_t 
 // x = (LU)^{-1} P rhs; rhs and x distinct
 static int lu_solve(const float* LU, int64_t lda, int64_t R, const int* perm, const float* rhs, float* x,
                     cudaStream_t st) {
+  constexpr size_t kDiagSmem = sizeof(float) * kSB * (kSB + 1);
+  static const cudaError_t attr[2] = {
+      cudaFuncSetAttribute(k_trsv_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem),
+      cudaFuncSetAttribute(k_trsv_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem)};
+  RF_CUDA_TRY(attr[0]);
+  RF_CUDA_TRY(attr[1]);
   k_permute<<<(unsigned)std::min<int64_t>(ceil_div(R, 256), 4096), 256, 0, st>>>(rhs, perm, R, x);
   RF_LAUNCH_CHECK();
   for (int64_t j0 = 0; j0 < R; j0 += kSB) {
     const int nbk = (int)std::min<int64_t>(kSB, R - j0);
-    k_trsv_diag<true><<<1, kSB, 0, st>>>(LU, lda, R, j0, x);
+    k_trsv_diag<true><<<1, kSB, kDiagSmem, st>>>(LU, lda, R, j0, x);
     const int64_t r0 = j0 + nbk;
     if (r0 < R) k_trsv_update<<<(unsigned)ceil_div(R - r0, 256), 256, 0, st>>>(LU, lda, j0, nbk, r0, R, x);
   }
   const int64_t last = (R - 1) / kSB * kSB;
   for (int64_t j0 = last; j0 >= 0; j0 -= kSB) {
     const int nbk = (int)std::min<int64_t>(kSB, R - j0);
-    k_trsv_diag<false><<<1, kSB, 0, st>>>(LU, lda, R, j0, x);
+    k_trsv_diag<false><<<1, kSB, kDiagSmem, st>>>(LU, lda, R, j0, x);
     if (j0 > 0) k_trsv_update<<<(unsigned)ceil_div(j0, 256), 256, 0, st>>>(LU, lda, j0, nbk, 0, j0, x);
   }
   RF_LAUNCH_CHECK();
   return RF_OK;
 }
 
-// r = b - A x (A FP32 column-major, x FP64, accumulation FP64); ||r||^2 and
-// ||b||^2 partial sums into part[blk*2 + {0,1}].
-__global__ void __launch_bounds__(256) k_residual64(const float* __restrict__ A, int64_t lda, int64_t R,
-                                                    const double* __restrict__ x, const float* __restrict__ b,
-                                                    double* __restrict__ r) {
+// r = b - A x (A FP32 column-major, x FP64, accumulation FP64): the columns
+// are split over blockIdx.y (nsplit chunks of cps columns), each split writes
+// FP64 partial rows, and k_residual_sum adds them in fixed order.
+__global__ void __launch_bounds__(256) k_residual64_part(const float* __restrict__ A, int64_t lda, int64_t R,
+                                                         const double* __restrict__ x, int64_t cps,
+                                                         double* __restrict__ part) {
   const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (row >= R) return;
-  double s = 0.0;
-  for (int64_t c = 0; c < R; ++c) s = fma((double)A[row + c * lda], x[c], s);
-  r[row] = (double)b[row] - s;
+  const int64_t c0 = (int64_t)blockIdx.y * cps, c1 = std::min<int64_t>(R, c0 + cps);
+  double s0 = 0.0, s1 = 0.0;
+  int64_t c = c0;
+  for (; c + 1 < c1; c += 2) {
+    s0 = fma((double)__ldcs(A + row + c * lda), x[c], s0);
+    s1 = fma((double)__ldcs(A + row + (c + 1) * lda), x[c + 1], s1);
+  }
+  if (c < c1) s0 = fma((double)__ldcs(A + row + c * lda), x[c], s0);
+  part[(int64_t)blockIdx.y * R + row] = s0 + s1;
+}
+
+__global__ void k_residual_sum(const double* __restrict__ part, int nsplit, int64_t R, const float* __restrict__ b,
+                               double* __restrict__ r) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int p = 0; p < nsplit; ++p) s += part[(int64_t)p * R + i];
+    r[i] = (double)b[i] - s;
+  }
+}
+
+static int launch_residual64(const LuSetup& s, const float* A, const float* b, cudaStream_t st) {
+  const int64_t R = s.R;
+  const int row_blocks = (int)ceil_div(R, 256);
+  int nsplit = std::max(1, std::min(kLuResidualSplits, (int)ceil_div(148 * 8, row_blocks)));
+  nsplit = (int)std::min<int64_t>(nsplit, R);
+  const int64_t cps = ceil_div(R, nsplit);
+  nsplit = (int)ceil_div(R, cps);
+  k_residual64_part<<<dim3((unsigned)row_blocks, (unsigned)nsplit), 256, 0, st>>>(A, s.lda, R, s.x64, cps, s.rpart);
+  RF_LAUNCH_CHECK();
+  k_residual_sum<<<(unsigned)std::min<int64_t>(ceil_div(R, 256), 1024), 256, 0, st>>>(s.rpart, nsplit, R, b, s.r64);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
 }
 
 __global__ void k_norm2_pair(const double* __restrict__ r, const float* __restrict__ b, int64_t R,
@@ -715,11 +752,29 @@ __global__ void k_axpy64(double* __restrict__ x, const float* __restrict__ d, in
 
 // Factor a copy of A (panels, swaps, triangular block rows, trailing updates)
 // and compose the row permutation.
-static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t st, int* launches_out) {
-  const int64_t R = s.R, lda = s.lda;
+static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t st, int* launches_out,
+                     bool* pivoted, bool* tc_factors) {
+  *tc_factors = false;
+  const int64_t R = s.R, lda = s.ldlu ? s.ldlu : s.lda;
   constexpr int NB = 64;
-  RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, lda * sizeof(float), R * sizeof(float), R,
+  *pivoted = false;
+  RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, s.lda * sizeof(float), R * sizeof(float), R,
                                 cudaMemcpyDeviceToDevice, st));
+  if (!split && s.use_tc && s.LT && (lda % 4) == 0) {
+    // the tensor-core factorization without row exchanges; its factors are
+    // kept when they are those of partial pivoting (every |l_ij| <= 1)
+    bool clean = false;
+    const int rc = lu_factor_tc(s, st, &clean, launches_out);
+    if (rc == RF_E_TIMEOUT) return rc;
+    if (rc == RF_OK && clean) {
+      *tc_factors = true;
+      return RF_OK;
+    }
+    cudaGetLastError();
+    RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, s.lda * sizeof(float), R * sizeof(float), R,
+                                  cudaMemcpyDeviceToDevice, st));
+  }
+  *pivoted = true;
   RF_CUDA_TRY(cudaMemsetAsync(s.info, 0, sizeof(int), st));
   int launches = 0;
   // float4 staging needs every column start 16-byte aligned (k and the chunk
@@ -804,7 +859,7 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
 
 int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1,
                   float* ms) {
-  const int64_t R = s.R, lda = s.lda, k = 0;
+  const int64_t R = s.R, lda = s.ldlu ? s.ldlu : s.lda, k = 0;
   const int nb = (int)std::min<int64_t>(64, R);
   static const cudaError_t smem_attr =
       cudaFuncSetAttribute(k_lu_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemBytes);
@@ -815,7 +870,7 @@ int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st,
   const size_t psmem = (size_t)rows_per * nb * sizeof(float);
   if (psmem > (size_t)kPanelSmemBytes) return RF_E_UNSUPPORTED;
   const int nblk = (int)ceil_div(R - k, rows_per);
-  RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, lda * sizeof(float), R * sizeof(float), R,
+  RF_CUDA_TRY(cudaMemcpy2DAsync(s.LU, lda * sizeof(float), A, s.lda * sizeof(float), R * sizeof(float), R,
                                 cudaMemcpyDeviceToDevice, st));
   RF_CUDA_TRY(cudaMemsetAsync(s.info, 0, sizeof(int), st));
   PanelSmArgs pa{s.LU, lda, R, k, nb, rows_per, s.ipiv, s.pmax, s.pidx, s.prow, s.jrow, s.info};
@@ -833,24 +888,30 @@ int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st,
 // step, after the first two), the matrix is factored again with the split
 // 3xTF32 update and refined from the start.
 int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res) {
-  const int64_t R = s.R, lda = s.lda;
+  const int64_t R = s.R, lda = s.lda, ldlu = s.ldlu ? s.ldlu : s.lda;
+  bool pivoted = false;
   const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 4096);
   int launches = 0, steps = 0;
   double rel = 0.0;
   int factorizations = 0;
   for (int pass = 0; pass < 2; ++pass) {
     const bool split = pass == 1;
-    RF_TRY_RF(lu_factor(s, A, split, st, &launches));
+    bool tcf = false;
+    RF_TRY_RF(lu_factor(s, A, split, st, &launches, &pivoted, &tcf));
+    auto solve = [&](const float* rhs, float* out) -> int {
+      launches += tcf ? 2 : 1 + 4 * (int)ceil_div(R, kSB);
+      return tcf ? lu_solve_tc(s, rhs, out, st) : lu_solve(s.LU, ldlu, R, s.perm, rhs, out, st);
+    };
     ++factorizations;
     // x0 = (LU)^{-1} P b, then refine: r = b - A x (FP64), d = (LU)^{-1} P r
-    RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, b, s.d, st));
+    RF_TRY_RF(solve(b, s.d));
     k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 1);
     double h[2] = {0, 0};
     steps = 0;
     double prev = 0.0;
     bool stalled = false;
     for (;;) {
-      k_residual64<<<(unsigned)ceil_div(R, 256), 256, 0, st>>>(A, lda, R, s.x64, b, s.r64);
+      RF_TRY_RF(launch_residual64(s, A, b, st));
       k_norm2_pair<<<1, 256, 0, st>>>(s.r64, b, R, s.norms);
       RF_LAUNCH_CHECK();
       RF_CUDA_TRY(cudaMemcpyAsync(h, s.norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -862,7 +923,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
       prev = rel;
       // the FP32 residual goes through the output vector, which is overwritten at the end
       k_to_float<<<eb, 256, 0, st>>>(s.r64, x, R);
-      RF_TRY_RF(lu_solve(s.LU, lda, R, s.perm, x, s.d, st));
+      RF_TRY_RF(solve(x, s.d));
       k_axpy64<<<eb, 256, 0, st>>>(s.x64, s.d, R, 0);
       ++steps;
     }
@@ -874,6 +935,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   res->relative_residual = rel;
   res->launches = launches;
   res->factorizations = factorizations;
+  res->pivoted = pivoted;
   return rel <= s.tol ? RF_OK : RF_E_NOCONV;
 }
 

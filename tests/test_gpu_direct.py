@@ -42,7 +42,7 @@ def test_golden_direct(golden, integ):
         st = sim.stats()
         assert st["relative_residual"] <= 1e-6
         # the TF32 tensor-core factors alone suffice for these systems
-        assert st["factorizations"] == 1 and st["refinement_steps"] <= 4
+        assert st["factorizations"] == 1 and st["refinement_steps"] <= 4 and st["pivoted"] == 0
 
 
 def _lu_solve(A, b, tol=1e-7):
@@ -88,3 +88,51 @@ def test_lu_singular_matrix_reports_error():
     A[:, 33] = 0.0
     rc, _ = _lu_solve(A, np.ones(R, np.float32))
     assert rc == C.RF_E_SINGULAR
+
+
+@pytest.mark.parametrize("R", [1, 37, 128, 131, 256, 300, 640, 1000, 4099])
+def test_lu_without_row_exchanges_on_dominant_matrices(R):
+    """Matrices of this problem's kind (identity plus small couplings): every
+    multiplier of the unpivoted factorization is below 1, so partial pivoting
+    would exchange no row and the tensor-core factorization is kept (sizes
+    cover partial last panels, a single panel, and panel pairs); within 1e-5 of
+    an FP64 LAPACK solve after refinement."""
+    rng = np.random.default_rng(100 + R)
+    A = (np.eye(R) + 0.4 * rng.standard_normal((R, R)) / np.sqrt(R)).astype(np.float32)
+    b = rng.standard_normal(R).astype(np.float32)
+    rc, x = _lu_solve(A, b)
+    assert rc == 0
+    ref = np.linalg.solve(A.astype(np.float64), b.astype(np.float64))
+    assert _rel(x, ref) <= 1e-5
+
+
+def test_fiber_system_is_factored_without_row_exchanges():
+    """An N=300 suspension at the precision configuration's density: the
+    direct solver keeps the exchange-free tensor-core factors (stats.pivoted 0)
+    and its forces match the FP64 oracle within 1e-5."""
+    from oracle import oracle as O
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    n = 300
+    pos, ori = sphere_layout(n, 18.0 * (n / 4000.0) ** (1 / 3), 0.2, seed=layout_seed(3, n))
+    sim = Simulation(Config(solver="direct"), pos, ori)
+    sim.assembleSystem()
+    sim.solveSystem()
+    st = sim.stats()
+    assert st["pivoted"] == 0 and st["relative_residual"] <= 1e-6
+    A64, b64 = O.assemble(pos, ori, O.Params(), False, np.float64)
+    ref = np.linalg.solve(A64, b64)
+    assert _rel(sim.solution(), ref) <= 1e-5
+
+
+def test_random_matrix_falls_back_to_row_exchanges():
+    """A general random matrix has multipliers above 1, so the exchange-free
+    factors are discarded and the matrix is factored again with partial
+    pivoting (through the standalone entry point); the answer matches LAPACK."""
+    rng = np.random.default_rng(7)
+    R = 700
+    A = rng.standard_normal((R, R)).astype(np.float32)
+    b = rng.standard_normal(R).astype(np.float32)
+    rc, x = _lu_solve(A, b)
+    assert rc == 0
+    assert _rel(x, np.linalg.solve(A.astype(np.float64), b.astype(np.float64))) <= 1e-5
