@@ -108,9 +108,13 @@ typedef struct rf_stats {
                                 captured CUDA graph (0 while profiling is on) */
   int factorizations;        /* direct solver: 1 = TF32 tensor-core factors refined,
                                 2 = refactored with the 3xTF32 split update */
-  int pivoted;               /* direct solver: 1 when the factorization without row
-                                exchanges met a multiplier above 1 (or a zero pivot)
-                                and the factors were computed with row exchanges */
+  int pivoted;               /* direct solver: 1 when the factors were computed with
+                                row exchanges (partial pivoting) because those without
+                                (static pivoting) met a zero pivot, a multiplier above
+                                64 or did not refine */
+  double max_multiplier;     /* direct solver: largest |l_ij| of the factorization
+                                without row exchanges (at most 1: partial pivoting
+                                would exchange no row; 0 if it did not run) */
 } rf_stats;
 
 typedef struct rf_handle rf_handle;
@@ -229,11 +233,15 @@ int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
  * ViennaCL prod(A, x) behind the reference's GMRES
  * (lib/viennacl/linalg/cuda/matrix_operations_col.hpp:1251-1278). */
 int rf_dense_matvec(const float* A, const float* x, float* y, int64_t R, void* stream);
-/* rf_dense_lu_solve: x = A^{-1} b for column-major FP32 A (R x R) by LU with
- * partial pivoting and FP64-residual refinement until ||b - A x|| / ||b|| <=
- * tol (RF_E_NOCONV after 20 steps, RF_E_SINGULAR on a zero pivot); A and b
- * are not modified.  Replaces MAGMA's magma_sgesv_gpu behind the reference's
- * --magma path (src/simulation.cu:403-418). */
+/* rf_dense_lu_solve: x = A^{-1} b for column-major FP32 A (R x R) by LU and
+ * FP64-residual refinement until ||b - A x|| / ||b|| <= tol (RF_E_NOCONV after
+ * 20 steps, RF_E_SINGULAR on a zero pivot); A and b are not modified.  The LU
+ * is first computed without row exchanges on the tensor cores (static
+ * pivoting; with every multiplier at most 1 these are partial pivoting's
+ * factors) and recomputed with partial pivoting when a pivot vanishes, a
+ * multiplier exceeds 64 or the refinement does not converge.  Replaces
+ * MAGMA's magma_sgesv_gpu behind the reference's --magma path
+ * (src/simulation.cu:403-418). */
 int rf_dense_lu_solve(const float* A, const float* b, float* x, int64_t R, double tol, void* stream);
 /* rf_dense_matvec_noalloc: the same y = A x, for callers that cannot let a
  * library allocate device memory (a host program whose pool allocator owns all

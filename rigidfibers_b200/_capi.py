@@ -58,6 +58,7 @@ class rf_stats(ctypes.Structure):
         ("graph_replays", ctypes.c_int),
         ("factorizations", ctypes.c_int),
         ("pivoted", ctypes.c_int),
+        ("max_multiplier", ctypes.c_double),
     ]
 
 

@@ -618,6 +618,7 @@ int rf_solve(rf_handle* h) {
     h->stats.refinement_steps = lr.refinement_steps;
     h->stats.factorizations = lr.factorizations;
     h->stats.pivoted = lr.pivoted ? 1 : 0;
+    h->stats.max_multiplier = lr.max_multiplier;
     h->stats.relative_residual = lr.relative_residual;
     if (lrc != RF_OK && lrc != RF_E_NOCONV) return lrc;
     h->solved = true;

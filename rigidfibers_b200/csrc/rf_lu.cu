@@ -753,7 +753,7 @@ __global__ void k_axpy64(double* __restrict__ x, const float* __restrict__ d, in
 // Factor a copy of A (panels, swaps, triangular block rows, trailing updates)
 // and compose the row permutation.
 static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t st, int* launches_out,
-                     bool* pivoted, bool* tc_factors) {
+                     bool* pivoted, bool* tc_factors, float* max_l) {
   *tc_factors = false;
   const int64_t R = s.R, lda = s.ldlu ? s.ldlu : s.lda;
   constexpr int NB = 64;
@@ -764,7 +764,7 @@ static int lu_factor(const LuSetup& s, const float* A, bool split, cudaStream_t 
     // the tensor-core factorization without row exchanges; its factors are
     // kept when they are those of partial pivoting (every |l_ij| <= 1)
     bool clean = false;
-    const int rc = lu_factor_tc(s, st, &clean, launches_out);
+    const int rc = lu_factor_tc(s, st, &clean, launches_out, max_l);
     if (rc == RF_E_TIMEOUT) return rc;
     if (rc == RF_OK && clean) {
       *tc_factors = true;
@@ -890,6 +890,7 @@ int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st,
 int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res) {
   const int64_t R = s.R, lda = s.lda, ldlu = s.ldlu ? s.ldlu : s.lda;
   bool pivoted = false;
+  float max_l = 0.f;
   const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 4096);
   int launches = 0, steps = 0;
   double rel = 0.0;
@@ -897,7 +898,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   for (int pass = 0; pass < 2; ++pass) {
     const bool split = pass == 1;
     bool tcf = false;
-    RF_TRY_RF(lu_factor(s, A, split, st, &launches, &pivoted, &tcf));
+    RF_TRY_RF(lu_factor(s, A, split, st, &launches, &pivoted, &tcf, &max_l));
     auto solve = [&](const float* rhs, float* out) -> int {
       launches += tcf ? 2 : 1 + 4 * (int)ceil_div(R, kSB);
       return tcf ? lu_solve_tc(s, rhs, out, st) : lu_solve(s.LU, ldlu, R, s.perm, rhs, out, st);
@@ -917,8 +918,17 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
       RF_CUDA_TRY(cudaMemcpyAsync(h, s.norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
       RF_CUDA_TRY(cudaStreamSynchronize(st));
       rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
-      if (!std::isfinite(rel)) return RF_E_NAN;
-      if (rel <= s.tol || steps >= s.max_refine) break;
+      // factors without row exchanges that do not refine (non-finite, stalled
+      // or out of steps) are replaced by partially pivoted ones
+      if (!std::isfinite(rel)) {
+        if (tcf) { stalled = true; break; }
+        return RF_E_NAN;
+      }
+      if (rel <= s.tol) break;
+      if (steps >= s.max_refine) {
+        stalled = tcf;
+        break;
+      }
       if (!split && steps >= 2 && rel > 0.5 * prev) { stalled = true; break; }
       prev = rel;
       // the FP32 residual goes through the output vector, which is overwritten at the end
@@ -936,6 +946,7 @@ int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, 
   res->launches = launches;
   res->factorizations = factorizations;
   res->pivoted = pivoted;
+  res->max_multiplier = max_l;
   return rel <= s.tol ? RF_OK : RF_E_NOCONV;
 }
 

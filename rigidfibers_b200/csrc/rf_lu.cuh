@@ -44,7 +44,8 @@ struct LuResult {
   int factorizations = 0;   // 2 when the TF32 factors stalled and the split update was used
   int launches = 0;
   double relative_residual = 0.0;
-  bool pivoted = false;     // the row-exchanging factorization ran (a multiplier exceeded 1)
+  bool pivoted = false;     // the row-exchanging factorization ran
+  double max_multiplier = 0.0;   // largest |l_ij| of the factorization without row exchanges
 };
 
 int64_t lu_tc_lt_floats(int64_t R);
@@ -53,9 +54,10 @@ int64_t lu_tc_sinv_floats(int64_t R);
 // x = (LU)^-1 rhs with the factors of lu_factor_tc (no permutation)
 int lu_solve_tc(const LuSetup& s, const float* rhs, float* x, cudaStream_t st);
 // The blocked factorization without row exchanges, all products on tcgen05
-// (s.LU holds a copy of A): *clean when every |l_ij| <= 1 and no pivot
-// vanished, i.e. when these are the factors partial pivoting would produce.
-int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches);
+// (s.LU holds a copy of A): *clean when no pivot vanished and every |l_ij|
+// stays within the static-pivoting limit (at most 1: the factors partial
+// pivoting would produce); *max_l the largest |l_ij|.
+int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches, float* max_l);
 
 // Factor A (column-major, lda) into s.LU and solve A x = b with refinement.
 int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res);

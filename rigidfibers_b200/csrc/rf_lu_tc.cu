@@ -1,17 +1,20 @@
 // Blocked LU without row exchanges, every O(R^3) product on the tensor cores.
 //
-// On the systems of this problem partial pivoting never exchanges a row: the
-// diagonal blocks are the identity, the largest off-diagonal entry stays
-// below 1 (0.55 at N=1000), and elimination keeps every candidate below its
-// diagonal entry.  At step j of LAPACK's sgetrf (MAGMA's magma_sgetrf_gpu
-// behind the reference's --magma path, src/simulation.cu:403-418), the pivot
-// is the diagonal entry exactly when |a_ij / a_jj| <= 1 for every i > j, i.e.
-// when the multipliers l_ij of the unpivoted factorization are at most 1 in
-// magnitude.  So the unpivoted factorization is computed here with BLAS-3
-// operations, and the largest |l_ij| (and any zero pivot) is recorded; when it
-// exceeds 1 the caller discards the factors and runs the pivoted
-// factorization instead, so the factors are always those of partial pivoting
-// (up to rounding order).
+// The systems of this problem have identity diagonal blocks and couplings
+// that are mostly well below 1 (largest off-diagonal entry 0.55 at N=1000 in a
+// sphere of radius 14), so elimination without row exchanges is stable for
+// them.  At step j of LAPACK's sgetrf (MAGMA's magma_sgetrf_gpu behind the
+// reference's --magma path, src/simulation.cu:403-418) the pivot is the
+// diagonal entry exactly when |a_ij / a_jj| <= 1 for every i > j, i.e. when
+// the multipliers l_ij of the unpivoted factorization are at most 1 in
+// magnitude: then these are partial pivoting's factors (up to rounding
+// order).  Nearly touching fibers give multipliers above 1 (up to ~24 in the
+// benchmark layouts); the factors are then kept as a static-pivoting
+// factorization (Li & Demmel, "Making sparse Gaussian elimination scalable
+// by static pivoting", SC 1998: no row exchanges, accuracy recovered by
+// iterative refinement) as long as no pivot vanished and every |l_ij| stays
+// within kStaticPivotLimit; the caller's FP64-residual refinement then
+// decides, and refactors with partial pivoting if it does not converge.
 //
 // Per pair of 128-column panels k, k2 = k + 128 (Golub & Van Loan, the
 // right-looking blocked LU, with the second panel's update looked ahead so the
@@ -61,6 +64,8 @@ constexpr int kTcStages = 2;
 constexpr int kPanel = 128;         // panel width
 constexpr int kLtCols = 2 * kPanel; // columns of the row-major L21 copy
 constexpr uint64_t kDrainNs = 1000000000ull;
+// largest multiplier of factors kept without row exchanges (bounded growth)
+constexpr float kStaticPivotLimit = 64.f;
 
 enum TcMode { kTcStore = 0, kTcSub = 1, kTcStoreL = 2 };
 
@@ -658,29 +663,23 @@ constexpr size_t tc_smem() {
 // ---------------------------------------------------------------------------
 // The w x w diagonal block (w <= 128) at (k, k): factored in shared memory
 // without row exchanges (multiplier a * (1 / pivot), then fmaf(-l, u, a), as
-// the pivoted panel does), written back; the inverses of its factors into
-// Linv (row-major 128 x 128, L11^-1), UinvT (row n = column n of U11^-1) and
-// the triangular solves' copy LinvC (L11^-1 then U11^-1, both column-major),
-// zero outside w x w; the largest |l| into lmax, a zero pivot into status.
+// the pivoted panel does) and written back; the largest |l| into lmax, a zero
+// pivot into status.  The inverses of its factors follow in k_lu_diag_inv.
 //
 // 32 warps, warp w owning columns w, w + 32, w + 64, w + 96, lane l rows
 // l, l + 32, l + 64, l + 96 of each.  No step waits for the whole CTA: the
 // owner of column j + 1 applies step j to that column first, scales it and
 // publishes it through flag[j + 1] (a bounded spin in shared memory), then
 // applies step j to its other columns; every warp applies the steps to its
-// columns in order.  The inverses are column by column, each column of L^-1
-// and U^-1 computed by the warp that owns it from the finished factors.
+// columns in order.
 // ---------------------------------------------------------------------------
 constexpr int kDiagLd = kPanel + 1;
 constexpr uint32_t kDiagSpin = 1u << 26;
 
 __global__ void __launch_bounds__(1024) k_lu_diag(float* __restrict__ A, int64_t lda, int64_t k, int w,
-                                                  float* __restrict__ Linv, float* __restrict__ UinvT,
-                                                  float* __restrict__ LinvC, unsigned int* __restrict__ lmax,
-                                                  int* __restrict__ status) {
+                                                  unsigned int* __restrict__ lmax, int* __restrict__ status) {
   extern __shared__ float sm[];
   float* a = sm;                          // [128][129] row-major block
-  float* x = sm + kPanel * kDiagLd;       // [128][129] inverse being built
   __shared__ volatile int flag[kPanel];   // 1: column j scaled, 2: abort
   const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
   for (int e = tid; e < kPanel * kPanel; e += nt) {
@@ -762,67 +761,78 @@ __global__ void __launch_bounds__(1024) k_lu_diag(float* __restrict__ A, int64_t
     const int r = e % w, c = e / w;
     A[(k + r) + (k + c) * lda] = a[r * kDiagLd + c];
   }
-  // L11^-1: column c starts as e_c; step j (from c on) subtracts l_ij x_jc from
-  // the rows below j (each column independent: only its own warp touches it)
-#pragma unroll 1
-  for (int q = 0; q < 4; ++q) {
-    const int c = warp + 32 * q;
+}
+
+// The inverses of the factored diagonal block (written back by k_lu_diag):
+// 8 CTAs, CTAs 0-3 columns 32b.. of L11^-1, CTAs 4-7 those of U11^-1, one warp
+// per column (lane l: rows l, l + 32, l + 64, l + 96), so the eight run side
+// by side on eight SMs.  L11^-1: column c starts as e_c; step j (from c on)
+// subtracts l_ij x_jc from the rows below j.  U11^-1: step j (from c down to
+// 0) divides x_jc by u_jj and subtracts u_ij x_jc from the rows above j.
+// Outputs: Linv row-major, UinvT (row n = column n of U11^-1), LinvC (both
+// column-major); zero outside w x w.
+__global__ void __launch_bounds__(1024) k_lu_diag_inv(const float* __restrict__ A, int64_t lda, int64_t k, int w,
+                                                      float* __restrict__ Linv, float* __restrict__ UinvT,
+                                                      float* __restrict__ LinvC, const int* __restrict__ status) {
+  if (*status != 0) return;   // a zero pivot: the factors are discarded
+  extern __shared__ float sm[];
+  float* a = sm;                          // [128][129] the factored block
+  float* x = sm + kPanel * kDiagLd;       // [128][33]  this CTA's 32 columns
+  constexpr int kXLd = 33;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool upper = blockIdx.x >= 4;
+  const int c = (blockIdx.x & 3) * 32 + warp;
+  for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+    const int r = e % kPanel, cc = e / kPanel;
+    a[r * kDiagLd + cc] = (r < w && cc < w) ? A[(k + r) + (k + cc) * lda] : (r == cc ? 1.f : 0.f);
+  }
+  __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      x[i * kDiagLd + c] = (i == c && c < w) ? 1.f : 0.f;
-    }
-    __syncwarp();
-    if (c < w) {
+  for (int r = 0; r < 4; ++r) {
+    const int i = lane + 32 * r;
+    x[i * kXLd + warp] = (i == c && c < w) ? 1.f : 0.f;
+  }
+  __syncwarp();
+  if (c < w) {
+    if (!upper) {
       for (int j = c; j < w - 1; ++j) {
-        const float v = x[j * kDiagLd + c];
+        const float v = x[j * kXLd + warp];
         for (int r = (j + 1) >> 5; r < 4; ++r) {
           const int i = lane + 32 * r;
-          if (i > j && i < w) x[i * kDiagLd + c] = fmaf(-a[i * kDiagLd + j], v, x[i * kDiagLd + c]);
+          if (i > j && i < w) x[i * kXLd + warp] = fmaf(-a[i * kDiagLd + j], v, x[i * kXLd + warp]);
         }
         __syncwarp();
       }
-    }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      LinvC[c * kPanel + i] = x[i * kDiagLd + c];
-    }
-  }
-  __syncthreads();
-  for (int e = tid; e < kPanel * kPanel; e += nt) {
-    const int r = e / kPanel, cc = e % kPanel;
-    Linv[r * kPanel + cc] = x[r * kDiagLd + cc];
-  }
-  __syncthreads();
-  // U11^-1: column c starts as e_c; step j (from c down to 0) divides x_jc by
-  // u_jj and subtracts u_ij x_jc from the rows above j
-#pragma unroll 1
-  for (int q = 0; q < 4; ++q) {
-    const int c = warp + 32 * q;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      x[i * kDiagLd + c] = (i == c && c < w) ? 1.f : 0.f;
-    }
-    __syncwarp();
-    if (c < w) {
+    } else {
       for (int j = c; j >= 0; --j) {
-        const float v = x[j * kDiagLd + c] / a[j * kDiagLd + j];
+        const float v = x[j * kXLd + warp] / a[j * kDiagLd + j];
         __syncwarp();
-        if (lane == (j & 31)) x[j * kDiagLd + c] = v;
+        if (lane == (j & 31)) x[j * kXLd + warp] = v;
         for (int r = 0; r <= (j >> 5); ++r) {
           const int i = lane + 32 * r;
-          if (i < j) x[i * kDiagLd + c] = fmaf(-a[i * kDiagLd + j], v, x[i * kDiagLd + c]);
+          if (i < j) x[i * kXLd + warp] = fmaf(-a[i * kDiagLd + j], v, x[i * kXLd + warp]);
         }
         __syncwarp();
       }
     }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = lane + 32 * r;
-      LinvC[kPanel * kPanel + c * kPanel + i] = x[i * kDiagLd + c];
-      UinvT[c * kPanel + i] = x[i * kDiagLd + c];
+  }
+  __syncthreads();
+  // write this CTA's 32 columns (rows 0..127)
+  const int cb = (blockIdx.x & 3) * 32;
+  for (int e = tid; e < kPanel * 32; e += blockDim.x) {
+    const int i = e & (kPanel - 1), cl = e >> 7;   // column-major: coalesced over i
+    const float v = x[i * kXLd + cl];
+    if (!upper) {
+      LinvC[(cb + cl) * kPanel + i] = v;
+    } else {
+      LinvC[kPanel * kPanel + (cb + cl) * kPanel + i] = v;
+      UinvT[(cb + cl) * kPanel + i] = v;
+    }
+  }
+  if (!upper) {
+    for (int e = tid; e < kPanel * 32; e += blockDim.x) {
+      const int cl = e & 31, i = e >> 5;   // row-major rows of L11^-1: 32 consecutive columns
+      Linv[i * kPanel + cb + cl] = x[i * kXLd + cl];
     }
   }
 }
@@ -1040,11 +1050,11 @@ int lu_solve_tc(const LuSetup& s, const float* rhs, float* x, cudaStream_t st) {
 }
 
 // The unpivoted factorization of s.LU (already a copy of A).  Returns RF_OK
-// with *clean = true when every multiplier is at most 1 in magnitude and no
-// pivot vanished (the factors are then those of partial pivoting, with the
-// identity permutation); *clean = false otherwise (the caller refactors with
-// pivoting).  RF_E_TIMEOUT when a bounded wait gave up.
-int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches) {
+// with *clean = true when no pivot vanished and every multiplier is at most
+// kStaticPivotLimit in magnitude (at most 1: the factors of partial pivoting),
+// *max_l the largest |l_ij|; *clean = false otherwise (the caller refactors
+// with pivoting).  RF_E_TIMEOUT when a bounded wait gave up.
+int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches, float* max_l) {
   const int64_t R = s.R, lda = s.ldlu ? s.ldlu : s.lda;
   *clean = false;
   if ((lda % 4) != 0 || (reinterpret_cast<uintptr_t>(s.LU) % 16) != 0 || !s.LT || !s.inv || !s.flags || !s.sinv) {
@@ -1076,10 +1086,13 @@ int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches) 
   RF_TRY_RF(make_map(&mp.uinvT, UinvT, kPanel, kPanel, kPanel * 4, 128));
   const int64_t lim = device_wait_limit();
   const uint64_t wait_ns = lim < 0 ? 1000000000ull : (uint64_t)lim;
-  static const cudaError_t diag_attr =
+  static const cudaError_t diag_attr[2] = {
       cudaFuncSetAttribute(k_lu_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(2 * kPanel * kDiagLd * sizeof(float)));
-  RF_CUDA_TRY(diag_attr);
+                           (int)(kPanel * kDiagLd * sizeof(float))),
+      cudaFuncSetAttribute(k_lu_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)((kPanel * kDiagLd + kPanel * 33) * sizeof(float)))};
+  RF_CUDA_TRY(diag_attr[0]);
+  RF_CUDA_TRY(diag_attr[1]);
   int nl = 0;
   auto base_args = [&]() {
     TcArgs t{};
@@ -1093,9 +1106,12 @@ int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches) 
   // factor the panel at column k (width w): diagonal block, then L21 for rows
   // k + w .. R into the matrix and into LT columns lt_col .. lt_col + 128
   auto panel = [&](int64_t k, int w, int lt_col) -> int {
-    k_lu_diag<<<1, 1024, 2 * kPanel * kDiagLd * sizeof(float), st>>>(
-        s.LU, lda, k, w, Linv, UinvT, s.sinv + (k / kPanel) * 2 * kPanel * kPanel, lmax, status);
+    k_lu_diag<<<1, 1024, kPanel * kDiagLd * sizeof(float), st>>>(s.LU, lda, k, w, lmax, status);
     RF_LAUNCH_CHECK();
+    k_lu_diag_inv<<<8, 1024, (kPanel * kDiagLd + kPanel * 33) * sizeof(float), st>>>(
+        s.LU, lda, k, w, Linv, UinvT, s.sinv + (k / kPanel) * 2 * kPanel * kPanel, status);
+    RF_LAUNCH_CHECK();
+    ++nl;
     ++nl;
     const int64_t m = R - k - w;
     if (m <= 0) return RF_OK;
@@ -1185,7 +1201,8 @@ int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches) 
   }
   float lm;
   std::memcpy(&lm, &h[0], sizeof(float));
-  *clean = h[1] == 0 && lm <= 1.0f;
+  if (max_l) *max_l = lm;
+  *clean = h[1] == 0 && lm <= kStaticPivotLimit;
   return RF_OK;
 }
 

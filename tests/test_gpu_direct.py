@@ -136,3 +136,46 @@ def test_random_matrix_falls_back_to_row_exchanges():
     rc, x = _lu_solve(A, b)
     assert rc == 0
     assert _rel(x, np.linalg.solve(A.astype(np.float64), b.astype(np.float64))) <= 1e-5
+
+
+@pytest.mark.parametrize("big", [5.0, 300.0])
+def test_static_pivoting_and_its_fallback(big):
+    """Multipliers above 1 (a row exchange under partial pivoting): with the
+    largest at 5 the factors without exchanges are kept (static pivoting) and
+    the FP64 refinement recovers the accuracy; at 300 they exceed the limit of
+    64 and the matrix is refactored with partial pivoting.  Either way the
+    solution matches LAPACK within 1e-5."""
+    rng = np.random.default_rng(int(big))
+    R = 700
+    A = np.eye(R) + 0.2 * rng.standard_normal((R, R)) / np.sqrt(R)
+    for i, j in ((3, 200), (150, 400), (500, 650)):
+        A[j, i] = big                     # row j, column i: l_ji ~ big
+    A = A.astype(np.float32)
+    b = rng.standard_normal(R).astype(np.float32)
+    rc, x = _lu_solve(A, b)
+    assert rc == 0
+    assert _rel(x, np.linalg.solve(A.astype(np.float64), b.astype(np.float64))) <= 1e-5
+
+
+def test_evolving_suspension_direct_steps_match_fp64():
+    """Three direct-solver steps of an N=400 suspension at the precision
+    configuration's density (nearly touching pairs appear as it evolves): the
+    forces stay within 1e-5 of the FP64 oracle's solve of the same FP32-formed
+    system, whichever factorization was kept."""
+    from oracle import oracle as O
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200.generate import layout_seed, sphere_layout
+    n = 400
+    pos, ori = sphere_layout(n, 18.0 * (n / 4000.0) ** (1 / 3), 0.2, seed=layout_seed(3, n))
+    sim = Simulation(Config(solver="direct"), pos, ori)
+    for t in range(3):
+        p0, o0 = sim.state()
+        sim.assembleSystem()
+        sim.solveSystem()
+        st = sim.stats()
+        assert st["relative_residual"] <= 1e-6
+        assert st["max_multiplier"] > 0.0
+        A64, b64 = O.assemble(p0, o0, O.Params(), False, np.float64)
+        assert _rel(sim.solution(), np.linalg.solve(A64, b64)) <= 1e-5
+        sim.updateVelocities()
+        sim.updateFibers(t == 0)
