@@ -50,7 +50,8 @@ def parse():
                     help="suspensions in the served ensemble (0: skip the serving leg)")
     ap.add_argument("--serve-max-active", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
-    ap.add_argument("--serve-graphs", type=int, default=1, help="replay GMRES cycles from CUDA graphs (1) or not (0)")
+    ap.add_argument("--serve-graphs", type=int, default=2,
+                    help="CUDA graph mode of the served requests: 2 restart cycles only (default), 1 whole steps, 0 off")
     ap.add_argument("--serve-pack-fibers", type=int, default=0,
                     help="requests of at most this many fibers step together with packed solves (0: off)")
     ap.add_argument("--serve-pack-compare", type=int, default=64,
@@ -400,11 +401,11 @@ def _stream_of(lib, sim):
 
 def time_path(args, dist, cfg, pos, ori, clocks=None, profile=True):
     """W warm-up steps and the autotuner, a checkpoint C, two steps that
-    capture the GMRES graphs (discarded: C is restored), then K steps from C
-    device-timed with the library's defaults (graph replay, no per-launch
-    events; CUDA events on the handle's stream), then the same K steps from C
-    again with CUDA events around every matvec launch (the roofline's
-    per-launch figures; those events rule out graph replay)."""
+    capture the step graph (discarded: C is restored), then K steps from C
+    device-timed with the library's defaults (each step one CUDA graph, no
+    per-launch events; CUDA events on the handle's stream), then the same K
+    steps from C again launched stage by stage with CUDA events around every
+    matvec launch (the roofline's per-launch figures and the stage times)."""
     import ctypes
 
     import torch
@@ -419,7 +420,7 @@ def time_path(args, dist, cfg, pos, ori, clocks=None, profile=True):
     tuned = sim.autotune()          # launch choices, timed on this operator
     ckpt = sim.checkpoint()
     t = args.warmup
-    for _ in range(2):
+    for _ in range(3):
         sim.step(t)
         t += 1
     acc = {"stage": {"assemble_system": 0.0, "solve_system": 0.0, "update_velocities": 0.0, "update_fibers": 0.0},
@@ -437,8 +438,6 @@ def time_path(args, dist, cfg, pos, ori, clocks=None, profile=True):
         sim.step(t)
         t += 1
         st = sim.stats()
-        for k in acc["stage"]:
-            acc["stage"][k] += st["ms_" + k]
         acc["iters"] += st["iterations"]
         acc["iters_per_step"].append(st["iterations"])
         acc["restarts"] += st["restarts"]
@@ -457,6 +456,11 @@ def time_path(args, dist, cfg, pos, ori, clocks=None, profile=True):
         for _ in range(args.steps):
             sim.step(t)
             t += 1
+            # stage times: this pass launches stage by stage (the timed pass
+            # runs each step as one graph and reports its total only)
+            st = sim.stats()
+            for k in acc["stage"]:
+                acc["stage"][k] += st["ms_" + k]
             nl, tm = ctypes.c_int(), ctypes.c_double()
             lib.rf_matvec_profile(sim._h, ctypes.byref(nl), ctypes.byref(tm))
             acc["mv_launches"] += nl.value
@@ -650,7 +654,7 @@ def serve_ensemble(args, dist, pack_fibers=None):
             "completed": int(dist.sum(st["completed"])), "failed": int(dist.sum(st["failed"])),
             "steps": int(dist.sum(st["steps"])), "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
             "max_active": args.serve_max_active, "peak_active": st["peak_active"],
-            "cuda_graphs": bool(args.serve_graphs), "pack_max_fibers": pack,
+            "cuda_graph_mode": args.serve_graphs, "pack_max_fibers": pack,
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps 0.01 or 0.005, 5-50 steps, Poisson arrivals; latency = "
                         "host wall time of one step while others run"}
@@ -695,7 +699,7 @@ def direct_leg(args, n=None, integration="analytical", solvers=("direct", "gmres
 
 
 def _plain(args, dist, total_fiber_steps, cfg):
-    r = time_path(args, dist, cfg, *workload(args), profile=False)
+    r = time_path(args, dist, cfg, *workload(args))
     ms = dist.max(r["ms"])
     return {"value": total_fiber_steps / (ms / 1000.0), "ms_per_step": ms / args.steps,
             "gmres_restart": cfg.gmres_restart,

@@ -105,7 +105,8 @@ def step_record(t, n_fibers, st):
     --verbose, src/main.cu:85-99, as machine-readable records)."""
     rec = {"step": t, "fibers": n_fibers}
     rec.update({k: (round(v, 6) if isinstance(v, float) else v) for k, v in st.items()})
-    rec["ms_step"] = round(sum(st["ms_" + n] for n in STEP_NAMES), 6)
+    # a step run as one CUDA graph reports its total only (stage times 0)
+    rec["ms_step"] = round(st["ms_step"] if st.get("ms_step", 0.0) > 0 else sum(st["ms_" + n] for n in STEP_NAMES), 6)
     return json.dumps(rec, sort_keys=True)
 
 
@@ -200,6 +201,9 @@ def benchmark(args):
                 pos, ori = grown_sphere_layout(n, args.min_distance, seed=layout_seed(100 + rep, n))
                 rep += 1
                 sim = Simulation(make_config(params, args), pos, ori, allow_noconv=True)
+                # per-stage times (performance.out) need the stages launched one by one:
+                # CUDA graphs for the restart cycles only
+                sim.set_cuda_graphs(2)
                 acc = {k: [] for k in STEP_NAMES}
                 for t in range(params["NUMBER_OF_TIMESTEPS"]):
                     sim.step(t)

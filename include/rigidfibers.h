@@ -115,6 +115,9 @@ typedef struct rf_stats {
   double max_multiplier;     /* direct solver: largest |l_ij| of the factorization
                                 without row exchanges (at most 1: partial pivoting
                                 would exchange no row; 0 if it did not run) */
+  double ms_step;            /* the whole last rf_step (CUDA events on the handle's
+                                stream); when the step ran as one CUDA graph the four
+                                stage times above are 0 */
 } rf_stats;
 
 typedef struct rf_handle rf_handle;
@@ -222,9 +225,16 @@ typedef struct rf_tune_report {
 } rf_tune_report;
 int rf_autotune(rf_handle* h, rf_tune_report* report);
 
-/* GMRES restart cycles are captured as CUDA graphs on their second use and
- * replayed afterwards (default on; results are identical either way). */
-int rf_set_cuda_graphs(rf_handle* h, int enable);
+/* CUDA graphs; results are identical in every mode.  mode 1 (default): with
+ * GMRES, rf_step runs the whole time step as one graph from the second step of
+ * its kind on (the first step, and second-order steps): assembly, the restart
+ * cycles in a conditional WHILE node that the solve ends on the device,
+ * velocities and the fiber update, with one read of the solver's control
+ * block afterwards (rf_stats then has ms_step but no stage times).  mode 2:
+ * only the GMRES restart cycles replay from graphs (captured on their second
+ * use; stage times measured).  mode 0: no graphs.  Stage-by-stage calls
+ * (rf_assemble, rf_solve, ...) never use the whole-step graph. */
+int rf_set_cuda_graphs(rf_handle* h, int mode);
 int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
 
 /* Device-pointer entry points (no host copies; pointers are device memory
@@ -272,7 +282,9 @@ typedef struct rf_server rf_server;
 typedef struct rf_server_config {
   int max_active;            /* requests running at once on their own handles */
   int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
-  int use_cuda_graphs;       /* rf_set_cuda_graphs for every request's handle */
+  int use_cuda_graphs;       /* rf_set_cuda_graphs mode of every request's handle
+                                (default 2: restart cycles only; whole-step graphs cost
+                                a capture and an instantiation per request) */
   int pack_max_fibers;       /* requests of at most this many fibers (<= 128, mixed
                                 precision, GMRES, 5 terms, 8x3 quadrature) step together
                                 with packed solves (rf_step_packed); 0: off */

@@ -59,6 +59,7 @@ class rf_stats(ctypes.Structure):
         ("factorizations", ctypes.c_int),
         ("pivoted", ctypes.c_int),
         ("max_multiplier", ctypes.c_double),
+        ("ms_step", ctypes.c_double),
     ]
 
 

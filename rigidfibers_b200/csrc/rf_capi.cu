@@ -136,6 +136,7 @@ struct rf_handle {
   float4* rv[2] = {nullptr, nullptr};
   int vprev = 0, vcur = 1;   // velocity buffers; vcur is written by update_velocities
   int vlast = -1;            // buffer holding the most recent velocities
+  bool vel_fresh = false;    // velocities computed since the last fiber update
   // linear system
   bool mixed = false;        // structured operator + refinement (RF_PREC_MIXED_*)
   float* A = nullptr;        // dense FP32 (RF_PREC_FP32)
@@ -185,7 +186,18 @@ struct rf_handle {
   int restart = 10;          // Krylov dimension per cycle
   int64_t steps_taken = 0;   // completed rf_update_fibers calls (checkpoint metadata)
   GmresGraphCache gmres_graphs;   // captured restart cycles (GMRES)
-  bool use_graphs = true;
+  // The whole time step as one CUDA graph (GMRES): assembly, the first restart
+  // cycle, later cycles in a conditional WHILE node the solve itself ends,
+  // velocities and the fiber update; [0] second-order steps, [1] the first
+  // step.  state: 0 unused, 2 run once directly (captured on the next use),
+  // 1 ready, -1 not capturable here.
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int state = 0;
+    int pre_kernels = 0, cycle_kernels = 0, post_kernels = 0;
+  } step_graph[2];
+  bool use_graphs = true;         // GMRES restart cycles from graphs
+  bool use_step_graphs = true;    // rf_step as one graph
   int mv_variant = 0;             // structured matvec kernel (rf_autotune)
   int64_t ypart_floats = 0;       // capacity of ypart
   bool assembled = false, solved = false;
@@ -220,8 +232,15 @@ struct rf_handle {
     device_bytes += (int64_t)bytes;
     return RF_OK;
   }
+  void release_step_graphs() {
+    for (auto& g : step_graph) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g = StepGraph();
+    }
+  }
   ~rf_handle() {
     gmres_graphs.release();
+    release_step_graphs();
     for (auto e : mv_events) cudaEventDestroy(e);
     for (void* p : allocations) cudaFreeAsync(p, st);
     if (st) cudaStreamSynchronize(st);
@@ -356,6 +375,7 @@ int rf_set_state(rf_handle* h, const double* pos, const double* ori) {
   RF_CUDA_TRY(cudaMemcpyAsync(h->ori32, o32.data(), b32, cudaMemcpyHostToDevice, h->st));
   RF_CUDA_TRY(cudaStreamSynchronize(h->st));
   h->assembled = h->solved = false;
+  h->vel_fresh = false;
   return RF_OK;
 }
 
@@ -534,18 +554,21 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+static int enqueue_assemble(rf_handle* h) {
+  if (h->mixed)
+    return launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
+                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st);
+  if (h->cfg.integration == RF_ANALYTICAL)
+    return launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
+                                      h->lda, h->ffpart, h->F, h->b, h->st);
+  return launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->A, h->lda, h->ffpart,
+                                   h->F, h->b, h->st);
+}
+
 int rf_assemble(rf_handle* h) {
   if (!h) return RF_E_INPUT;
   RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
-  if (h->mixed)
-    RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
-                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st));
-  else if (h->cfg.integration == RF_ANALYTICAL)
-    RF_TRY(launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
-                                      h->lda, h->ffpart, h->F, h->b, h->st));
-  else
-    RF_TRY(launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->A, h->lda, h->ffpart,
-                                     h->F, h->b, h->st));
+  RF_TRY(enqueue_assemble(h));
   h->launches += 2;
   RF_CUDA_TRY(cudaEventRecord(h->ev[1], h->st));
   h->assembled = true;
@@ -553,11 +576,7 @@ int rf_assemble(rf_handle* h) {
   return RF_OK;
 }
 
-int rf_solve(rf_handle* h) {
-  if (!h) return RF_E_INPUT;
-  if (!h->assembled) { set_last_error_str("rf_solve before rf_assemble"); return RF_E_STATE; }
-  RF_CUDA_TRY(cudaEventRecord(h->ev[2], h->st));
-  h->stats.graph_replays = 0;
+static GmresSetup gmres_setup(rf_handle* h) {
   GmresSetup s;
   s.R = h->R;
   s.m = h->restart;
@@ -579,9 +598,13 @@ int rf_solve(rf_handle* h) {
   // launch every cycle directly; otherwise the cycles replay captured graphs
   // (an injected device-wait limit is a kernel argument: no capture or replay then)
   s.graphs = (h->profile || !h->use_graphs || device_wait_limit() >= 0) ? nullptr : &h->gmres_graphs;
-  h->mv_used = 0;
-  int mv_launches = 0;
-  MatvecFn mv = [h, &mv_launches](const float* xin, const int* skip, cudaStream_t st) -> int {
+  return s;
+}
+
+// The Krylov matvec of the handle's operator (optionally timed by events),
+// counting its kernel launches into *launches
+static MatvecFn make_matvec(rf_handle* h, int* launches) {
+  return [h, launches](const float* xin, const int* skip, cudaStream_t st) -> int {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (h->profile) {
       while ((int)h->mv_events.size() < h->mv_used + 2) {
@@ -594,19 +617,38 @@ int rf_solve(rf_handle* h) {
       h->mv_used += 2;
       RF_CUDA_TRY(cudaEventRecord(e0, st));
     }
-    ++mv_launches;
+    ++*launches;
     int rc;
     if (h->mixed) {
       const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
       rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
                                 &h->ctl->timeout, st, h->mv_variant);
-      mv_launches += 2;
+      *launches += 2;
     } else {
       rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
     }
     if (h->profile) RF_CUDA_TRY(cudaEventRecord(e1, st));
     return rc;
   };
+}
+
+// FP64-accumulated residual r = b - A x over the FP32 pair blocks (mixed modes)
+static ResidualFn make_residual(rf_handle* h) {
+  return [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
+    return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
+                                    h->b, r, skip, &h->ctl->timeout, st);
+  };
+}
+
+int rf_solve(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  if (!h->assembled) { set_last_error_str("rf_solve before rf_assemble"); return RF_E_STATE; }
+  RF_CUDA_TRY(cudaEventRecord(h->ev[2], h->st));
+  h->stats.graph_replays = 0;
+  GmresSetup s = gmres_setup(h);
+  h->mv_used = 0;
+  int mv_launches = 0;
+  MatvecFn mv = make_matvec(h, &mv_launches);
   if (h->cfg.solver == RF_SOLVER_DIRECT) {
     LuResult lr;
     const int lrc = lu_factor_solve(h->lu, h->A, h->b, h->x, h->st, &lr);
@@ -645,10 +687,7 @@ int rf_solve(rf_handle* h) {
       // residual, its correction and the FP64 solution use the Krylov basis
       // buffers (the GMRES basis is idle under this solver)
       RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
-      ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
-        return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin),
-                                        h->zpart64, h->b, r, skip, &h->ctl->timeout, st);
-      };
+      ResidualFn resid = make_residual(h);
       BicgIr ir;
       ir.x64 = h->x64;
       ir.r = h->V;
@@ -689,10 +728,7 @@ int rf_solve(rf_handle* h) {
   GmresResult res;
   int rc;
   if (h->mixed) {
-    ResidualFn resid = [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
-      return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
-                                      h->b, r, skip, &h->ctl->timeout, st);
-    };
+    ResidualFn resid = make_residual(h);
     h->refinements = 0;
     rc = gmres_solve_ex(s, mv, resid, h->b, h->x64, true, h->st, &res);
     h->refinements = res.residual_calls;
@@ -718,56 +754,206 @@ int rf_solve(rf_handle* h) {
   return rc;
 }
 
-int rf_update_velocities(rf_handle* h) {
-  if (!h) return RF_E_INPUT;
-  if (!h->solved) { set_last_error_str("rf_update_velocities before rf_solve"); return RF_E_STATE; }
-  RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
+// the velocity kernels and the non-finite guard (read by rf_step after its
+// sync); returns the number of kernels in *kernels
+static int enqueue_velocities(rf_handle* h, int* kernels) {
   const int vint = h->cfg.velocity_integration < 0 ? h->cfg.integration : h->cfg.velocity_integration;
   if (vint == RF_ANALYTICAL) {
     RF_TRY(launch_velocity_analytical(h->tab, h->N, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->x,
                                       h->vpart, h->tv[h->vcur], h->rv[h->vcur], h->st));
-    h->launches += 2;
+    *kernels += 2;
   } else if (h->mixed) {
     RF_TRY(launch_struct_velocity(h->tab, h->N, h->S32, h->ori32, h->F, h->x, h->svpart, h->tv[h->vcur],
                                   h->rv[h->vcur], h->st));
-    h->launches += 2;
+    *kernels += 2;
   } else {
     RF_TRY(launch_velocity_numerical(h->tab, h->N, h->pos64[h->icur], h->ori32, h->x, h->fw, h->vpart, h->tv[h->vcur],
                                      h->rv[h->vcur], h->st));
-    h->launches += 3;
+    *kernels += 3;
   }
-  // non-finite guard on the new velocities (read by rf_step after its sync)
   RF_TRY(launch_check_finite(h->tv[h->vcur], h->rv[h->vcur], h->N, h->vflag, h->st));
-  h->launches += 1;
+  *kernels += 1;
+  return RF_OK;
+}
+
+int rf_update_velocities(rf_handle* h) {
+  if (!h) return RF_E_INPUT;
+  if (!h->solved) { set_last_error_str("rf_update_velocities before rf_solve"); return RF_E_STATE; }
+  RF_CUDA_TRY(cudaEventRecord(h->ev[4], h->st));
+  RF_TRY(enqueue_velocities(h, &h->launches));
   RF_CUDA_TRY(cudaEventRecord(h->ev[5], h->st));
   h->vlast = h->vcur;
+  h->vel_fresh = true;
+  return RF_OK;
+}
+
+// halt: a device word that, when set, makes the update leave the state as it
+// is (the whole-step graph passes the solve's failure word; null otherwise)
+static int enqueue_update_fibers(rf_handle* h, int first_step, const int* halt = nullptr) {
+  // the state rotates in place inside the kernel (src/simulation.cu:307-311;
+  // fortran/fibers.f95:325-341 swap buffers instead)
+  return launch_update_fibers(h->N, first_step, h->cfg.timestep, h->pos64[h->iprev], h->pos64[h->icur],
+                              h->ori64[h->iprev], h->ori64[h->icur], h->tv[h->vprev], h->tv[h->vcur],
+                              h->rv[h->vprev], h->rv[h->vcur], h->pos32, h->ori32, halt, h->st);
+}
+
+static bool step_graph_eligible(const rf_handle* h) {
+  return h->use_graphs && h->use_step_graphs && !h->profile && device_wait_limit() < 0 &&
+         h->cfg.solver == RF_SOLVER_GMRES;
+}
+
+// Capture one stream segment into a graph (nothing runs during the capture).
+static int capture_segment(cudaStream_t st, const std::function<int()>& fn, cudaGraph_t* out) {
+  *out = nullptr;
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return RF_E_CUDA;
+  }
+  int rc = fn();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc == RF_OK && (e != cudaSuccess || !g)) rc = RF_E_CUDA;
+  if (rc != RF_OK) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc;
+  }
+  *out = g;
+  return RF_OK;
+}
+
+// The step graph: [assembly, first GMRES cycle, loop condition] ->
+// WHILE(condition) { later cycle, loop condition } -> [solution cast,
+// velocities, fiber update].  The WHILE node runs the restart cycles on the
+// device, so a step is one graph launch and one read of the control block.
+static int build_step_graph(rf_handle* h, int first_step, rf_handle::StepGraph* sg) {
+  cudaGraph_t G = nullptr, pre = nullptr, body = nullptr, post = nullptr;
+  auto fail = [&](int rc) {
+    for (cudaGraph_t g : {pre, body, post, G})
+      if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    sg->state = -1;
+    return rc;
+  };
+  if (cudaGraphCreate(&G, 0) != cudaSuccess) return fail(RF_E_CUDA);
+  cudaGraphConditionalHandle cond;
+  if (cudaGraphConditionalHandleCreate(&cond, G, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+    return fail(RF_E_CUDA);
+  GmresSetup s = gmres_setup(h);
+  s.graphs = nullptr;
+  int mvk = 0;
+  MatvecFn mv = make_matvec(h, &mvk);
+  ResidualFn resid = h->mixed ? make_residual(h) : ResidualFn();
+  void* xsol = h->mixed ? static_cast<void*>(h->x64) : static_cast<void*>(h->x);
+  int kpre = 2, kcycle = 0, kpost = 1;
+  int rc = capture_segment(h->st, [&]() -> int {
+    RF_TRY(enqueue_assemble(h));
+    return gmres_enqueue_first(s, mv, resid, h->b, xsol, h->mixed, cond, h->st, &kpre);
+  }, &pre);
+  if (rc) return fail(rc);
+  kpre += mvk;
+  mvk = 0;
+  rc = capture_segment(h->st, [&]() -> int {
+    return gmres_enqueue_cycle(s, mv, resid, h->b, xsol, h->mixed, cond, h->st, &kcycle);
+  }, &body);
+  if (rc) return fail(rc);
+  kcycle += mvk + (h->mixed ? 3 : 0);   // the FP64 residual's kernels
+  rc = capture_segment(h->st, [&]() -> int {
+    if (h->mixed) {
+      RF_TRY(launch_cast_to_float(h->x64, h->x, h->R, h->st));
+      ++kpost;
+    }
+    RF_TRY(enqueue_velocities(h, &kpost));
+    return enqueue_update_fibers(h, first_step, &h->ctl->halt);
+  }, &post);
+  if (rc) return fail(rc);
+  cudaGraphNode_t npre, ncond, nbody, npost;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if (cudaGraphAddChildGraphNode(&npre, G, nullptr, 0, pre) != cudaSuccess ||
+      cudaGraphAddNode(&ncond, G, &npre, 1, &cp) != cudaSuccess ||
+      cudaGraphAddChildGraphNode(&nbody, cp.conditional.phGraph_out[0], nullptr, 0, body) != cudaSuccess ||
+      cudaGraphAddChildGraphNode(&npost, G, &ncond, 1, post) != cudaSuccess ||
+      cudaGraphInstantiate(&sg->exec, G, 0) != cudaSuccess) {
+    sg->exec = nullptr;
+    return fail(RF_E_CUDA);
+  }
+  for (cudaGraph_t g : {pre, body, post, G}) cudaGraphDestroy(g);
+  sg->pre_kernels = kpre;
+  sg->cycle_kernels = kcycle;
+  sg->post_kernels = kpost;
+  sg->state = 1;
   return RF_OK;
 }
 
 int rf_update_fibers(rf_handle* h, int first_step) {
   if (!h) return RF_E_INPUT;
-  if (h->vlast != h->vcur) { set_last_error_str("rf_update_fibers before rf_update_velocities"); return RF_E_STATE; }
+  if (!h->vel_fresh) { set_last_error_str("rf_update_fibers before rf_update_velocities"); return RF_E_STATE; }
   RF_CUDA_TRY(cudaEventRecord(h->ev[6], h->st));
-  RF_TRY(launch_update_fibers(h->N, first_step, h->cfg.timestep, h->pos64[h->iprev], h->pos64[h->icur],
-                              h->ori64[h->iprev], h->ori64[h->icur], h->tv[h->vprev], h->tv[h->vcur],
-                              h->rv[h->vprev], h->rv[h->vcur], h->pos64[h->inext], h->ori64[h->inext], h->pos32,
-                              h->ori32, h->st));
+  RF_TRY(enqueue_update_fibers(h, first_step));
   h->launches += 1;
   RF_CUDA_TRY(cudaEventRecord(h->ev[7], h->st));
-  // rotate (src/simulation.cu:307-311; fortran/fibers.f95:325-341)
-  const int p = h->iprev;
-  h->iprev = h->icur;
-  h->icur = h->inext;
-  h->inext = p;
-  std::swap(h->vprev, h->vcur);
+  h->vel_fresh = false;
   h->assembled = h->solved = false;
   h->steps_taken += 1;
   return RF_OK;
 }
 
+// One step as a graph launch (see build_step_graph); the control block and the
+// velocity guard are read once afterwards.
+static int run_step_graph(rf_handle* h, const rf_handle::StepGraph& g) {
+  RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
+  RF_CUDA_TRY(cudaGraphLaunch(g.exec, h->st));
+  RF_CUDA_TRY(cudaEventRecord(h->ev[7], h->st));
+  int vbad = 0;
+  RF_CUDA_TRY(cudaMemcpyAsync(h->host_ctl, h->ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  const GmresCtl c = *h->host_ctl;
+  GmresResult res;
+  const int rc = gmres_result_from_ctl(c, h->mixed, &res);
+  h->launches = g.pre_kernels + c.heads * g.cycle_kernels + g.post_kernels;
+  h->matvecs_done = res.matvecs;
+  h->mv_used = 0;
+  h->refinements = h->mixed ? res.residual_calls : 0;
+  h->stats.iterations = res.iterations;
+  h->stats.restarts = res.restarts;
+  h->stats.refinement_steps = h->refinements;
+  h->stats.relative_residual = res.relative_residual;
+  h->stats.graph_replays = 1;
+  h->stats.ms_assemble_system = h->stats.ms_solve_system = 0.0;
+  h->stats.ms_update_velocities = h->stats.ms_update_fibers = 0.0;
+  h->stats.ms_step = elapsed(h->ev[0], h->ev[7]);
+  h->stats.kernel_launches = h->launches;
+  if (rc == RF_E_NAN || rc == RF_E_TIMEOUT) {
+    // the update left the state as it was; the velocities are not valid
+    h->assembled = h->solved = false;
+    h->vel_fresh = false;
+    return rc;
+  }
+  h->vlast = h->vcur;
+  h->vel_fresh = false;
+  h->assembled = h->solved = false;
+  h->steps_taken += 1;
+  if (vbad) {
+    set_last_error_str("non-finite velocity");
+    return RF_E_NAN;
+  }
+  return rc;
+}
+
 int rf_step(rf_handle* h, int t) {
   if (!h) return RF_E_INPUT;
   h->launches = 0;
+  if (step_graph_eligible(h)) {
+    rf_handle::StepGraph& g = h->step_graph[t == 0 ? 1 : 0];
+    if (g.state == 2) build_step_graph(h, t == 0, &g);   // -1 when not capturable: direct launches
+    if (g.state == 1) return run_step_graph(h, g);
+    if (g.state == 0) g.state = 2;                         // the next step of this kind is captured
+  }
   // NVTX ranges with the reference's step names (src/performance.cc)
   struct Range {
     explicit Range(const char* n) { nvtxRangePushA(n); }
@@ -803,6 +989,7 @@ int rf_step(rf_handle* h, int t) {
   h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
   h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
   h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
+  h->stats.ms_step = elapsed(h->ev[0], h->ev[7]);
   h->stats.kernel_launches = h->launches;
   return rc;
 }
@@ -1188,11 +1375,15 @@ int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* st
   const bool idx_ok = c.iprev >= 0 && c.iprev < 3 && c.icur >= 0 && c.icur < 3 && c.iprev != c.icur &&
                       (c.vprev == 0 || c.vprev == 1) && c.vcur == 1 - c.vprev && c.vlast >= -1 && c.vlast < 2;
   if (!idx_ok) { set_last_error_str("rf_checkpoint_load: corrupt buffer indices"); return RF_E_INPUT; }
+  // the step graphs hold the buffer roles they were captured with
+  if (h->iprev != c.iprev || h->icur != c.icur || h->vprev != c.vprev || h->vcur != c.vcur)
+    h->release_step_graphs();
   h->iprev = c.iprev;
   h->icur = c.icur;
   h->inext = 3 - c.iprev - c.icur;
   h->vprev = c.vprev;
   h->vcur = c.vcur;
+  h->vel_fresh = false;
   h->vlast = c.vlast;
   h->steps_taken = c.steps_taken;
   const unsigned char* in = static_cast<const unsigned char*>(buf);
@@ -1234,6 +1425,7 @@ static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
     h->gemv_plan = plan_dense_gemv(h->R, h->num_sms, t.gemv_ctas_per_sm);
   }
   h->gmres_graphs.release();   // the captured cycles hold the old launch parameters
+  h->release_step_graphs();
 }
 
 int rf_autotune(rf_handle* h, rf_tune_report* out) {
@@ -1334,9 +1526,11 @@ int rf_debug_fail_allocation_after(int n) {
   return RF_OK;
 }
 
-int rf_set_cuda_graphs(rf_handle* h, int enable) {
-  if (!h) return RF_E_INPUT;
-  h->use_graphs = enable != 0;
+int rf_set_cuda_graphs(rf_handle* h, int mode) {
+  if (!h || mode < 0 || mode > 2) return RF_E_INPUT;
+  h->use_graphs = mode != 0;
+  h->use_step_graphs = mode == 1;
+  if (!h->use_step_graphs) h->release_step_graphs();
   return RF_OK;
 }
 

@@ -99,8 +99,10 @@ int launch_velocity_numerical(const Tables& tab, int N, const double4* pos64, co
 int launch_velocity_analytical(const Tables& tab, int N, const float4* ori, const double4* pos64,
                                const double4* ori64, const float* x, float* vpart, float4* tvel, float4* rvel,
                                cudaStream_t st);
-int launch_update_fibers(int N, int first, double dt, const double4* pp, const double4* cp, const double4* po,
-                         const double4* co, const float4* ptv, const float4* ctv, const float4* prv,
-                         const float4* crv, double4* np, double4* no, float4* pos32, float4* ori32,
-                         cudaStream_t st);
+// The second-order (or first-step Euler) update; rotates the state in place:
+// prev <- cur, cur <- new, previous velocities <- current ones.  halt (may be
+// null): a device word that, when set, leaves the state untouched.
+int launch_update_fibers(int N, int first, double dt, double4* pp, double4* cp, double4* po, double4* co,
+                         float4* ptv, const float4* ctv, float4* prv, const float4* crv, float4* pos32, float4* ori32,
+                         const int* halt, cudaStream_t st);
 }  // namespace rf

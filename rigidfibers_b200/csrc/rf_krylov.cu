@@ -263,6 +263,7 @@ __global__ void k_gmres_residual(GmresArgs a, int mode) {
       V0[r] *= inv;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (mode != 0) a.ctl->heads += 1;
     a.ctl->beta = beta;
     a.ctl->converged = conv ? 1 : 0;
     a.ctl->nan = bad ? 1 : 0;
@@ -581,6 +582,122 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   res->restarts = h.restarts;
   // a restart cycle opens with a matvec of x, or with the caller's residual (not a matvec)
   res->matvecs = h.total_iters + (residual ? 0 : cycles_run - 1);
+  res->relative_residual = h.bnorm > 0 ? h.beta / h.bnorm : 0.0;
+  if (h.timeout) {
+    set_last_error_str("a bounded device-side wait timed out");
+    return RF_E_TIMEOUT;
+  }
+  if (h.nan) return RF_E_NAN;
+  if (!h.converged) return RF_E_NOCONV;
+  return RF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// GMRES as a graph with a device-side restart loop
+// ---------------------------------------------------------------------------
+__global__ void k_gmres_ctl_init(GmresCtl* ctl, double tol, int maxit) {
+  GmresCtl c{};
+  c.tol = tol;
+  c.maxit = maxit;
+  *ctl = c;
+}
+
+// another restart cycle is needed: not converged, no failure, iterations left
+__global__ void k_gmres_loop_cond(cudaGraphConditionalHandle cond, GmresCtl* ctl) {
+  const bool more = !ctl->converged && !ctl->nan && !ctl->timeout && ctl->total_iters < ctl->maxit &&
+                    ctl->restarts <= ctl->maxit + 2;
+  ctl->halt = (ctl->nan || ctl->timeout) ? 1 : 0;
+  cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+static GmresArgs gmres_args(const GmresSetup& s, const float* b, void* x, bool x_double) {
+  GmresArgs a;
+  a.ypart = s.ypart;
+  a.nsplit = s.nsplit;
+  a.b = b;
+  a.x = x;
+  a.x_double = x_double ? 1 : 0;
+  a.V = s.V;
+  a.ldv = s.ldv;
+  a.R = s.R;
+  a.m = s.m;
+  a.part = s.part;
+  a.stride = kMaxRestart + 2;
+  a.H = s.H;
+  a.cs = s.cs;
+  a.sn = s.sn;
+  a.g = s.g;
+  a.ctl = s.ctl;
+  return a;
+}
+
+// m x (matvec + Arnoldi step) of the cycle whose first basis vector is in V[0]
+static int enqueue_arnoldi_steps(const GmresSetup& s, GmresArgs& a, const MatvecFn& matvec, cudaStream_t st,
+                                 int* kernels) {
+  for (int j = 0; j < s.m; ++j) {
+    int rc = matvec(s.V + (int64_t)j * s.ldv, &s.ctl->cycle_done, st);
+    if (rc) return rc;
+    void* args[] = {&a, &j};
+    rc = coop_launch((const void*)k_gmres_arnoldi, s.coop_blocks, 256, args, st);
+    if (rc) return rc;
+    *kernels += 1;
+  }
+  k_gmres_update<<<s.coop_blocks, 256, 0, st>>>(a);
+  RF_LAUNCH_CHECK();
+  *kernels += 1;
+  return RF_OK;
+}
+
+int gmres_enqueue_first(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                        void* x, bool x_double, cudaGraphConditionalHandle cond, cudaStream_t st, int* kernels) {
+  if (s.m < 1 || s.m > kMaxRestart) {
+    set_last_error_str("gmres: restart length out of range");
+    return RF_E_INPUT;
+  }
+  GmresArgs a = gmres_args(s, b, x, x_double);
+  k_gmres_ctl_init<<<1, 1, 0, st>>>(s.ctl, s.tol, s.maxit);
+  if (x_double)
+    k_fill_zero<double><<<std::min<int64_t>(ceil_div(s.R, 256), 1024), 256, 0, st>>>(static_cast<double*>(x), s.R);
+  else
+    k_fill_zero<float><<<std::min<int64_t>(ceil_div(s.R, 256), 1024), 256, 0, st>>>(static_cast<float*>(x), s.R);
+  RF_LAUNCH_CHECK();
+  *kernels += 2;
+  void* args0[] = {&a};
+  if (int rc = coop_launch((const void*)k_gmres_init, s.coop_blocks, 256, args0, st)) return rc;
+  int mode = 0;
+  void* args1[] = {&a, &mode};
+  if (int rc = coop_launch((const void*)k_gmres_residual, s.coop_blocks, 256, args1, st)) return rc;
+  *kernels += 2;
+  if (int rc = enqueue_arnoldi_steps(s, a, matvec, st, kernels)) return rc;
+  k_gmres_loop_cond<<<1, 1, 0, st>>>(cond, s.ctl);
+  RF_LAUNCH_CHECK();
+  *kernels += 1;
+  (void)residual;
+  return RF_OK;
+}
+
+int gmres_enqueue_cycle(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                        void* x, bool x_double, cudaGraphConditionalHandle cond, cudaStream_t st, int* kernels) {
+  GmresArgs a = gmres_args(s, b, x, x_double);
+  const int rc0 = residual ? residual(x, s.V, &s.ctl->converged, st)
+                           : matvec(static_cast<const float*>(x), &s.ctl->converged, st);
+  if (rc0) return rc0;
+  int mode = residual ? 2 : 1;
+  void* args1[] = {&a, &mode};
+  if (int rc = coop_launch((const void*)k_gmres_residual, s.coop_blocks, 256, args1, st)) return rc;
+  *kernels += 1;
+  if (int rc = enqueue_arnoldi_steps(s, a, matvec, st, kernels)) return rc;
+  k_gmres_loop_cond<<<1, 1, 0, st>>>(cond, s.ctl);
+  RF_LAUNCH_CHECK();
+  *kernels += 1;
+  return RF_OK;
+}
+
+int gmres_result_from_ctl(const GmresCtl& h, bool has_residual, GmresResult* res) {
+  res->iterations = h.total_iters;
+  res->restarts = h.restarts;
+  res->residual_calls = has_residual ? h.heads : 0;
+  res->matvecs = h.total_iters + (has_residual ? 0 : h.heads);
   res->relative_residual = h.bnorm > 0 ? h.beta / h.bnorm : 0.0;
   if (h.timeout) {
     set_last_error_str("a bounded device-side wait timed out");

@@ -18,6 +18,8 @@ struct GmresCtl {
   int maxit;
   int restarts;
   int timeout;        // a bounded device-side wait gave up (set by kernels)
+  int heads;          // restart cycles opened from the residual of x (after the first)
+  int halt;           // the solve failed (non-finite or timed out): later stages skip
   double tol;
   double bnorm;
   double beta;        // true residual norm at the last cycle start
@@ -93,6 +95,21 @@ int gmres_solve(const GmresSetup& s, const MatvecFn& matvec, const float* b, flo
 // with `residual` and accumulates the correction into x (FP64 if x_double).
 int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b, void* x,
                    bool x_double, cudaStream_t st, GmresResult* res);
+
+// The same solve as launches without host synchronisation, for capture into a
+// graph whose restart loop is a conditional WHILE node (handle `cond`):
+// gmres_enqueue_first enqueues the control-block set-up, x = 0, ||b||, the
+// first cycle and the loop condition; gmres_enqueue_cycle one later cycle
+// (residual of x, m Arnoldi steps, update) and the loop condition.  Steps after
+// convergence return at once on the device.  *kernels counts the kernels
+// these functions launch themselves (the callbacks count theirs).
+int gmres_enqueue_first(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                        void* x, bool x_double, cudaGraphConditionalHandle cond, cudaStream_t st, int* kernels);
+int gmres_enqueue_cycle(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn& residual, const float* b,
+                        void* x, bool x_double, cudaGraphConditionalHandle cond, cudaStream_t st, int* kernels);
+// The solve's outcome from a host copy of its control block (after such a
+// graph ran); returns the status gmres_solve_ex would have returned.
+int gmres_result_from_ctl(const GmresCtl& h, bool has_residual, GmresResult* res);
 
 // BiCGSTAB control block (device); stop_word is what the matvec kernels read.
 struct BicgCtl {

@@ -312,7 +312,7 @@ int rf_server_config_default(rf_server_config* c) {
   if (!c) return RF_E_INPUT;
   std::memset(c, 0, sizeof(*c));
   c->max_active = 16;
-  c->use_cuda_graphs = 1;
+  c->use_cuda_graphs = 2;   // restart cycles only: short requests do not repay capturing whole steps
   c->pack_max_fibers = 0;
   c->pack_max_members = 148;
   size_t fr = 0, tot = 0;

@@ -278,12 +278,18 @@ int launch_velocity_numerical(const Tables& tab, int N, const double4* pos64, co
 
 // first != 0: x1 = x0 + dt U0, t1 = normalize(t0 + dt W0)
 // otherwise: x^{n+1} = 4/3 x^n - 1/3 x^{n-1} + 2/3 dt (2 U^n - U^{n-1}), same for t, normalised.
-__global__ void k_update_fibers(int N, int first, double dt, const double4* __restrict__ prev_pos,
-                                const double4* __restrict__ cur_pos, const double4* __restrict__ prev_ori,
-                                const double4* __restrict__ cur_ori, const float4* __restrict__ prev_tv,
-                                const float4* __restrict__ cur_tv, const float4* __restrict__ prev_rv,
-                                const float4* __restrict__ cur_rv, double4* __restrict__ next_pos,
-                                double4* __restrict__ next_ori, float4* __restrict__ pos32, float4* __restrict__ ori32) {
+// The state rotates in place (the reference swaps buffers, src/simulation.cu:
+// 307-311): each fiber's previous state becomes its current one, the current
+// one the new state, and the previous velocities the current ones, so the
+// buffers a step reads and writes never change (one CUDA graph serves every
+// step).
+__global__ void k_update_fibers(int N, int first, double dt, double4* __restrict__ prev_pos,
+                                double4* __restrict__ cur_pos, double4* __restrict__ prev_ori,
+                                double4* __restrict__ cur_ori, float4* __restrict__ prev_tv,
+                                const float4* __restrict__ cur_tv, float4* __restrict__ prev_rv,
+                                const float4* __restrict__ cur_rv, float4* __restrict__ pos32,
+                                float4* __restrict__ ori32, const int* __restrict__ halt) {
+  if (halt != nullptr && *halt) return;   // the solve failed: the state stays as it is
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double4 xc = cur_pos[i], tc = cur_ori[i];
@@ -305,18 +311,21 @@ __global__ void k_update_fibers(int N, int first, double dt, const double4* __re
   }
   const double inv = 1.0 / sqrt(tn.x * tn.x + tn.y * tn.y + tn.z * tn.z);
   tn.x *= inv; tn.y *= inv; tn.z *= inv;
-  next_pos[i] = xn;
-  next_ori[i] = tn;
+  prev_pos[i] = xc;
+  prev_ori[i] = tc;
+  cur_pos[i] = xn;
+  cur_ori[i] = tn;
+  prev_tv[i] = u;
+  prev_rv[i] = w;
   pos32[i] = make_float4((float)xn.x, (float)xn.y, (float)xn.z, 0.f);
   ori32[i] = make_float4((float)tn.x, (float)tn.y, (float)tn.z, 0.f);
 }
 
-int launch_update_fibers(int N, int first, double dt, const double4* pp, const double4* cp, const double4* po,
-                         const double4* co, const float4* ptv, const float4* ctv, const float4* prv,
-                         const float4* crv, double4* np, double4* no, float4* pos32, float4* ori32,
-                         cudaStream_t st) {
-  k_update_fibers<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(N, first, dt, pp, cp, po, co, ptv, ctv, prv, crv, np,
-                                                              no, pos32, ori32);
+int launch_update_fibers(int N, int first, double dt, double4* pp, double4* cp, double4* po, double4* co,
+                         float4* ptv, const float4* ctv, float4* prv, const float4* crv, float4* pos32, float4* ori32,
+                         const int* halt, cudaStream_t st) {
+  k_update_fibers<<<(unsigned)ceil_div(N, 128), 128, 0, st>>>(N, first, dt, pp, cp, po, co, ptv, ctv, prv, crv, pos32,
+                                                              ori32, halt);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }

@@ -45,7 +45,9 @@ class Server:
         if hbm_budget_bytes is not None:
             sc.hbm_budget_bytes = int(hbm_budget_bytes)
         if use_cuda_graphs is not None:
-            sc.use_cuda_graphs = int(bool(use_cuda_graphs))
+            # True / False as before; an int is the rf_set_cuda_graphs mode (0, 1 or 2)
+            sc.use_cuda_graphs = (2 if use_cuda_graphs else 0) if isinstance(use_cuda_graphs, bool) else \
+                int(use_cuda_graphs)
         if pack_max_fibers is not None:
             sc.pack_max_fibers = int(pack_max_fibers)
         if pack_max_members is not None:

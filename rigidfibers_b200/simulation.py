@@ -172,6 +172,11 @@ class Simulation:
         C.check(self._lib.rf_operator_apply(self._h, C.ptr(xx), C.ptr(y), int(which)), "rf_operator_apply")
         return y
 
+    def set_cuda_graphs(self, mode):
+        """0: no CUDA graphs; 1: each rf_step one graph (default); 2: graphs for
+        the GMRES restart cycles only, so that the stage times are measured."""
+        C.check(self._lib.rf_set_cuda_graphs(self._h, int(mode)), "rf_set_cuda_graphs")
+
     def autotune(self):
         """Time the matvec launch choices on the assembled operator and keep the
         fastest (rf_autotune); assembles first if needed."""

@@ -296,6 +296,35 @@ def test_graph_replays_equal_direct_launches(prec):
     assert np.array_equal(tv0, tv1) and np.array_equal(rv0, rv1)
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed_fp16"])
+def test_whole_step_graph_equals_direct_launches(prec):
+    """rf_step as one CUDA graph (restart cycles in a conditional WHILE node
+    ended on the device) gives the same bits and the same iteration counts as
+    the step launched kernel by kernel with graphs off, for the first step and
+    the second-order steps."""
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(90, 3.8, seed=29)
+    runs = []
+    for graphs in (0, 1):
+        sim = Simulation(Config(precision=prec, gmres_restart=6, refinement_restart=6), pos, ori)
+        C.load().rf_set_cuda_graphs(sim._h, graphs)
+        its, whole = [], 0
+        for t in range(7):
+            sim.step(t)
+            st = sim.stats()
+            its.append(st["iterations"])
+            whole += st["ms_step"] > 0 and st["ms_solve_system"] == 0.0
+        runs.append((sim.state(), sim.velocities(), its, whole))
+        sim.close()
+    (p0, o0), (tv0, rv0), it0, w0 = runs[0]
+    (p1, o1), (tv1, rv1), it1, w1 = runs[1]
+    assert w0 == 0 and w1 >= 4          # steps 2..6 of the second kind replay the graph
+    assert it0 == it1
+    assert np.array_equal(p0, p1) and np.array_equal(o0, o1)
+    assert np.array_equal(tv0, tv1) and np.array_equal(rv0, rv1)
+
+
 @pytest.mark.parametrize("n", [100, 300, 600])
 def test_gmres_iterations_match_oracle_over_three_steps(n):
     """The plain FP32 path's GMRES(10) (tol 1e-5, x0 = 0) against the oracle's
