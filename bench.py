@@ -655,6 +655,8 @@ def serve_ensemble(args, dist, pack_fibers=None):
             "steps": int(dist.sum(st["steps"])), "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
             "max_active": args.serve_max_active, "peak_active": st["peak_active"],
             "cuda_graph_mode": args.serve_graphs, "pack_max_fibers": pack,
+            **({"pack_steps": st["pack_steps"], "pack_p50_ms": st["pack_p50_ms"], "pack_p99_ms": st["pack_p99_ms"],
+                "pack_max_ms": st["pack_max_ms"], "pack_mean_members": st["pack_mean_members"]} if pack else {}),
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps 0.01 or 0.005, 5-50 steps, Poisson arrivals; latency = "
                         "host wall time of one step while others run"}

@@ -308,6 +308,11 @@ typedef struct rf_server_stats {
   int peak_active;
   int64_t peak_bytes;
   int completed, failed, queued, active;
+  /* the pack (pack_max_fibers > 0): its rf_step_packed calls, their host wall
+     time percentiles and maximum, and the mean suspensions per call */
+  int64_t pack_steps;
+  double pack_p50_ms, pack_p99_ms, pack_max_ms;
+  double pack_mean_members;
 } rf_server_stats;
 
 /* Device bytes a handle of this configuration and size allocates (an upper

@@ -106,6 +106,11 @@ class rf_server_stats(ctypes.Structure):
         ("failed", ctypes.c_int),
         ("queued", ctypes.c_int),
         ("active", ctypes.c_int),
+        ("pack_steps", ctypes.c_int64),
+        ("pack_p50_ms", ctypes.c_double),
+        ("pack_p99_ms", ctypes.c_double),
+        ("pack_max_ms", ctypes.c_double),
+        ("pack_mean_members", ctypes.c_double),
     ]
 
 

@@ -90,10 +90,25 @@ struct AsmOut {
   const double4* ori64;
 };
 
+// Tile pair L of a suspension of N fibers: numerical, unordered pairs (I <= J)
+// whose one evaluation of K serves both blocks; analytical, ordered pairs.
+template <int Q, int INTEG>
+__device__ __forceinline__ void asm_tile_of(int N, unsigned L, int& I, int& J) {
+  constexpr int TI = 192 / Q;
+  if (INTEG == kNumerical) {
+    tile_pair(L, I, J);
+  } else {
+    const int T = (N + TI - 1) / TI;
+    I = (int)(L / T);
+    J = (int)(L % T);
+  }
+}
+
+// One CTA's tile pair (I, J) of one suspension (the body of k_assemble_pairs and
+// of the packed assembly, which maps its blocks onto many suspensions' tiles).
 template <int M, int Q, int MODE, int INTEG>
-__global__ void __launch_bounds__(192, INTEG == kNumerical ? 4 : 2)
-k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
-                 AsmOut out) {
+__device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, const float4* __restrict__ pos,
+                                                   const float4* __restrict__ ori, const AsmOut& out, int I, int J) {
   using S = AsmShape<M, Q>;
   constexpr int TI = S::TI, K1 = S::K1, NC = S::NC, H = S::H;
   constexpr int M3 = 3 * M;
@@ -114,14 +129,6 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   // evaluation of K; analytical: ordered tile pairs, direct blocks only
   constexpr bool SYM = INTEG == kNumerical;
   static_assert(SYM || MODE == kAsmDense, "structured storage needs the symmetric numerical blocks");
-  int I, J;
-  if (SYM) {
-    tile_pair(blockIdx.x, I, J);
-  } else {
-    const int T = (N + TI - 1) / TI;
-    I = (int)(blockIdx.x / T);
-    J = (int)(blockIdx.x % T);
-  }
   const bool diag = (I == J);
   const int tid = threadIdx.x;
   const int i0 = I * TI, j0 = J * TI;
@@ -417,13 +424,22 @@ k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const 
   }
 }
 
-// F[i][k] = sum_X ffpart[X][i][k] (fixed order); b[i][k'] = -C_i(k') F[i][k'+1].
-__global__ void k_force_terms(const Tables tab, int N, const float4* __restrict__ ori,
-                              const float* __restrict__ ffpart, int nparts, float* __restrict__ F,
-                              float* __restrict__ b) {
+template <int M, int Q, int MODE, int INTEG>
+__global__ void __launch_bounds__(192, INTEG == kNumerical ? 4 : 2)
+k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
+                 AsmOut out) {
+  int I, J;
+  asm_tile_of<Q, INTEG>(N, blockIdx.x, I, J);
+  assemble_pair_tile<M, Q, MODE, INTEG>(tab, N, pos, ori, out, I, J);
+}
+
+// F[i][k] = sum_X ffpart[X][i][k] (fixed order); b[i][k'] = -C_i(k') F[i][k'+1]
+// for unit u = (i, k) of N (M + 1).
+__device__ __forceinline__ void force_term_unit(const Tables& tab, int N, const float4* __restrict__ ori,
+                                                const float* __restrict__ ffpart, int nparts, float* __restrict__ F,
+                                                float* __restrict__ b, int64_t u) {
   const int M = tab.M, K1 = M + 1, FFn = 3 * K1;
-  const int64_t n = (int64_t)N * K1;
-  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+  {
     const int i = (int)(u / K1), k = (int)(u % K1);
     float s[3] = {0.f, 0.f, 0.f};
     for (int p = 0; p < nparts; ++p) {
@@ -443,6 +459,63 @@ __global__ void k_force_terms(const Tables tab, int N, const float4* __restrict_
       for (int a = 0; a < 3; ++a) dst[a] = kp == 0 ? -coef * t3[a] * QF : -coef * (s[a] - E * t3[a] * QF);
     }
   }
+}
+
+__global__ void k_force_terms(const Tables tab, int N, const float4* __restrict__ ori,
+                              const float* __restrict__ ffpart, int nparts, float* __restrict__ F,
+                              float* __restrict__ b) {
+  const int64_t n = (int64_t)N * (tab.M + 1);
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x)
+    force_term_unit(tab, N, ori, ffpart, nparts, F, b, u);
+}
+
+// ---- packed step: every member of a group (one Tables) in one launch ------
+// Block b belongs to the member whose tile pairs it falls in; the member's
+// blocks run exactly the single-suspension kernel's tile code, so a member's
+// system is bit for bit the one k_assemble_pairs forms.
+template <int MODE>
+__global__ void __launch_bounds__(192, 4)
+k_pack_assemble(const Tables tab, const PackStepMember* __restrict__ mem, int n) {
+  const int L = (int)blockIdx.x;
+  const PackStepMember& p = mem[pack_member_of(n, L, [&](int m) { return mem[m].asm_start; })];
+  AsmOut out{};
+  out.S32 = p.S32;
+  out.S16 = p.S16;
+  out.ffpart = p.ffpart;
+  out.pos64 = p.pos64;
+  int I, J;
+  asm_tile_of<24, kNumerical>(p.N, (unsigned)(L - p.asm_start), I, J);
+  assemble_pair_tile<5, 24, MODE, kNumerical>(tab, p.N, p.pos32, p.ori32, out, I, J);
+}
+
+// one block per member: its force terms and right-hand side
+__global__ void __launch_bounds__(256) k_pack_force_terms(const Tables tab, const PackStepMember* __restrict__ mem) {
+  const PackStepMember& p = mem[blockIdx.x];
+  const int N = p.N;
+  const int64_t n = (int64_t)N * (tab.M + 1);
+  const int nparts = (N + AsmShape<5, 24>::TI - 1) / AsmShape<5, 24>::TI;
+  for (int64_t u = threadIdx.x; u < n; u += blockDim.x) force_term_unit(tab, N, p.ori32, p.ffpart, nparts, p.F, p.b, u);
+}
+
+int launch_pack_assemble(const Tables& tab, const PackStepMember* members, int n, int64_t blocks, bool bf16,
+                         cudaStream_t st) {
+  if (tab.M != 5 || tab.Q != 24 || n < 1 || blocks < 1) return RF_E_UNSUPPORTED;
+  constexpr size_t smem = AsmShape<5, 24>::kSmem;
+  if (bf16) {
+    static const cudaError_t attr = cudaFuncSetAttribute(k_pack_assemble<kAsmStructBF16>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    RF_CUDA_TRY(attr);
+    k_pack_assemble<kAsmStructBF16><<<(unsigned)blocks, 192, smem, st>>>(tab, members, n);
+  } else {
+    static const cudaError_t attr = cudaFuncSetAttribute(k_pack_assemble<kAsmStructF16>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    RF_CUDA_TRY(attr);
+    k_pack_assemble<kAsmStructF16><<<(unsigned)blocks, 192, smem, st>>>(tab, members, n);
+  }
+  RF_LAUNCH_CHECK();
+  k_pack_force_terms<<<(unsigned)n, 256, 0, st>>>(tab, members);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
 }
 
 // out[r] = sum over parts p of part[p][r], fixed order.

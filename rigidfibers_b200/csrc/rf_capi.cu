@@ -5,7 +5,6 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
-#include <thread>
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
@@ -34,6 +33,107 @@ void set_last_error_str(const char* msg) { g_last_error = msg; }
 static std::atomic<int64_t> g_wait_limit{-1};
 static std::atomic<int> g_fail_alloc_after{-1};
 int64_t device_wait_limit() { return g_wait_limit.load(); }
+
+// ---- memory for handles that come and go while others step ----------------
+// Allocating or freeing page-locked host memory is an implicit synchronisation
+// point of the whole device, so the handles' small page-locked control blocks
+// come from this process-wide pool: slabs are allocated once and never freed,
+// blocks are recycled per power-of-two size class.
+class PinnedPool {
+ public:
+  void* get(size_t bytes) {
+    const size_t cls = size_class(bytes);
+    std::lock_guard<std::mutex> lk(mu_);
+    std::vector<void*>& fl = free_[cls];
+    if (!fl.empty()) {
+      void* p = fl.back();
+      fl.pop_back();
+      return p;
+    }
+    if (cls > left_) {
+      const size_t slab = std::max<size_t>(size_t(1) << 20, cls);
+      void* m = nullptr;
+      if (cudaMallocHost(&m, slab) != cudaSuccess) return nullptr;
+      cur_ = static_cast<char*>(m);
+      left_ = slab;
+    }
+    void* p = cur_;
+    cur_ += cls;
+    left_ -= cls;
+    return p;
+  }
+  void put(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu_);
+    free_[size_class(bytes)].push_back(p);
+  }
+
+ private:
+  static size_t size_class(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c <<= 1;
+    return c;
+  }
+  std::mutex mu_;
+  std::map<size_t, std::vector<void*>> free_;
+  char* cur_ = nullptr;
+  size_t left_ = 0;
+};
+static PinnedPool& pinned_pool() {
+  static PinnedPool* p = new PinnedPool();   // outlives every handle (never destroyed)
+  return *p;
+}
+
+// Device memory of the handles comes from one memory pool per device that
+// keeps what is freed (release threshold at its maximum) while any handle or
+// server is alive, and gives it back when the last one goes.  The default pool
+// returns unused memory to the driver at every synchronisation, so each new
+// request of a serving loop would map its buffers afresh.
+struct DevicePools {
+  std::mutex mu;
+  std::map<int, cudaMemPool_t> pool;
+  int live = 0;   // handles + servers
+};
+static DevicePools& device_pools() {
+  static DevicePools* p = new DevicePools();
+  return *p;
+}
+cudaError_t handle_pool(int dev, cudaMemPool_t* out) {
+  DevicePools& d = device_pools();
+  std::lock_guard<std::mutex> lk(d.mu);
+  auto it = d.pool.find(dev);
+  if (it != d.pool.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = cudaMemPoolCreate(&pool, &props);
+  if (e != cudaSuccess) return e;
+  uint64_t keep = ~uint64_t(0);
+  e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e != cudaSuccess) {
+    cudaMemPoolDestroy(pool);
+    return e;
+  }
+  d.pool[dev] = pool;
+  *out = pool;
+  return cudaSuccess;
+}
+void pools_acquire() {
+  DevicePools& d = device_pools();
+  std::lock_guard<std::mutex> lk(d.mu);
+  d.live += 1;
+}
+void pools_release() {
+  DevicePools& d = device_pools();
+  std::lock_guard<std::mutex> lk(d.mu);
+  if (--d.live == 0)
+    for (auto& kv : d.pool) cudaMemPoolTrimTo(kv.second, 0);
+}
 
 bool mq_supported(int M, int Q) {
 #define RF_MQ_CASE(MM, QQ) \
@@ -205,6 +305,7 @@ struct rf_handle {
   std::vector<void*> allocations;
 
   bool dry = false;          // count bytes only (rf_device_bytes_estimate)
+  bool pooled = false;       // counted in the device pools' live handles
   // Stream-ordered allocations: creating or destroying a handle does not
   // synchronise the device, so handles of a serving loop come and go without
   // stalling the others.
@@ -222,7 +323,9 @@ struct rf_handle {
       set_last_error_str("device allocation failed (injected)");
       return RF_E_OOM;
     }
-    cudaError_t e = cudaMallocAsync(p, bytes, st);
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = handle_pool(dev, &pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, st);
     if (e != cudaSuccess) {
       *p = nullptr;
       set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -244,11 +347,13 @@ struct rf_handle {
     for (auto e : mv_events) cudaEventDestroy(e);
     for (void* p : allocations) cudaFreeAsync(p, st);
     if (st) cudaStreamSynchronize(st);
-    if (host_ctl) cudaFreeHost(host_ctl);
-    if (host_bctl) cudaFreeHost(host_bctl);
-    if (host_ir_norm) cudaFreeHost(host_ir_norm);
-    if (lu.host_ipiv) cudaFreeHost(lu.host_ipiv);
-    if (lu.host_perm) cudaFreeHost(lu.host_perm);
+    PinnedPool& pp = pinned_pool();
+    pp.put(host_ctl, sizeof(GmresCtl));
+    pp.put(host_bctl, sizeof(BicgCtl));
+    pp.put(host_ir_norm, sizeof(double));
+    pp.put(lu.host_ipiv, (size_t)lu.R * sizeof(int));
+    pp.put(lu.host_perm, (size_t)lu.R * sizeof(int));
+    if (pooled) pools_release();
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (order_ev) cudaEventDestroy(order_ev);
@@ -441,7 +546,7 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   if (!rc) rc = h->alloc((void**)&h->sn, (size_t)m * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->g, (size_t)(m + 1) * sizeof(double));
   if (!rc) rc = h->alloc((void**)&h->ctl, sizeof(GmresCtl));
-  if (!rc && !h->dry && cudaMallocHost((void**)&h->host_ctl, sizeof(GmresCtl)) != cudaSuccess) rc = RF_E_OOM;
+  if (!rc && !h->dry && !(h->host_ctl = static_cast<GmresCtl*>(pinned_pool().get(sizeof(GmresCtl))))) rc = RF_E_OOM;
   if (cfg->solver == RF_SOLVER_DIRECT) {
     LuSetup& L = h->lu;
     L.R = R;
@@ -466,16 +571,16 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     if (!rc) rc = h->alloc((void**)&L.inv, (size_t)lu_tc_inv_floats() * sizeof(float));
     if (!rc) rc = h->alloc((void**)&L.flags, 2 * sizeof(int));
     if (!rc) rc = h->alloc((void**)&L.sinv, (size_t)lu_tc_sinv_floats(R) * sizeof(float));
-    if (!rc && !h->dry && cudaMallocHost((void**)&L.host_ipiv, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
-    if (!rc && !h->dry && cudaMallocHost((void**)&L.host_perm, (size_t)R * sizeof(int)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && !h->dry && !(L.host_ipiv = static_cast<int*>(pinned_pool().get((size_t)R * sizeof(int))))) rc = RF_E_OOM;
+    if (!rc && !h->dry && !(L.host_perm = static_cast<int*>(pinned_pool().get((size_t)R * sizeof(int))))) rc = RF_E_OOM;
   }
   if (cfg->solver == RF_SOLVER_BICGSTAB) {
     if (!rc) rc = h->alloc((void**)&h->bicg_work, (size_t)6 * (size_t)ldv * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->bctl, sizeof(BicgCtl));
-    if (!rc && !h->dry && cudaMallocHost((void**)&h->host_bctl, sizeof(BicgCtl)) != cudaSuccess) rc = RF_E_OOM;
+    if (!rc && !h->dry && !(h->host_bctl = static_cast<BicgCtl*>(pinned_pool().get(sizeof(BicgCtl))))) rc = RF_E_OOM;
     if (h->mixed) {
       if (!rc) rc = h->alloc((void**)&h->ir_norm, sizeof(double));
-      if (!rc && !h->dry && cudaMallocHost((void**)&h->host_ir_norm, sizeof(double)) != cudaSuccess) rc = RF_E_OOM;
+      if (!rc && !h->dry && !(h->host_ir_norm = static_cast<double*>(pinned_pool().get(sizeof(double))))) rc = RF_E_OOM;
     }
   }
   // velocities
@@ -523,6 +628,8 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (e != cudaSuccess) { set_last_error(cudaGetErrorString(e), __FILE__, __LINE__); return fail(RF_E_CUDA); }
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev);
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) return fail(RF_E_CUDA);
+  pools_acquire();
+  h->pooled = true;
   for (auto& ev : h->ev)
     if (cudaEventCreate(&ev) != cudaSuccess) return fail(RF_E_CUDA);
   int rc = allocate_buffers(h, cfg);
@@ -994,64 +1101,107 @@ int rf_step(rf_handle* h, int t) {
   return rc;
 }
 
-// ---- packed solves of many small suspensions ------------------------------
+// ---- packed solves and steps of many small suspensions --------------------
+// The conditions of the packed solve (k_pack_gmres_ir): mixed precision,
+// GMRES, M = 5, Q = 24, at most kPackMaxFibers fibers, one restart length.
+static int pack_check(rf_handle** hs, int n, bool need_assembled, const char* who, int* m_out, int* Rmax_out) {
+  int m = -1, Rmax = 0;
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    if (!h) return RF_E_INPUT;
+    if (need_assembled && !h->assembled) {
+      set_last_error_str((std::string(who) + " before rf_assemble").c_str());
+      return RF_E_STATE;
+    }
+    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers) {
+      set_last_error_str(
+          (std::string(who) + ": mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 128 fibers").c_str());
+      return RF_E_UNSUPPORTED;
+    }
+    if (m >= 0 && h->restart != m) {
+      set_last_error_str((std::string(who) + ": one restart length per pack").c_str());
+      return RF_E_INPUT;
+    }
+    m = h->restart;
+    Rmax = std::max<int>(Rmax, (int)h->R);
+  }
+  *m_out = m;
+  *Rmax_out = Rmax;
+  return RF_OK;
+}
+
+// every member's earlier work on its own stream before the pack's launches on st
+static int pack_order_streams(rf_handle** hs, int n, cudaStream_t st) {
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    if (h->st == st) continue;
+    if (!h->order_ev) RF_CUDA_TRY(cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming));
+    RF_CUDA_TRY(cudaEventRecord(h->order_ev, h->st));
+    RF_CUDA_TRY(cudaStreamWaitEvent(st, h->order_ev, 0));
+  }
+  return RF_OK;
+}
+
+// the packed solve's descriptor of h (out: 4 ints, relres: 1 double, on the device)
+static void pack_member(rf_handle* h, int* out, double* relres, PackMember* q) {
+  std::memset(q, 0, sizeof(*q));
+  q->N = h->N;
+  q->smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+  q->maxit = h->cfg.gmres_max_iterations;
+  q->tol = h->cfg.refinement_tolerance;
+  q->S16 = h->S16;
+  q->S32 = h->S32;
+  q->ori = h->ori32;
+  q->b = h->b;
+  q->x64 = h->x64;
+  q->x = h->x;
+  q->V = h->V;
+  q->ldv = ceil_div(h->R, 32) * 32;
+  q->out = out;
+  q->relres = relres;
+  for (int k = 0; k < 5; ++k) {
+    q->coef[k] = h->tab.gamma[k];
+    q->eig[k] = h->tab.eigen[k];
+  }
+}
+
+// a member's solve outcome (o: its 4 output ints) into its handle
+static int pack_record_solve(rf_handle* h, const int* o, double relres) {
+  h->matvecs_done = o[0];
+  h->mv_used = 0;   // no per-launch matvec windows: the matvecs ran inside the packed kernel
+  h->refinements = o[2];
+  h->stats.iterations = o[0];
+  h->stats.restarts = o[1];
+  h->stats.refinement_steps = o[2];
+  h->stats.relative_residual = relres;
+  h->stats.graph_replays = 0;
+  h->pack_status = o[3] == 0 ? RF_OK : (o[3] == 1 ? RF_E_NOCONV : RF_E_NAN);
+  if (h->pack_status != RF_E_NAN) h->solved = true;
+  return h->pack_status;
+}
+
 // One launch solves every handle's assembled system (k_pack_gmres_ir: one CTA
 // per suspension, the rf_solve algorithm for the mixed modes); each handle's
 // result depends only on its own data.
 int rf_solve_packed(rf_handle** hs, int n) {
   if (!hs || n < 1) return RF_E_INPUT;
-  int m = -1, Rmax = 0;
-  for (int i = 0; i < n; ++i) {
-    rf_handle* h = hs[i];
-    if (!h) return RF_E_INPUT;
-    if (!h->assembled) { set_last_error_str("rf_solve_packed before rf_assemble"); return RF_E_STATE; }
-    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers) {
-      set_last_error_str("rf_solve_packed: mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 128 fibers");
-      return RF_E_UNSUPPORTED;
-    }
-    if (m >= 0 && h->restart != m) { set_last_error_str("rf_solve_packed: one restart length per pack"); return RF_E_INPUT; }
-    m = h->restart;
-    Rmax = std::max<int>(Rmax, (int)h->R);
-  }
+  int m = 0, Rmax = 0;
+  RF_TRY(pack_check(hs, n, true, "rf_solve_packed", &m, &Rmax));
   rf_handle* h0 = hs[0];
   cudaStream_t st = h0->st;
-  // every member's assembly (on its own stream) before the packed launch
-  for (int i = 1; i < n; ++i) {
-    rf_handle* h = hs[i];
-    if (!h->order_ev) RF_CUDA_TRY(cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming));
-    RF_CUDA_TRY(cudaEventRecord(h->order_ev, h->st));
-    RF_CUDA_TRY(cudaStreamWaitEvent(st, h->order_ev, 0));
-  }
+  RF_TRY(pack_order_streams(hs, n, st));
   const size_t bm = (size_t)n * sizeof(PackMember), bo = (size_t)n * 4 * sizeof(int), br = (size_t)n * sizeof(double);
   unsigned char* dbuf = nullptr;
-  RF_CUDA_TRY(cudaMallocAsync((void**)&dbuf, bm + bo + br, st));
+  cudaMemPool_t pool = nullptr;
+  RF_CUDA_TRY(handle_pool(h0->dev, &pool));
+  RF_CUDA_TRY(cudaMallocFromPoolAsync((void**)&dbuf, bm + bo + br, pool, st));
   PackMember* dm = reinterpret_cast<PackMember*>(dbuf);
   double* drel = reinterpret_cast<double*>(dbuf + bm);
   int* dout = reinterpret_cast<int*>(dbuf + bm + br);
   std::vector<PackMember> pm((size_t)n);
   for (int i = 0; i < n; ++i) {
-    rf_handle* h = hs[i];
-    PackMember& q = pm[(size_t)i];
-    std::memset(&q, 0, sizeof(q));
-    q.N = h->N;
-    q.smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
-    q.maxit = h->cfg.gmres_max_iterations;
-    q.tol = h->cfg.refinement_tolerance;
-    q.S16 = h->S16;
-    q.S32 = h->S32;
-    q.ori = h->ori32;
-    q.b = h->b;
-    q.x64 = h->x64;
-    q.x = h->x;
-    q.V = h->V;
-    q.ldv = ceil_div(h->R, 32) * 32;
-    q.out = dout + 4 * i;
-    q.relres = drel + i;
-    for (int k = 0; k < 5; ++k) {
-      q.coef[k] = h->tab.gamma[k];
-      q.eig[k] = h->tab.eigen[k];
-    }
-    RF_CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    pack_member(hs[i], dout + 4 * i, drel + i, &pm[(size_t)i]);
+    RF_CUDA_TRY(cudaEventRecord(hs[i]->ev[2], st));
   }
   RF_CUDA_TRY(cudaMemcpyAsync(dm, pm.data(), bm, cudaMemcpyHostToDevice, st));
   int rc = launch_pack_gmres_ir(dm, n, Rmax, m, st);
@@ -1069,94 +1219,175 @@ int rf_solve_packed(rf_handle** hs, int n) {
   int worst = RF_OK;
   for (int i = 0; i < n; ++i) {
     rf_handle* h = hs[i];
-    const int* o = &out[(size_t)i * 4];
     h->launches += (i == 0) ? 1 : 0;
-    h->matvecs_done = o[0];
-    h->mv_used = 0;   // no per-launch matvec windows: the matvecs ran inside the packed kernel
-    h->refinements = o[2];
-    h->stats.iterations = o[0];
-    h->stats.restarts = o[1];
-    h->stats.refinement_steps = o[2];
-    h->stats.relative_residual = rel[(size_t)i];
-    h->stats.graph_replays = 0;
-    h->pack_status = o[3] == 0 ? RF_OK : (o[3] == 1 ? RF_E_NOCONV : RF_E_NAN);
-    if (h->pack_status != RF_E_NAN) h->solved = true;
-    if (h->pack_status == RF_E_NAN) worst = RF_E_NAN;
-    else if (h->pack_status == RF_E_NOCONV && worst == RF_OK) worst = RF_E_NOCONV;
+    const int s = pack_record_solve(h, &out[(size_t)i * 4], rel[(size_t)i]);
+    if (s == RF_E_NAN) worst = RF_E_NAN;
+    else if (s == RF_E_NOCONV && worst == RF_OK) worst = RF_E_NOCONV;
   }
   return worst;
 }
 
-// fn(i) for i < n from up to 8 host threads (members of a pack are
-// independent: each one's launches go to its own stream)
-static void for_members(int n, const std::function<void(int)>& fn) {
-  const int nt = std::min(8, std::max(1, n / 8));
-  if (nt == 1) {
-    for (int i = 0; i < n; ++i) fn(i);
-    return;
-  }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::vector<std::thread> th;
-  for (int k = 0; k < nt; ++k)
-    th.emplace_back([&, k] {
-      cudaSetDevice(dev);
-      for (int i = k; i < n; i += nt) fn(i);
-    });
-  for (auto& x : th) x.join();
-}
-
+// A whole time step of every member as one launch sequence on the first
+// member's stream: per group of members with the same Tables and storage,
+// the packed assembly (k_pack_assemble, k_pack_force_terms); the packed solve
+// of all members; per group the packed velocities and update (k_pack_velocity,
+// k_pack_finish).  One upload of the descriptors, one download of the
+// outcomes, one synchronisation.  A member whose solve ends non-finite keeps
+// its state; one whose velocities are not finite has taken the step and
+// reports RF_E_NAN (as rf_step's stages do).
 int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   if (!hs || !timesteps || !status || n < 1) return RF_E_INPUT;
   for (int i = 0; i < n; ++i) {
     if (!hs[i]) return RF_E_INPUT;
-    hs[i]->launches = 0;
     status[i] = RF_OK;
+  }
+  int m = 0, Rmax = 0;
+  const int chk = pack_check(hs, n, false, "rf_step_packed", &m, &Rmax);
+  if (chk != RF_OK) {
+    for (int i = 0; i < n; ++i) status[i] = chk;
+    return chk;
   }
   nvtxRangePushA("rf_step_packed");
   struct Pop {
     ~Pop() { nvtxRangePop(); }
   } pop;
-  // each member's assembly, velocities and update run on its own stream (so
-  // they overlap on the device), issued from several host threads; the solve
-  // is the one shared launch.  Members whose assembly fails keep that status
-  // and sit out this step.
-  for_members(n, [&](int i) { status[i] = rf_assemble(hs[i]); });
-  std::vector<rf_handle*> ok;
-  for (int i = 0; i < n; ++i)
-    if (status[i] == RF_OK) ok.push_back(hs[i]);
-  if (!ok.empty()) {
-    const int rc = rf_solve_packed(ok.data(), (int)ok.size());
-    if (rc != RF_OK && rc != RF_E_NOCONV && rc != RF_E_NAN) {
-      for (int i = 0; i < n; ++i)
-        if (status[i] == RF_OK) status[i] = rc;
-      return rc;
+  rf_handle* h0 = hs[0];
+  cudaStream_t st = h0->st;
+  RF_TRY(pack_order_streams(hs, n, st));
+
+  // groups: members with the same Tables (slenderness) and 16-bit format
+  std::vector<int> order;
+  std::vector<int> gbeg;   // group g: order[gbeg[g] .. gbeg[g+1])
+  {
+    std::vector<bool> taken((size_t)n, false);
+    for (int i = 0; i < n; ++i) {
+      if (taken[(size_t)i]) continue;
+      gbeg.push_back((int)order.size());
+      for (int j = i; j < n; ++j) {
+        if (taken[(size_t)j] || hs[j]->cfg.precision != hs[i]->cfg.precision ||
+            std::memcmp(&hs[j]->tab, &hs[i]->tab, sizeof(Tables)) != 0)
+          continue;
+        taken[(size_t)j] = true;
+        order.push_back(j);
+      }
+    }
+    gbeg.push_back(n);
+  }
+  const int ngroups = (int)gbeg.size() - 1;
+
+  // device block: [PackMember n][PackStepMember n][relres n][out 4n][vbad n]
+  const size_t bm = (size_t)n * sizeof(PackMember), bs = (size_t)n * sizeof(PackStepMember);
+  const size_t br = (size_t)n * sizeof(double), bo = (size_t)n * 5 * sizeof(int);
+  unsigned char* dbuf = nullptr;
+  cudaMemPool_t pool = nullptr;
+  RF_CUDA_TRY(handle_pool(h0->dev, &pool));
+  RF_CUDA_TRY(cudaMallocFromPoolAsync((void**)&dbuf, bm + bs + br + bo, pool, st));
+  PackMember* dpm = reinterpret_cast<PackMember*>(dbuf);
+  PackStepMember* dsm = reinterpret_cast<PackStepMember*>(dbuf + bm);
+  double* drel = reinterpret_cast<double*>(dbuf + bm + bs);
+  int* dout = reinterpret_cast<int*>(dbuf + bm + bs + br);
+  int* dvbad = dout + 4 * n;
+  std::vector<unsigned char> host(bm + bs);
+  PackMember* pm = reinterpret_cast<PackMember*>(host.data());
+  PackStepMember* sm = reinterpret_cast<PackStepMember*>(host.data() + bm);
+  std::vector<int64_t> asm_blocks((size_t)ngroups, 0), vel_blocks((size_t)ngroups, 0);
+  for (int g = 0; g < ngroups; ++g) {
+    for (int k = gbeg[g]; k < gbeg[g + 1]; ++k) {
+      const int i = order[(size_t)k];
+      rf_handle* h = hs[i];
+      pack_member(h, dout + 4 * i, drel + i, &pm[i]);
+      PackStepMember& q = sm[k];
+      std::memset(&q, 0, sizeof(q));
+      q.N = h->N;
+      q.first = timesteps[i] == 0 ? 1 : 0;
+      q.asm_start = (int)asm_blocks[(size_t)g];
+      q.vel_start = (int)vel_blocks[(size_t)g];
+      const int64_t T = ceil_div(h->N, 8);
+      asm_blocks[(size_t)g] += T * (T + 1) / 2;
+      vel_blocks[(size_t)g] += struct_store_tiles(h->N);
+      q.dt = h->cfg.timestep;
+      q.solve_status = dout + 4 * i + 3;
+      q.vbad = dvbad + i;
+      q.pos64 = h->pos64[h->icur];
+      q.pos64_prev = h->pos64[h->iprev];
+      q.ori64 = h->ori64[h->icur];
+      q.ori64_prev = h->ori64[h->iprev];
+      q.pos32 = h->pos32;
+      q.ori32 = h->ori32;
+      q.tv = h->tv[h->vcur];
+      q.tv_prev = h->tv[h->vprev];
+      q.rv = h->rv[h->vcur];
+      q.rv_prev = h->rv[h->vprev];
+      q.S32 = h->S32;
+      q.S16 = h->S16;
+      q.ffpart = h->ffpart;
+      q.F = h->F;
+      q.b = h->b;
+      q.x = h->x;
+      q.vpart = h->svpart;
     }
   }
-  auto finish = [&](int i) -> int {
-    rf_handle* h = hs[i];
-    if (status[i] != RF_OK) return status[i];
-    if (h->pack_status == RF_E_NAN) return RF_E_NAN;
-    RF_TRY(rf_update_velocities(h));
-    RF_TRY(rf_update_fibers(h, timesteps[i] == 0));
-    int vbad = 0;
-    RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
-    if (vbad) {
-      set_last_error_str("non-finite velocity");
-      return RF_E_NAN;
-    }
-    h->stats.ms_assemble_system = elapsed(h->ev[0], h->ev[1]);
-    h->stats.ms_solve_system = elapsed(h->ev[2], h->ev[3]);
-    h->stats.ms_update_velocities = elapsed(h->ev[4], h->ev[5]);
-    h->stats.ms_update_fibers = elapsed(h->ev[6], h->ev[7]);
-    h->stats.kernel_launches = h->launches;
-    return h->pack_status;
-  };
-  for_members(n, [&](int i) { status[i] = finish(i); });
+  cudaEvent_t* ev = h0->ev;
+  int launches = 1;
+  RF_CUDA_TRY(cudaEventRecord(ev[0], st));
+  RF_CUDA_TRY(cudaMemcpyAsync(dbuf, host.data(), bm + bs, cudaMemcpyHostToDevice, st));
+  int rc = RF_OK;
+  for (int g = 0; g < ngroups && rc == RF_OK; ++g) {
+    rf_handle* hg = hs[order[(size_t)gbeg[g]]];
+    rc = launch_pack_assemble(hg->tab, dsm + gbeg[g], gbeg[g + 1] - gbeg[g], asm_blocks[(size_t)g],
+                              hg->cfg.precision == RF_PREC_MIXED_BF16, st);
+    launches += 2;
+  }
+  RF_CUDA_TRY(cudaEventRecord(ev[1], st));
+  if (rc == RF_OK) rc = launch_pack_gmres_ir(dpm, n, Rmax, m, st);
+  RF_CUDA_TRY(cudaEventRecord(ev[3], st));
+  for (int g = 0; g < ngroups && rc == RF_OK; ++g) {
+    rf_handle* hg = hs[order[(size_t)gbeg[g]]];
+    rc = launch_pack_velocity_update(hg->tab, dsm + gbeg[g], gbeg[g + 1] - gbeg[g], vel_blocks[(size_t)g], st);
+    launches += 2;
+  }
+  RF_CUDA_TRY(cudaEventRecord(ev[5], st));
+  std::vector<unsigned char> res(br + bo);
+  if (rc == RF_OK) RF_CUDA_TRY(cudaMemcpyAsync(res.data(), drel, br + bo, cudaMemcpyDeviceToHost, st));
+  RF_CUDA_TRY(cudaFreeAsync(dbuf, st));
+  RF_CUDA_TRY(cudaStreamSynchronize(st));
+  if (rc != RF_OK) {
+    for (int i = 0; i < n; ++i) status[i] = rc;
+    return rc;
+  }
+  const double* rel = reinterpret_cast<const double*>(res.data());
+  const int* out = reinterpret_cast<const int*>(res.data() + br);
+  const int* vbad = out + 4 * n;
+  const float ms_asm = elapsed(ev[0], ev[1]), ms_solve = elapsed(ev[1], ev[3]), ms_vel = elapsed(ev[3], ev[5]);
   int worst = RF_OK;
-  for (int i = 0; i < n; ++i)
-    if (status[i] != RF_OK && status[i] != RF_E_NOCONV && worst == RF_OK) worst = status[i];
+  for (int i = 0; i < n; ++i) {
+    rf_handle* h = hs[i];
+    h->launches = i == 0 ? launches : 0;
+    h->assembled = true;
+    h->solved = false;
+    int s = pack_record_solve(h, &out[(size_t)i * 4], rel[i]);
+    if (s != RF_E_NAN) {
+      // velocities computed, state rotated in place (as rf_update_velocities + rf_update_fibers)
+      h->vlast = h->vcur;
+      h->vel_fresh = false;
+      h->assembled = h->solved = false;
+      h->steps_taken += 1;
+      if (vbad[i]) {
+        set_last_error_str("non-finite velocity");
+        s = RF_E_NAN;
+      }
+    }
+    // stage times are the pack's: its assembly, its solve, and its velocities
+    // with the update fused into their last kernel
+    h->stats.ms_assemble_system = ms_asm;
+    h->stats.ms_solve_system = ms_solve;
+    h->stats.ms_update_velocities = ms_vel;
+    h->stats.ms_update_fibers = 0.0;
+    h->stats.ms_step = ms_asm + ms_solve + ms_vel;
+    h->stats.kernel_launches = h->launches;
+    status[i] = s;
+    if (s != RF_OK && s != RF_E_NOCONV && worst == RF_OK) worst = s;
+  }
   return worst;
 }
 

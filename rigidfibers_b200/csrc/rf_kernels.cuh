@@ -86,9 +86,53 @@ struct PackMember {
 size_t pack_smem_bytes(int Rmax, int m);
 int launch_pack_gmres_ir(const PackMember* members, int n, int Rmax, int m, cudaStream_t st);
 
+// One suspension of a packed step: the buffers its assembly, velocities and
+// update read and write.  The packed stage kernels launch once per group of
+// members with the same Tables (slenderness); within a group, member m owns
+// blocks [asm_start, asm_start + its tile pairs) of the assembly grid and
+// [vel_start, ...) of the velocity grid.
+struct PackStepMember {
+  int N, first;               // fibers; 1 on a first (Euler) step
+  int asm_start, vel_start;   // first block of the member in the group's grids
+  double dt;
+  const int* solve_status;    // the packed solve's status word (2: non-finite, the member sits out)
+  int* vbad;                  // set to 1 when a velocity is not finite, else 0
+  double4 *pos64, *pos64_prev, *ori64, *ori64_prev;   // FP64 state: current, previous
+  float4 *pos32, *ori32;      // FP32 copies of the current state
+  float4 *tv, *tv_prev, *rv, *rv_prev;                 // velocities: current, previous
+  float* S32;
+  uint32_t* S16;
+  float *ffpart, *F, *b;      // assembly scratch, force terms, right-hand side
+  const float* x;             // the solve's FP32 solution
+  float* vpart;               // velocity partials
+};
+// The member of a packed group that owns block L of a grid whose members'
+// first blocks (ascending) are starts(m): the last member with starts(m) <= L.
+template <class StartOf>
+__device__ __forceinline__ int pack_member_of(int n, int L, StartOf starts) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (starts(mid) <= L) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// numerical structured assembly + force terms of every member of one group
+int launch_pack_assemble(const Tables& tab, const PackStepMember* members, int n, int64_t blocks, bool bf16,
+                         cudaStream_t st);
+// velocities, the non-finite guard and the fiber update of every member of one group
+int launch_pack_velocity_update(const Tables& tab, const PackStepMember* members, int n, int64_t blocks,
+                                cudaStream_t st);
+
 }  // namespace rf
 
 namespace rf {
+// The handles' device memory pool of device dev (csrc/rf_capi.cu), and the
+// count of its users (handles and servers) that keeps freed memory in it.
+cudaError_t handle_pool(int dev, cudaMemPool_t* out);
+void pools_acquire();
+void pools_release();
 int velocity_chunks(int N);
 // fw: N*Q float4 scratch; vpart: velocity_chunks(N) * N * 6 floats scratch.
 int launch_check_finite(const float4* a, const float4* b, int N, int* flag, cudaStream_t st);
@@ -99,6 +143,49 @@ int launch_velocity_numerical(const Tables& tab, int N, const double4* pos64, co
 int launch_velocity_analytical(const Tables& tab, int N, const float4* ori, const double4* pos64,
                                const double4* ori64, const float* x, float* vpart, float4* tvel, float4* rvel,
                                cudaStream_t st);
+// Fiber i's second-order step (fortran/update_fibers.incl; the first step,
+// fortran/update_fibers_firststep.incl, is explicit Euler):
+// x' = 4/3 x - 1/3 x_prev + 2/3 dt (2 U - U_prev), the same for t with W, then
+// t' normalised.  Writes the rotated state: prev <- current, current <- new.
+// Every rounding is explicit (fma, __dmul_rn), so kernels that inline this
+// agree bit for bit whatever the compiler would contract.
+__device__ __forceinline__ double bdf2_coord(double c43, double c13, double c23, double xc, double xp, float u,
+                                             float up) {
+  return fma(c23, fma(2.0, (double)u, -(double)up), fma(c43, xc, __dmul_rn(-c13, xp)));
+}
+__device__ __forceinline__ void update_fiber(int i, int first, double dt, double4* __restrict__ prev_pos,
+                                             double4* __restrict__ cur_pos, double4* __restrict__ prev_ori,
+                                             double4* __restrict__ cur_ori, float4* __restrict__ prev_tv,
+                                             float4 u, float4* __restrict__ prev_rv, float4 w,
+                                             float4* __restrict__ pos32, float4* __restrict__ ori32) {
+  const double4 xc = cur_pos[i], tc = cur_ori[i];
+  double4 xn, tn;
+  if (first) {
+    xn = make_double4(fma(dt, (double)u.x, xc.x), fma(dt, (double)u.y, xc.y), fma(dt, (double)u.z, xc.z), 0.0);
+    tn = make_double4(fma(dt, (double)w.x, tc.x), fma(dt, (double)w.y, tc.y), fma(dt, (double)w.z, tc.z), 0.0);
+  } else {
+    const double4 xp = prev_pos[i], tp = prev_ori[i];
+    const float4 up = prev_tv[i], wp = prev_rv[i];
+    const double c43 = 4.0 / 3.0, c13 = 1.0 / 3.0, c23 = (2.0 / 3.0) * dt;
+    xn = make_double4(bdf2_coord(c43, c13, c23, xc.x, xp.x, u.x, up.x), bdf2_coord(c43, c13, c23, xc.y, xp.y, u.y, up.y),
+                      bdf2_coord(c43, c13, c23, xc.z, xp.z, u.z, up.z), 0.0);
+    tn = make_double4(bdf2_coord(c43, c13, c23, tc.x, tp.x, w.x, wp.x), bdf2_coord(c43, c13, c23, tc.y, tp.y, w.y, wp.y),
+                      bdf2_coord(c43, c13, c23, tc.z, tp.z, w.z, wp.z), 0.0);
+  }
+  const double inv = 1.0 / sqrt(fma(tn.z, tn.z, fma(tn.y, tn.y, __dmul_rn(tn.x, tn.x))));
+  tn.x = __dmul_rn(tn.x, inv);
+  tn.y = __dmul_rn(tn.y, inv);
+  tn.z = __dmul_rn(tn.z, inv);
+  prev_pos[i] = xc;
+  prev_ori[i] = tc;
+  cur_pos[i] = xn;
+  cur_ori[i] = tn;
+  prev_tv[i] = u;
+  prev_rv[i] = w;
+  pos32[i] = make_float4((float)xn.x, (float)xn.y, (float)xn.z, 0.f);
+  ori32[i] = make_float4((float)tn.x, (float)tn.y, (float)tn.z, 0.f);
+}
+
 // The second-order (or first-step Euler) update; rotates the state in place:
 // prev <- cur, cur <- new, previous velocities <- current ones.  halt (may be
 // null): a device word that, when set, leaves the state untouched.

@@ -888,7 +888,7 @@ int lu_time_panel(const LuSetup& s, const float* A, int blocks, cudaStream_t st,
 // step, after the first two), the matrix is factored again with the split
 // 3xTF32 update and refined from the start.
 int lu_factor_solve(const LuSetup& s, const float* A, const float* b, float* x, cudaStream_t st, LuResult* res) {
-  const int64_t R = s.R, lda = s.lda, ldlu = s.ldlu ? s.ldlu : s.lda;
+  const int64_t R = s.R, ldlu = s.ldlu ? s.ldlu : s.lda;
   bool pivoted = false;
   float max_l = 0.f;
   const unsigned eb = (unsigned)std::min<int64_t>(ceil_div(R, 256), 4096);

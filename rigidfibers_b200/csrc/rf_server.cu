@@ -85,6 +85,8 @@ struct rf_server {
   int packed_active = 0;
   std::thread pack_worker;
   std::vector<double> all_step_ms;
+  std::vector<double> pack_ms;          // wall time of each rf_step_packed call
+  int64_t pack_member_steps = 0;        // suspensions stepped by those calls
   int64_t fiber_steps = 0;
   double t0 = 0, t_last = 0;
 };
@@ -236,6 +238,11 @@ static void pack_loop(rf_server* s) {
         const auto t0 = Clock::now();
         rf_step_packed(hs.data(), ts.data(), (int)nb, st.data());
         const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        {
+          std::lock_guard<std::mutex> lk(s->mu);
+          s->pack_ms.push_back(ms);
+          s->pack_member_steps += (int64_t)nb;
+        }
         for (size_t q = 0; q < nb; ++q) {
           Member& mm = mem[g.second[a + q]];
           if (st[q] == RF_OK || st[q] == RF_E_NOCONV) {
@@ -330,6 +337,7 @@ int rf_server_create(const rf_server_config* cfg, rf_server** out) {
   rf_server* s = new rf_server();
   s->cfg = *cfg;
   cudaGetDevice(&s->device);
+  rf::pools_acquire();   // requests' memory stays in the handles' pool between requests
   s->t0 = now_s();
   s->dispatcher = std::thread(dispatch_loop, s);
   if (cfg->pack_max_fibers > 0) s->pack_worker = std::thread(pack_loop, s);
@@ -461,6 +469,16 @@ int rf_server_get_stats(rf_server* s, rf_server_stats* out) {
   out->failed = failed;
   out->queued = queued;
   out->active = s->active + s->packed_active;
+  std::vector<double> pk = s->pack_ms;
+  std::sort(pk.begin(), pk.end());
+  out->pack_steps = (int64_t)pk.size();
+  if (!pk.empty()) {
+    auto pq = [&](double p) { return pk[(size_t)std::min<double>(pk.size() - 1, std::ceil(p * pk.size()) - 1)]; };
+    out->pack_p50_ms = pq(0.50);
+    out->pack_p99_ms = pq(0.99);
+    out->pack_max_ms = pk.back();
+    out->pack_mean_members = (double)s->pack_member_steps / (double)pk.size();
+  }
   return RF_OK;
 }
 
@@ -483,6 +501,7 @@ int rf_server_destroy(rf_server* s) {
   for (auto& t : s->finished_workers)
     if (t.joinable()) t.join();
   delete s;
+  rf::pools_release();
   return RF_OK;
 }
 

@@ -828,16 +828,19 @@ __global__ void k_struct_finalize(const Tables tab, int N, const float4* __restr
 // Velocity partials from the FP32 blocks:
 //   u_i += sum_kJ T^{ij}[P0][kJ+1] x_{j,kJ},  w_i += sum_kJ T^{ij}[P1][kJ+1] x_{j,kJ}
 //   u_j += sum_kI T^{ij}[kI+1][P0] x_{i,kI},  w_j += sum_kI T^{ij}[kI+1][P1] x_{i,kI}
+// (storage tile L of one suspension: the body of k_struct_velocity and of the
+// packed velocities)
 template <int M, int TI>
-__global__ void __launch_bounds__(256)
-k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict__ x, float* __restrict__ vpart) {
+__device__ __forceinline__ void struct_velocity_tile(int N, const float* __restrict__ S32,
+                                                     const float* __restrict__ x, float* __restrict__ vpart,
+                                                     unsigned L) {
   constexpr int K1 = M + 1, M3 = 3 * M;
   constexpr int NQ32 = K1 * K1 * 6;
   constexpr int SUB = kStoreTile / TI;
   __shared__ float sx[2][kStoreTile][M3];
   __shared__ float sz[2][kStoreTile][kStoreTile][7];
   int I16, J16;
-  tile_pair16(blockIdx.x, I16, J16);
+  tile_pair16(L, I16, J16);
   const bool diag = I16 == J16;
   const int t = threadIdx.x;
   for (int k = t; k < 2 * kStoreTile * M3; k += blockDim.x) {
@@ -850,7 +853,7 @@ k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict_
   const int i = I16 * kStoreTile + mp.i16(), j = J16 * kStoreTile + mp.j16();
   float vi[6] = {0, 0, 0, 0, 0, 0}, vj[6] = {0, 0, 0, 0, 0, 0};
   if (i < j && j < N) {
-    const int64_t rec = ((int64_t)blockIdx.x * SUB * SUB + mp.sub) * TI + mp.jl;
+    const int64_t rec = ((int64_t)L * SUB * SUB + mp.sub) * TI + mp.jl;
     const float* p = S32 + rec * (int64_t)(NQ32 * TI) + mp.tl;
     const float* xi = sx[0][mp.i16()];
     const float* xj = sx[1][mp.j16()];
@@ -895,30 +898,94 @@ k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict_
   }
 }
 
+template <int M, int TI>
+__global__ void __launch_bounds__(256)
+k_struct_velocity(int N, const float* __restrict__ S32, const float* __restrict__ x, float* __restrict__ vpart) {
+  struct_velocity_tile<M, TI>(N, S32, x, vpart, blockIdx.x);
+}
+
 // U_i = (0.5/d) [ (d+2)F + (d-2)(t.F)t + F_i[P0] + sum u ],
-// W_i = (1.5/d) (I - t t^T) [ F_i[P1] + sum w ]
-__global__ void k_struct_velocity_finalize(const Tables tab, int N, const float4* __restrict__ ori,
-                                           const float* __restrict__ F, const float* __restrict__ vpart, int nparts,
-                                           float4* __restrict__ tvel, float4* __restrict__ rvel) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+// W_i = (1.5/d) (I - t t^T) [ F_i[P1] + sum w ]   (fiber i < N).
+// Every rounding is spelled out (fmaf, __fmul_rn, __fadd_rn), so the result
+// does not depend on which multiply-adds the compiler would contract in the
+// kernel it is inlined into: the single-suspension and packed kernels agree
+// bit for bit.
+__device__ __forceinline__ void struct_velocity_fiber(const Tables& tab, int N, const float4* __restrict__ ori,
+                                                      const float* __restrict__ F, const float* __restrict__ vpart,
+                                                      int nparts, int i, float4& tv, float4& rv) {
   const int FFn = 3 * (tab.M + 1);
   const float4 t = ori[i];
   const float d = tab.d;
   const float Fz = 2.f * tab.fz_half;
-  const float tF = t.z * Fz;
+  const float tF = __fmul_rn(t.z, Fz);
+  const float cF = __fmul_rn(d - 2.f, tF);
   const float* Fi = F + (int64_t)i * FFn;
-  float U[3] = {(d - 2.f) * tF * t.x + Fi[0], (d - 2.f) * tF * t.y + Fi[1], (d + 2.f) * Fz + (d - 2.f) * tF * t.z + Fi[2]};
+  float U[3] = {fmaf(cF, t.x, Fi[0]), fmaf(cF, t.y, Fi[1]), __fadd_rn(fmaf(cF, t.z, __fmul_rn(d + 2.f, Fz)), Fi[2])};
   float W[3] = {Fi[3], Fi[4], Fi[5]};
   for (int p = 0; p < nparts; ++p) {
     const float* v = vpart + ((int64_t)p * N + i) * 6;
     U[0] += v[0]; U[1] += v[1]; U[2] += v[2];
     W[0] += v[3]; W[1] += v[4]; W[2] += v[5];
   }
-  const float tW = t.x * W[0] + t.y * W[1] + t.z * W[2];
+  const float tW = fmaf(t.z, W[2], fmaf(t.y, W[1], __fmul_rn(t.x, W[0])));
   const float su = 0.5f / d, sr = 1.5f / d;
-  tvel[i] = make_float4(U[0] * su, U[1] * su, U[2] * su, 0.f);
-  rvel[i] = make_float4((W[0] - t.x * tW) * sr, (W[1] - t.y * tW) * sr, (W[2] - t.z * tW) * sr, 0.f);
+  tv = make_float4(__fmul_rn(U[0], su), __fmul_rn(U[1], su), __fmul_rn(U[2], su), 0.f);
+  rv = make_float4(__fmul_rn(fmaf(-t.x, tW, W[0]), sr), __fmul_rn(fmaf(-t.y, tW, W[1]), sr),
+                   __fmul_rn(fmaf(-t.z, tW, W[2]), sr), 0.f);
+}
+
+__global__ void k_struct_velocity_finalize(const Tables tab, int N, const float4* __restrict__ ori,
+                                           const float* __restrict__ F, const float* __restrict__ vpart, int nparts,
+                                           float4* __restrict__ tvel, float4* __restrict__ rvel) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  float4 tv, rv;
+  struct_velocity_fiber(tab, N, ori, F, vpart, nparts, i, tv, rv);
+  tvel[i] = tv;
+  rvel[i] = rv;
+}
+
+// ---- packed step: velocities and update of every member of one group -----
+// Members whose packed solve ended non-finite (status 2) sit out: their state
+// stays as it is.  Per member the arithmetic is the single-suspension path's
+// (k_struct_velocity, k_struct_velocity_finalize, the non-finite guard,
+// k_update_fibers), so a member's step is bit for bit the one it takes alone.
+__global__ void __launch_bounds__(256)
+k_pack_velocity(const PackStepMember* __restrict__ mem, int n) {
+  const int L = (int)blockIdx.x;
+  const PackStepMember& p = mem[pack_member_of(n, L, [&](int m) { return mem[m].vel_start; })];
+  if (*p.solve_status == 2) return;
+  struct_velocity_tile<5, 8>(p.N, p.S32, p.x, p.vpart, (unsigned)(L - p.vel_start));
+}
+
+// one block per member: velocities, the guard and the second-order update
+__global__ void __launch_bounds__(128)
+k_pack_finish(const Tables tab, const PackStepMember* __restrict__ mem) {
+  const PackStepMember& p = mem[blockIdx.x];
+  if (*p.solve_status == 2) return;
+  const int N = p.N, nparts = (N + kStoreTile - 1) / kStoreTile;
+  int bad = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    float4 u, w;
+    struct_velocity_fiber(tab, N, p.ori32, p.F, p.vpart, nparts, i, u, w);
+    p.tv[i] = u;
+    p.rv[i] = w;
+    bad |= !(isfinite(u.x) && isfinite(u.y) && isfinite(u.z) && isfinite(w.x) && isfinite(w.y) && isfinite(w.z));
+    update_fiber(i, p.first, p.dt, p.pos64_prev, p.pos64, p.ori64_prev, p.ori64, p.tv_prev, u, p.rv_prev, w,
+                 p.pos32, p.ori32);
+  }
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) *p.vbad = bad ? 1 : 0;
+}
+
+int launch_pack_velocity_update(const Tables& tab, const PackStepMember* members, int n, int64_t blocks,
+                                cudaStream_t st) {
+  if (tab.M != 5 || tab.Q != 24 || n < 1 || blocks < 1) return RF_E_UNSUPPORTED;
+  k_pack_velocity<<<(unsigned)blocks, 256, 0, st>>>(members, n);
+  RF_LAUNCH_CHECK();
+  k_pack_finish<<<(unsigned)n, 128, 0, st>>>(tab, members);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
 }
 
 template <typename XT>

@@ -292,33 +292,8 @@ __global__ void k_update_fibers(int N, int first, double dt, double4* __restrict
   if (halt != nullptr && *halt) return;   // the solve failed: the state stays as it is
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const double4 xc = cur_pos[i], tc = cur_ori[i];
-  const float4 u = cur_tv[i], w = cur_rv[i];
-  double4 xn, tn;
-  if (first) {
-    xn = make_double4(xc.x + dt * u.x, xc.y + dt * u.y, xc.z + dt * u.z, 0.0);
-    tn = make_double4(tc.x + dt * w.x, tc.y + dt * w.y, tc.z + dt * w.z, 0.0);
-  } else {
-    const double4 xp = prev_pos[i], tp = prev_ori[i];
-    const float4 up = prev_tv[i], wp = prev_rv[i];
-    const double c43 = 4.0 / 3.0, c13 = 1.0 / 3.0, c23 = (2.0 / 3.0) * dt;
-    xn = make_double4(c43 * xc.x - c13 * xp.x + c23 * (2.0 * u.x - up.x),
-                      c43 * xc.y - c13 * xp.y + c23 * (2.0 * u.y - up.y),
-                      c43 * xc.z - c13 * xp.z + c23 * (2.0 * u.z - up.z), 0.0);
-    tn = make_double4(c43 * tc.x - c13 * tp.x + c23 * (2.0 * w.x - wp.x),
-                      c43 * tc.y - c13 * tp.y + c23 * (2.0 * w.y - wp.y),
-                      c43 * tc.z - c13 * tp.z + c23 * (2.0 * w.z - wp.z), 0.0);
-  }
-  const double inv = 1.0 / sqrt(tn.x * tn.x + tn.y * tn.y + tn.z * tn.z);
-  tn.x *= inv; tn.y *= inv; tn.z *= inv;
-  prev_pos[i] = xc;
-  prev_ori[i] = tc;
-  cur_pos[i] = xn;
-  cur_ori[i] = tn;
-  prev_tv[i] = u;
-  prev_rv[i] = w;
-  pos32[i] = make_float4((float)xn.x, (float)xn.y, (float)xn.z, 0.f);
-  ori32[i] = make_float4((float)tn.x, (float)tn.y, (float)tn.z, 0.f);
+  update_fiber(i, first, dt, prev_pos, cur_pos, prev_ori, cur_ori, prev_tv, cur_tv[i], prev_rv, cur_rv[i], pos32,
+               ori32);
 }
 
 int launch_update_fibers(int N, int first, double dt, double4* pp, double4* cp, double4* po, double4* co,

@@ -95,6 +95,36 @@ def test_packed_steps_follow_rf_step():
     assert st["ms_solve_system"] > 0 and st["ms_assemble_system"] > 0
 
 
+def test_packed_step_kernels_match_the_single_suspension_stages():
+    """rf_step_packed's packed assembly, velocities and update (a few launches
+    per pack) against the single-suspension stages around the same packed
+    solve: rf_assemble, rf_solve_packed, rf_update_velocities and
+    rf_update_fibers give the same state and velocities bit for bit.  The pack
+    holds three groups (FP16 and BF16 storage, two slendernesses); its first
+    member reports the pack's launches: the solve plus four per group."""
+    from rigidfibers_b200.simulation import solve_packed, step_packed
+    cfgs = [dict(precision="mixed_bf16"), dict(precision="mixed_fp16"),
+            dict(precision="mixed_bf16", slenderness=0.005), dict(precision="mixed_fp16")]
+    sizes = [1, 33, 128, 70]
+    lays = [_layout(n, 40 + k) for k, n in enumerate(sizes)]
+    staged = [_sim(*lay, **c) for lay, c in zip(lays, cfgs)]
+    packed = [_sim(*lay, **c) for lay, c in zip(lays, cfgs)]
+    for t in range(3):
+        for s in staged:
+            s.assembleSystem()
+            solve_packed([s])
+            s.updateVelocities()
+            s.updateFibers(t == 0)
+        assert step_packed(packed, [t] * len(packed)) == [0] * len(packed)
+        for a, b in zip(staged, packed):
+            for u, v in zip(a.state() + a.velocities(), b.state() + b.velocities()):
+                assert np.array_equal(u, v)
+    st = packed[0].stats()
+    assert st["kernel_launches"] == 1 + 4 * 3
+    assert packed[1].stats()["kernel_launches"] == 0
+    assert st["ms_assemble_system"] > 0 and st["ms_solve_system"] > 0 and st["ms_update_velocities"] > 0
+
+
 def test_packed_solve_refuses_what_it_does_not_take():
     from rigidfibers_b200 import _capi as C
     from rigidfibers_b200.simulation import solve_packed
