@@ -780,6 +780,7 @@ def run_ours(args, dist):
         "graph_replays_per_step": head["graph_replays"] / args.steps,
         "max_relative_residual": head["relres"],
         "matvec_variant": head["autotune"]["matvec_variant"],
+        "autotune": {k: head["autotune"][k] for k in ("asm_variant", "asm_ms", "matvec_variant", "matvec_ms")},
     }
     if args.direct_fibers > 0 and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)

@@ -208,9 +208,10 @@ int rf_set_profiling(rf_handle* h, int enable);
  * structured matvec kernel (matvec_variant 0 = TMA-staged, 2 = register-staged;
  * matvec_ms[0], [1] their times) in mixed precision, the column splits of the
  * dense FP32 matvec (gemv_ctas_per_sm of 2, 4, 8, 16; gemv_ms[] their times,
- * -1 when not tried) in FP32.  Call after rf_assemble; times each candidate with
- * CUDA events on the assembled operator, keeps the fastest for this handle and
- * caches it per (device, precision, M, N) for later calls (cached = 1).  The
+ * -1 when not tried) in FP32, and the numerical assembly's pair-tile kernel
+ * (asm_variant).  Call after rf_assemble; times each candidate with CUDA events
+ * on the assembled operator, keeps the fastest for this handle and caches it
+ * per (device, precision and solver, M, Q, N) for later calls (cached = 1).  The
  * summation order, hence the last bits of the solution, follow the choice.
  * (The reference compiles one kernel variant per run, runner/cuda_runner.py:49-117.) */
 typedef struct rf_tune_report {
@@ -222,8 +223,16 @@ typedef struct rf_tune_report {
   int panel_blocks;         /* direct solver: blocks of the LU panel kernel (one
                                grid sync per column): SMs, SMs/2, SMs/4 tried */
   double panel_ms[3];       /* first panel's time per candidate (-1: rows do not fit) */
+  int asm_variant;          /* numerical assembly's pair-tile kernel: 0 scalar FP32,
+                               1 packed two-lane FP32 (f32x2) for mirror points; both
+                               give bit-identical operators */
+  double asm_ms[2];         /* one assembly per candidate (-1: not tried, analytical) */
 } rf_tune_report;
 int rf_autotune(rf_handle* h, rf_tune_report* report);
+/* Select the numerical assembly's pair-tile kernel by hand (the asm_variant
+ * values of rf_tune_report); the operator is the same bit for bit either way.
+ * RF_E_INPUT for an unknown variant. */
+int rf_set_assembly_variant(rf_handle* h, int variant);
 
 /* CUDA graphs; results are identical in every mode.  mode 1 (default): with
  * GMRES, rf_step runs the whole time step as one graph from the second step of

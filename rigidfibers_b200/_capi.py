@@ -72,6 +72,8 @@ class rf_tune_report(ctypes.Structure):
         ("cached", ctypes.c_int),
         ("panel_blocks", ctypes.c_int),
         ("panel_ms", ctypes.c_double * 3),
+        ("asm_variant", ctypes.c_int),
+        ("asm_ms", ctypes.c_double * 2),
     ]
 
 
@@ -146,6 +148,7 @@ SIGNATURES = {
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_cuda_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_set_assembly_variant": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_autotune": (ctypes.c_int, [_H, ctypes.POINTER(rf_tune_report)]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "rf_checkpoint_bytes": (ctypes.c_int64, [_H]),

@@ -13,6 +13,9 @@
 //    unordered fiber pairs evaluates K once per (qi, qj) and serves both
 //    blocks (i,j) and (j,i)  -- half the kernel evaluations;
 //  * the reference re-evaluates K once per k_j (M times); here once;
+//  * the sum over fiber j's points splits each separation at its projection
+//    onto fiber j's axis (r = d + u t_j, d perpendicular to t_j), so the six
+//    components of K contract to four scalar moments (see phase 1);
 //  * the quadrature is mirror-symmetric (s_{Q-1-q} = -s_q, w equal, P_k of
 //    parity k), so both contractions fold q with Q-1-q into an even and an
 //    odd part and use half the multiply-adds;
@@ -104,9 +107,111 @@ __device__ __forceinline__ void asm_tile_of(int N, unsigned L, int& I, int& J) {
   }
 }
 
+// Phase 1 of a pair tile, numerical: G[c][k] = sum_q K_c(p - s_q t_j) W[k][q]
+// for one point p of fiber i (relative to fiber j's centre) against the Q
+// points of fiber j, written to gcol[(c K1 + k) GS].
+//
+// The separation r = p - s_q t_j is split at p's projection onto fiber j's
+// axis: r = d + u_q t_j with d = p - s* t_j perpendicular to t_j and
+// u_q = s* - s_q, so |r|^2 = |d|^2 + u_q^2 and
+//   K(r) = a I + b r r^T = a I + b [d d^T + u (d t^T + t d^T) + u^2 t t^T]
+// (a = 1/|r| + 2eps^2/|r|^3, b = 1/|r|^3 - 6eps^2/|r|^5).  The sum over q then
+// needs four scalar moments per k instead of six tensor components,
+//   A_k = sum W a,  B0_k = sum W b,  B1_k = sum W b u,  B2_k = sum W b u^2,
+// and every term of the recombination is bounded by |r|^2 (|d|, |u| <= |r|),
+// so nothing cancels.  s* is refined once (d . t_j, already ~1e-7 |p|, is
+// folded back) so that d is perpendicular to t_j to rounding.  Points q and
+// Q-1-q are evaluated together and their values folded into even and odd
+// parts (W[k][Q-1-q] = (-1)^k W[k][q]).
+//
+// P2 = true evaluates the two mirror points in the two lanes of packed FP32
+// instructions (add/mul/fma .f32x2) and accumulates the moments in lane pairs
+// (A, B0), (B1, B2) against the duplicated weights W2; every rounding is the
+// same as in the scalar form (all steps are explicit _rn operations, none can
+// be contracted), so both give bit-identical G.
+template <int K1, int Q, int GS, bool P2>
+__device__ __forceinline__ void stokeslet_moments_G(const Tables& tab, const float p[3], const float4 tj, float e2,
+                                                    float e2x3, float* __restrict__ gcol) {
+  constexpr int H = Q / 2;
+  float ss = fmaf(p[0], tj.x, fmaf(p[1], tj.y, p[2] * tj.z));
+  float dx = fmaf(-ss, tj.x, p[0]), dy = fmaf(-ss, tj.y, p[1]), dz = fmaf(-ss, tj.z, p[2]);
+  const float dl = fmaf(dx, tj.x, fmaf(dy, tj.y, dz * tj.z));
+  ss += dl;
+  dx = fmaf(-dl, tj.x, dx);
+  dy = fmaf(-dl, tj.y, dy);
+  dz = fmaf(-dl, tj.z, dz);
+  const float dd = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float2 m01[K1], m23[K1];   // (A_k, B0_k), (B1_k, B2_k)
+#pragma unroll
+  for (int k = 0; k < K1; ++k) m01[k] = m23[k] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < H; ++q) {
+    float2 fa, fb, fc, fd;   // lane x: point q, lane y: point Q-1-q
+    if constexpr (P2) {
+      const float2 u = __fadd2_rn(make_float2(ss, ss), make_float2(-tab.pts[q], -tab.pts[Q - 1 - q]));
+      const float2 r2 = __ffma2_rn(u, u, make_float2(dd, dd));
+      const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 inv2 = __fmul2_rn(inv, inv);
+      const float2 inv3 = __fmul2_rn(inv2, inv);
+      const float2 inv5 = __fmul2_rn(inv3, inv2);
+      fa = __ffma2_rn(make_float2(e2, e2), inv3, inv);
+      fb = __ffma2_rn(make_float2(e2x3, e2x3), inv5, inv3);
+      fc = __fmul2_rn(fb, u);
+      fd = __fmul2_rn(fc, u);
+    } else {
+      float r[4][2];
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const float u = __fadd_rn(ss, -tab.pts[side == 0 ? q : Q - 1 - q]);
+        const float r2 = __fmaf_rn(u, u, dd);
+        const float inv = rsqrtf(r2);
+        const float inv2 = __fmul_rn(inv, inv);
+        const float inv3 = __fmul_rn(inv2, inv);
+        const float inv5 = __fmul_rn(inv3, inv2);
+        r[0][side] = __fmaf_rn(e2, inv3, inv);
+        r[1][side] = __fmaf_rn(e2x3, inv5, inv3);
+        r[2][side] = __fmul_rn(r[1][side], u);
+        r[3][side] = __fmul_rn(r[2][side], u);
+      }
+      fa = make_float2(r[0][0], r[0][1]);
+      fb = make_float2(r[1][0], r[1][1]);
+      fc = make_float2(r[2][0], r[2][1]);
+      fd = make_float2(r[3][0], r[3][1]);
+    }
+    const float2 e01 = make_float2(__fadd_rn(fa.x, fa.y), __fadd_rn(fb.x, fb.y));
+    const float2 o01 = make_float2(__fsub_rn(fa.x, fa.y), __fsub_rn(fb.x, fb.y));
+    const float2 e23 = make_float2(__fadd_rn(fc.x, fc.y), __fadd_rn(fd.x, fd.y));
+    const float2 o23 = make_float2(__fsub_rn(fc.x, fc.y), __fsub_rn(fd.x, fd.y));
+#pragma unroll
+    for (int k = 0; k < K1; ++k) {
+      if constexpr (P2) {
+        m01[k] = __ffma2_rn((k & 1) ? o01 : e01, tab.W2[k][q], m01[k]);
+        m23[k] = __ffma2_rn((k & 1) ? o23 : e23, tab.W2[k][q], m23[k]);
+      } else {
+        const float w = tab.W[k][q];
+        m01[k].x = __fmaf_rn((k & 1) ? o01.x : e01.x, w, m01[k].x);
+        m01[k].y = __fmaf_rn((k & 1) ? o01.y : e01.y, w, m01[k].y);
+        m23[k].x = __fmaf_rn((k & 1) ? o23.x : e23.x, w, m23[k].x);
+        m23[k].y = __fmaf_rn((k & 1) ? o23.y : e23.y, w, m23[k].y);
+      }
+    }
+  }
+  // components in the order (11, 22, 33, 12, 13, 23)
+  const float Dd[6] = {dx * dx, dy * dy, dz * dz, dx * dy, dx * dz, dy * dz};
+  const float Sd[6] = {2.f * dx * tj.x, 2.f * dy * tj.y, 2.f * dz * tj.z, fmaf(dx, tj.y, dy * tj.x),
+                       fmaf(dx, tj.z, dz * tj.x), fmaf(dy, tj.z, dz * tj.y)};
+  const float Tt[6] = {tj.x * tj.x, tj.y * tj.y, tj.z * tj.z, tj.x * tj.y, tj.x * tj.z, tj.y * tj.z};
+#pragma unroll
+  for (int c = 0; c < 6; ++c)
+#pragma unroll
+    for (int k = 0; k < K1; ++k)
+      gcol[(c * K1 + k) * GS] =
+          fmaf(m01[k].y, Dd[c], fmaf(m23[k].x, Sd[c], fmaf(m23[k].y, Tt[c], c < 3 ? m01[k].x : 0.f)));
+}
+
 // One CTA's tile pair (I, J) of one suspension (the body of k_assemble_pairs and
 // of the packed assembly, which maps its blocks onto many suspensions' tiles).
-template <int M, int Q, int MODE, int INTEG>
+template <int M, int Q, int MODE, int INTEG, bool P2>
 __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, const float4* __restrict__ pos,
                                                    const float4* __restrict__ ori, const AsmOut& out, int I, int J) {
   using S = AsmShape<M, Q>;
@@ -115,7 +220,6 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
   constexpr int FF = K1 * 3;   // force-term floats per fiber
   static_assert(Q % 2 == 0, "mirror folding needs an even number of quadrature points");
 
-  __shared__ float4 sPj[TI][Q];          // s_q t_j for the J tile (numerical: offsets from the centre)
   __shared__ float4 sTi[TI], sTj[TI];    // orientations
   __shared__ float sD[TI][TI][3];        // x_i - x_j, formed in FP64 and rounded once (numerical)
   extern __shared__ __align__(16) float smem_dyn[];
@@ -145,18 +249,6 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     sD[a][c][0] = (float)(xi.x - xj.x);
     sD[a][c][1] = (float)(xi.y - xj.y);
     sD[a][c][2] = (float)(xi.z - xj.z);
-  }
-  if (tid < S::U) {
-    const int jl = tid / Q, q = tid % Q;
-    const int j = min(j0 + jl, N - 1);
-    const float4 t = ori[j];
-    const float s = tab.pts[q];
-    if (SYM) {
-      sPj[jl][q] = make_float4(s * t.x, s * t.y, s * t.z, 0.f);
-    } else {
-      const float4 x = pos[j];
-      sPj[jl][q] = make_float4(fmaf(s, t.x, x.x), fmaf(s, t.y, x.y), fmaf(s, t.z, x.z), 0.f);
-    }
   }
   for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
   if constexpr (MODE != kAsmDense) {
@@ -206,60 +298,36 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     const bool pair_ok = unit_ok && (!diag || (SYM ? il < jl : il != jl));
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj] (numerical, mirror-
     // folded over qj) or the closed-form integral (analytical)
-    float g[6][K1];
-#pragma unroll
-    for (int c = 0; c < 6; ++c)
-#pragma unroll
-      for (int k = 0; k < K1; ++k) g[c][k] = 0.f;
-    if (!SYM && pair_ok) {
-      const double4 xi4 = out.pos64[i], ti4 = out.ori64[i];
-      const double4 xj4 = out.pos64[j0 + jl], tj4 = out.ori64[j0 + jl];
-      const double s = (double)tab.pts[qi];
-      const double R0[3] = {xi4.x + s * ti4.x - xj4.x, xi4.y + s * ti4.y - xj4.y, xi4.z + s * ti4.z - xj4.z};
-      const double tj[3] = {tj4.x, tj4.y, tj4.z};
-      analytic_G<M>(R0, tj, 2.0 * (double)tab.eps * (double)tab.eps, g);
-    }
-    if (SYM && pair_ok) {
-      const float4 ti = sTi[il];
-      const float pix = fmaf(tab.pts[qi], ti.x, sD[il][jl][0]);
-      const float piy = fmaf(tab.pts[qi], ti.y, sD[il][jl][1]);
-      const float piz = fmaf(tab.pts[qi], ti.z, sD[il][jl][2]);
-#pragma unroll
-      for (int q = 0; q < H; ++q) {
-        float Kp[6], Km[6];
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-          const float4 pj = sPj[jl][side == 0 ? q : Q - 1 - q];
-          const float rx = pix - pj.x, ry = piy - pj.y, rz = piz - pj.z;
-          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-          const float inv = rsqrtf(r2);
-          const float inv2 = inv * inv;
-          const float inv3 = inv2 * inv;
-          const float inv5 = inv3 * inv2;
-          const float a = fmaf(e2, inv3, inv);        // inv + 2eps^2 inv^3
-          const float bb = fmaf(e2x3, inv5, inv3);    // inv^3 - 6eps^2 inv^5
-          const float bx = bb * rx, by = bb * ry, bz = bb * rz;
-          float* K = side == 0 ? Kp : Km;
-          K[0] = fmaf(bx, rx, a);
-          K[1] = fmaf(by, ry, a);
-          K[2] = fmaf(bz, rz, a);
-          K[3] = bx * ry;
-          K[4] = bx * rz;
-          K[5] = by * rz;
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          const float ev = Kp[c] + Km[c], od = Kp[c] - Km[c];
-#pragma unroll
-          for (int k = 0; k < K1; ++k) g[c][k] = fmaf((k & 1) ? od : ev, tab.W[k][q], g[c][k]);
-        }
-      }
-    }
-    if (tid < S::U) {
+    // G goes straight to shared memory, column c * K1 + k of unit tid
+    float* const gcol = &sG[0][0] + tid;
+    if (!SYM && tid < S::U) {
+      float g[6][K1];
 #pragma unroll
       for (int c = 0; c < 6; ++c)
 #pragma unroll
-        for (int k = 0; k < K1; ++k) sG[c * K1 + k][tid] = g[c][k];
+        for (int k = 0; k < K1; ++k) g[c][k] = 0.f;
+      if (pair_ok) {
+        const double4 xi4 = out.pos64[i], ti4 = out.ori64[i];
+        const double4 xj4 = out.pos64[j0 + jl], tj4 = out.ori64[j0 + jl];
+        const double s = (double)tab.pts[qi];
+        const double R0[3] = {xi4.x + s * ti4.x - xj4.x, xi4.y + s * ti4.y - xj4.y, xi4.z + s * ti4.z - xj4.z};
+        const double tj[3] = {tj4.x, tj4.y, tj4.z};
+        analytic_G<M>(R0, tj, 2.0 * (double)tab.eps * (double)tab.eps, g);
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+#pragma unroll
+        for (int k = 0; k < K1; ++k) gcol[(c * K1 + k) * S::GS] = g[c][k];
+    }
+    if (SYM && pair_ok) {
+      const float4 ti = sTi[il];
+      const float si = tab.pts[qi];
+      const float p[3] = {fmaf(si, ti.x, sD[il][jl][0]), fmaf(si, ti.y, sD[il][jl][1]),
+                          fmaf(si, ti.z, sD[il][jl][2])};
+      stokeslet_moments_G<K1, Q, S::GS, P2>(tab, p, sTj[jl], e2, e2x3, gcol);
+    } else if (SYM && tid < S::U) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) gcol[c * S::GS] = 0.f;
     }
     __syncthreads();
 
@@ -424,13 +492,13 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
   }
 }
 
-template <int M, int Q, int MODE, int INTEG>
+template <int M, int Q, int MODE, int INTEG, bool P2>
 __global__ void __launch_bounds__(192, INTEG == kNumerical ? 4 : 2)
 k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
                  AsmOut out) {
   int I, J;
   asm_tile_of<Q, INTEG>(N, blockIdx.x, I, J);
-  assemble_pair_tile<M, Q, MODE, INTEG>(tab, N, pos, ori, out, I, J);
+  assemble_pair_tile<M, Q, MODE, INTEG, P2>(tab, N, pos, ori, out, I, J);
 }
 
 // F[i][k] = sum_X ffpart[X][i][k] (fixed order); b[i][k'] = -C_i(k') F[i][k'+1]
@@ -485,7 +553,7 @@ k_pack_assemble(const Tables tab, const PackStepMember* __restrict__ mem, int n)
   out.pos64 = p.pos64;
   int I, J;
   asm_tile_of<24, kNumerical>(p.N, (unsigned)(L - p.asm_start), I, J);
-  assemble_pair_tile<5, 24, MODE, kNumerical>(tab, p.N, p.pos32, p.ori32, out, I, J);
+  assemble_pair_tile<5, 24, MODE, kNumerical, false>(tab, p.N, p.pos32, p.ori32, out, I, J);
 }
 
 // one block per member: its force terms and right-hand side
@@ -550,19 +618,32 @@ int64_t struct_words16(int M, int N) {
   return struct_store_tiles(N) * (int64_t)kStoreTile * kStoreTile * s16_record_words(M);
 }
 
-template <int M, int Q, int MODE, int INTEG>
-static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
-                              float* F, float* b, cudaStream_t st) {
+template <int M, int Q, int MODE, int INTEG, bool P2>
+static int launch_pairs(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
+                        cudaStream_t st) {
   using S = AsmShape<M, Q>;
   const int64_t T = ceil_div(N, S::TI);
   const int64_t ntp = INTEG == kNumerical ? T * (T + 1) / 2 : T * T;
   // once per process (thread-safe static initialisation; handles of a serving
   // loop launch from several threads)
-  static const cudaError_t attr = cudaFuncSetAttribute(k_assemble_pairs<M, Q, MODE, INTEG>,
+  static const cudaError_t attr = cudaFuncSetAttribute(k_assemble_pairs<M, Q, MODE, INTEG, P2>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
   RF_CUDA_TRY(attr);
-  k_assemble_pairs<M, Q, MODE, INTEG><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
+  k_assemble_pairs<M, Q, MODE, INTEG, P2><<<(unsigned)ntp, 192, S::kSmem, st>>>(tab, N, pos, ori, out);
   RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+template <int M, int Q, int MODE, int INTEG>
+static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
+                              float* F, float* b, int variant, cudaStream_t st) {
+  using S = AsmShape<M, Q>;
+  const int64_t T = ceil_div(N, S::TI);
+  if (INTEG == kNumerical && variant == 1) {
+    RF_TRY_RF((launch_pairs<M, Q, MODE, INTEG, INTEG == kNumerical>(tab, N, pos, ori, out, st)));
+  } else {
+    RF_TRY_RF((launch_pairs<M, Q, MODE, INTEG, false>(tab, N, pos, ori, out, st)));
+  }
   const int64_t n = (int64_t)N * (M + 1);
   k_force_terms<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 8), 256, 0, st>>>(tab, N, ori, out.ffpart,
                                                                                          (int)T, F, b);
@@ -572,9 +653,14 @@ static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const
 
 template <int MODE, int INTEG>
 static int dispatch_assemble(const Tables& tab, int N, const float4* pos, const float4* ori, const AsmOut& out,
-                             float* F, float* b, cudaStream_t st) {
+                             float* F, float* b, int variant, cudaStream_t st) {
+  if (variant < 0 || variant >= kAsmVariants) {
+    set_last_error_str("assemble: unknown kernel variant");
+    return RF_E_INPUT;
+  }
 #define RF_ASM_CASE(MM, QQ) \
-  if (tab.M == MM && tab.Q == QQ) return launch_assemble_mq<MM, QQ, MODE, INTEG>(tab, N, pos, ori, out, F, b, st);
+  if (tab.M == MM && tab.Q == QQ)  \
+    return launch_assemble_mq<MM, QQ, MODE, INTEG>(tab, N, pos, ori, out, F, b, variant, st);
   RF_FOR_EACH_MQ(RF_ASM_CASE)
 #undef RF_ASM_CASE
   set_last_error_str("assemble: (M, Q) combination not instantiated");
@@ -582,13 +668,14 @@ static int dispatch_assemble(const Tables& tab, int N, const float4* pos, const 
 }
 
 int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
-                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st) {
+                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st,
+                              int variant) {
   AsmOut out{};
   out.pos64 = pos64;
   out.A = A;
   out.lda = lda;
   out.ffpart = ffpart;
-  return dispatch_assemble<kAsmDense, kNumerical>(tab, N, pos, ori, out, F, b, st);
+  return dispatch_assemble<kAsmDense, kNumerical>(tab, N, pos, ori, out, F, b, variant, st);
 }
 
 int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
@@ -600,19 +687,19 @@ int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, cons
   out.A = A;
   out.lda = lda;
   out.ffpart = ffpart;
-  return dispatch_assemble<kAsmDense, kAnalytical>(tab, N, pos, ori, out, F, b, st);
+  return dispatch_assemble<kAsmDense, kAnalytical>(tab, N, pos, ori, out, F, b, 0, st);
 }
 
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
                                float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,
-                               cudaStream_t st) {
+                               cudaStream_t st, int variant) {
   AsmOut out{};
   out.pos64 = pos64;
   out.S32 = S32;
   out.S16 = S16;
   out.ffpart = ffpart;
-  if (bf16) return dispatch_assemble<kAsmStructBF16, kNumerical>(tab, N, pos, ori, out, F, b, st);
-  return dispatch_assemble<kAsmStructF16, kNumerical>(tab, N, pos, ori, out, F, b, st);
+  if (bf16) return dispatch_assemble<kAsmStructBF16, kNumerical>(tab, N, pos, ori, out, F, b, variant, st);
+  return dispatch_assemble<kAsmStructF16, kNumerical>(tab, N, pos, ori, out, F, b, variant, st);
 }
 
 }  // namespace rf

@@ -187,6 +187,7 @@ static Tables make_tables(const rf_config& c) {
     for (int k = 0; k <= M; ++k) {
       // weight and Legendre value rounded separately, as the REAL*4 tables are
       t.W[k][q] = (float)wts[q] * (float)P(pts[q], k);
+      if (2 * q < Q) t.W2[k][q] = make_float2(t.W[k][q], t.W[k][q]);
     }
   }
   const double eps = c.slenderness;
@@ -299,6 +300,7 @@ struct rf_handle {
   bool use_graphs = true;         // GMRES restart cycles from graphs
   bool use_step_graphs = true;    // rf_step as one graph
   int mv_variant = 0;             // structured matvec kernel (rf_autotune)
+  int asm_variant = 0;            // numerical pair-tile kernel (rf_autotune)
   int64_t ypart_floats = 0;       // capacity of ypart
   bool assembled = false, solved = false;
   int64_t device_bytes = 0;
@@ -664,12 +666,13 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
 static int enqueue_assemble(rf_handle* h) {
   if (h->mixed)
     return launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
-                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st);
+                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st,
+                                      h->asm_variant);
   if (h->cfg.integration == RF_ANALYTICAL)
     return launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
                                       h->lda, h->ffpart, h->F, h->b, h->st);
   return launch_assemble_numerical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->A, h->lda, h->ffpart,
-                                   h->F, h->b, h->st);
+                                   h->F, h->b, h->st, h->asm_variant);
 }
 
 int rf_assemble(rf_handle* h) {
@@ -1639,9 +1642,9 @@ int rf_checkpoint_load(rf_handle* h, const void* buf, int64_t bytes, int64_t* st
 // fastest; the choice is cached per (device, precision, M, N).
 namespace {
 struct TuneKey {
-  int dev, prec, M, N;
+  int dev, prec, M, Q, N;
   bool operator<(const TuneKey& o) const {
-    return std::tie(dev, prec, M, N) < std::tie(o.dev, o.prec, o.M, o.N);
+    return std::tie(dev, prec, M, Q, N) < std::tie(o.dev, o.prec, o.M, o.Q, o.N);
   }
 };
 std::mutex g_tune_mu;
@@ -1650,6 +1653,7 @@ std::map<TuneKey, rf_tune_report> g_tune_cache;
 
 static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
   if (h->cfg.solver == RF_SOLVER_DIRECT && t.panel_blocks > 0) h->lu.panel_blocks = t.panel_blocks;
+  h->asm_variant = t.asm_variant;
   if (h->mixed) {
     h->mv_variant = t.matvec_variant;
   } else {
@@ -1662,7 +1666,7 @@ static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
 int rf_autotune(rf_handle* h, rf_tune_report* out) {
   if (!h) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("rf_autotune needs an assembled system (rf_assemble)"); return RF_E_STATE; }
-  const TuneKey key{h->dev, h->cfg.precision * 4 + h->cfg.solver, h->M, h->N};
+  const TuneKey key{h->dev, h->cfg.precision * 4 + h->cfg.solver, h->M, h->tab.Q, h->N};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -1722,6 +1726,23 @@ int rf_autotune(rf_handle* h, rf_tune_report* out) {
     }
     t.matvec_variant = 0;
   }
+  // the numerical assembly's pair-tile kernel (the variants' results are bit
+  // for bit the same; re-assembling rewrites the same operator)
+  t.asm_variant = 0;
+  for (int v = 0; v < kAsmVariants; ++v) t.asm_ms[v] = -1;
+  if (h->cfg.integration == RF_NUMERICAL) {
+    double best = 1e30;
+    const int keep = h->asm_variant;
+    for (int v = 0; v < kAsmVariants; ++v) {
+      h->asm_variant = v;
+      double ms = 0;
+      const int rc = time_it([&]() { return enqueue_assemble(h); }, &ms);
+      if (rc != RF_OK) { h->asm_variant = keep; return rc; }
+      t.asm_ms[v] = ms;
+      if (ms < best) { best = ms; t.asm_variant = v; }
+    }
+    h->asm_variant = keep;
+  }
   if (h->cfg.solver == RF_SOLVER_DIRECT) {
     // LU panel: fewer blocks make each grid sync cheaper but give each block
     // more rows (they must fit in shared memory); time the first panel
@@ -1754,6 +1775,13 @@ int rf_debug_set_device_wait_limit(int64_t limit) {
 int rf_debug_fail_allocation_after(int n) {
   if (n < -1) return RF_E_INPUT;
   g_fail_alloc_after.store(n);
+  return RF_OK;
+}
+
+int rf_set_assembly_variant(rf_handle* h, int variant) {
+  if (!h || variant < 0 || variant >= kAsmVariants) return RF_E_INPUT;
+  if (h->asm_variant != variant) h->release_step_graphs();   // captured steps hold the old kernel
+  h->asm_variant = variant;
   return RF_OK;
 }
 

@@ -21,6 +21,9 @@ constexpr int kMaxQuad = 48;      // quadrature points per fiber (16 intervals x
 struct Tables {
   float pts[kMaxQuad];
   float W[kMaxTerms + 1][kMaxQuad];   // W[0][q] = w_q
+  // W2[k][q] = (W[k][q], W[k][q]) for q < Q/2: the weight as the second
+  // operand of a packed two-lane FP32 multiply-add
+  float2 W2[kMaxTerms + 1][kMaxQuad / 2];
   float gamma[kMaxTerms];   // gamma[0] = D1 (force index 0), gamma[k] for k>=1
   float eigen[kMaxTerms];   // E_k; unused for k = 0
   float e2;                 // 2 * eps^2

@@ -28,11 +28,16 @@ bool mq_supported(int M, int Q);
 int launch_reduce_rows(const float* part, int nparts, int64_t R, float* out, cudaStream_t st);
 int assemble_tiles(int M, int Q, int N);
 
+// Kernel variants of the numerical pair tiles (rf_autotune picks one; both
+// give bit-identical results): 0 scalar FP32, 1 packed two-lane FP32
+// (add/mul/fma .f32x2) for the two mirror points of each folded pair.
+constexpr int kAsmVariants = 2;
 // Numerical assembly.  ffpart: assemble_tiles(M,Q,N) x N x 3(M+1) floats of
 // scratch; F: N x 3(M+1) force terms sum_j T^{ij}[k][P0] F/2; b: R.  pos64:
 // the FP64 centres, from which the pair separations are formed.
 int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
-                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st);
+                              float* A, int64_t lda, float* ffpart, float* F, float* b, cudaStream_t st,
+                              int variant = 0);
 // Analytical integration (closed-form inner integral in FP64), dense A.
 int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
                                const double4* pos64, const double4* ori64, float* A, int64_t lda, float* ffpart,
@@ -40,7 +45,7 @@ int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, cons
 // Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
                                float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,
-                               cudaStream_t st);
+                               cudaStream_t st, int variant = 0);
 int64_t struct_store_tiles(int N);
 int64_t struct_floats32(int M, int N);
 int64_t struct_words16(int M, int N);

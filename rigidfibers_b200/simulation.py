@@ -178,8 +178,8 @@ class Simulation:
         C.check(self._lib.rf_set_cuda_graphs(self._h, int(mode)), "rf_set_cuda_graphs")
 
     def autotune(self):
-        """Time the matvec launch choices on the assembled operator and keep the
-        fastest (rf_autotune); assembles first if needed."""
+        """Time the matvec and assembly launch choices on the assembled operator
+        and keep the fastest (rf_autotune); assembles first if needed."""
         t = C.rf_tune_report()
         rc = self._lib.rf_autotune(self._h, ctypes.byref(t))
         if rc == C.RF_E_STATE:
@@ -188,7 +188,8 @@ class Simulation:
         C.check(rc, "rf_autotune")
         return {"matvec_variant": t.matvec_variant, "matvec_ms": list(t.matvec_ms),
                 "gemv_ctas_per_sm": t.gemv_ctas_per_sm, "gemv_ms": list(t.gemv_ms), "cached": bool(t.cached),
-                "panel_blocks": t.panel_blocks, "panel_ms": list(t.panel_ms)}
+                "panel_blocks": t.panel_blocks, "panel_ms": list(t.panel_ms),
+                "asm_variant": t.asm_variant, "asm_ms": list(t.asm_ms)}
 
     # -- checkpoint / resume ---------------------------------------------------
     def checkpoint(self):

@@ -176,8 +176,38 @@ def test_autotune_keeps_the_solution(prec):
         assert min(v for v in rep["gemv_ms"] if v > 0) > 0
     else:
         assert rep["matvec_variant"] in (0, 2) and min(rep["matvec_ms"]) > 0
+    assert rep["asm_variant"] in (0, 1) and min(rep["asm_ms"]) > 0
     sim.run(2)
     p1, o1 = sim.state()
     assert _rel(p1, p0) <= 1e-5 and _rel(o1, o0) <= 1e-5
     again = Simulation(Config(precision=prec), pos, ori)
     assert again.autotune()["cached"]
+
+
+@pytest.mark.parametrize("n", [7, 40, 130])
+@pytest.mark.parametrize("prec", ["fp32", "mixed_fp16", "mixed_bf16"])
+def test_assembly_variants_are_bit_identical(n, prec):
+    """The numerical pair-tile kernels (scalar FP32 and packed two-lane FP32)
+    round every step the same way: the dense operator and right-hand side are
+    equal bit for bit, and so are two whole steps of the structured path."""
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(n, radius=max(1.5, 0.8 * n ** (1 / 3)), seed=41 + n)
+    out = []
+    for v in (0, 1):
+        sim = _sim(pos, ori, precision=prec)
+        C.check(C.load().rf_set_assembly_variant(sim._h, v), "rf_set_assembly_variant")
+        sim.assembleSystem()
+        A, b = sim.system(with_matrix=prec == "fp32")
+        sim.run(2)
+        p, o = sim.state()
+        out.append((A, b, p, o))
+        sim.close()
+    for a, b in zip(out[0], out[1]):
+        if a is not None:
+            assert np.array_equal(np.asarray(a), np.asarray(b))
+    with pytest.raises(Exception):
+        sim = _sim(pos, ori, precision=prec)
+        try:
+            C.check(C.load().rf_set_assembly_variant(sim._h, 2), "rf_set_assembly_variant")
+        finally:
+            sim.close()
