@@ -57,10 +57,12 @@ struct AsmShape {
   static constexpr int K1 = M + 1;       // P_0..P_M
   static constexpr int NC = 6 * K1;      // G columns per unit
   static constexpr int H = Q / 2;        // folded quadrature points
-  // dynamic shared memory: G columns per unit (rows padded to an odd stride so
-  // that phase 2, where consecutive threads read consecutive columns, is free
-  // of bank conflicts), then the T blocks (6 floats each)
-  static constexpr int GS = U + 1;
+  static constexpr int NT = 192;         // threads per CTA
+  // dynamic shared memory: G as NC columns of U units (unit u = qi * TI + il),
+  // then the T blocks (6 floats each).  The column stride is TI (mod 32)
+  // words: phase 2 has lanes (col, tl), TI consecutive tl per column and
+  // 32 / TI columns per warp, and reads 32 distinct banks.
+  static constexpr int GS = (U + 31) / 32 * 32 + TI;
   // the T blocks start on a 16-byte boundary (they are copied out as float4);
   // NC * GS is odd for odd M + 1
   static constexpr int GOFF = (NC * GS + 3) / 4 * 4;
@@ -109,7 +111,7 @@ __device__ __forceinline__ void asm_tile_of(int N, unsigned L, int& I, int& J) {
 
 // Phase 1 of a pair tile, numerical: G[c][k] = sum_q K_c(p - s_q t_j) W[k][q]
 // for one point p of fiber i (relative to fiber j's centre) against the Q
-// points of fiber j, written to gcol[(c K1 + k) GS].
+// points of fiber j, written to gcol[(6 k + c) GS].
 //
 // The separation r = p - s_q t_j is split at p's projection onto fiber j's
 // axis: r = d + u_q t_j with d = p - s* t_j perpendicular to t_j and
@@ -205,7 +207,7 @@ __device__ __forceinline__ void stokeslet_moments_G(const Tables& tab, const flo
   for (int c = 0; c < 6; ++c)
 #pragma unroll
     for (int k = 0; k < K1; ++k)
-      gcol[(c * K1 + k) * GS] =
+      gcol[(k * 6 + c) * GS] =
           fmaf(m01[k].y, Dd[c], fmaf(m23[k].x, Sd[c], fmaf(m23[k].y, Tt[c], c < 3 ? m01[k].x : 0.f)));
 }
 
@@ -250,9 +252,9 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     sD[a][c][1] = (float)(xi.y - xj.y);
     sD[a][c][2] = (float)(xi.z - xj.z);
   }
-  for (int k = tid; k < TI * FF; k += blockDim.x) (&sfJ[0][0])[k] = 0.f;
+  for (int k = tid; k < TI * FF; k += S::NT) (&sfJ[0][0])[k] = 0.f;
   if constexpr (MODE != kAsmDense) {
-    for (int q = tid; q < S::NQ32; q += blockDim.x) {
+    for (int q = tid; q < S::NQ32; q += S::NT) {
       const int c = q % 6, blk = q / 6;
       int row = 0, col = 0;
       if (blk < M * M) {
@@ -267,8 +269,8 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     }
   }
 
-  // own unit
-  const int il = tid / Q, qi = tid % Q;
+  // own unit: u = qi * TI + il (a warp holds 32 / TI points of TI fibers)
+  const int il = tid % TI, qi = tid / TI;
   const int i = i0 + il;
   const bool unit_ok = (tid < S::U) && (i < N);
   // numerical: the separation of quadrature points is formed as
@@ -298,7 +300,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     const bool pair_ok = unit_ok && (!diag || (SYM ? il < jl : il != jl));
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj] (numerical, mirror-
     // folded over qj) or the closed-form integral (analytical)
-    // G goes straight to shared memory, column c * K1 + k of unit tid
+    // G goes straight to shared memory, column k * 6 + c of unit tid
     float* const gcol = &sG[0][0] + tid;
     if (!SYM && tid < S::U) {
       float g[6][K1];
@@ -317,7 +319,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
 #pragma unroll
       for (int c = 0; c < 6; ++c)
 #pragma unroll
-        for (int k = 0; k < K1; ++k) gcol[(c * K1 + k) * S::GS] = g[c][k];
+        for (int k = 0; k < K1; ++k) gcol[(k * 6 + c) * S::GS] = g[c][k];
     }
     if (SYM && pair_ok) {
       const float4 ti = sTi[il];
@@ -332,16 +334,17 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     __syncthreads();
 
     // ---- phase 2: T[ki][kj][c] = sum_qi W[ki][qi] G[qi][c][kj], folded over qi
-    for (int task = tid; task < TI * NC; task += blockDim.x) {
-      const int tl = task / NC, col = task % NC;
-      const int c = col / K1, kj = col % K1;
-      const float* gp = &sG[col][tl * Q];
+    // lanes (col, tl), tl fastest; column col = kj * 6 + c
+    for (int task = tid; task < TI * NC; task += S::NT) {
+      const int col = task / TI, tl = task % TI;
+      const int kj = col / 6, c = col % 6;
+      const float* gp = &sG[col][tl];
       float acc[K1];
 #pragma unroll
       for (int k = 0; k < K1; ++k) acc[k] = 0.f;
 #pragma unroll
       for (int q = 0; q < H; ++q) {
-        const float lo = gp[q], hi = gp[Q - 1 - q];
+        const float lo = gp[q * TI], hi = gp[(Q - 1 - q) * TI];
         const float ev = lo + hi, od = lo - hi;
 #pragma unroll
         for (int k = 0; k < K1; ++k) acc[k] = fmaf((k & 1) ? od : ev, tab.W[k][q], acc[k]);
@@ -354,7 +357,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     const int j = j0 + jl;
     if constexpr (MODE == kAsmDense) {
       // ---- phase 3a: block (i, j) -- rows of fiber i, columns of fiber j
-      for (int task = tid; task < TI * M * M; task += blockDim.x) {
+      for (int task = tid; task < TI * M * M; task += S::NT) {
         const int kJp = task / (TI * M), rem = task % (TI * M);
         const int tl = rem / M, kIp = rem % M;
         const int ii = i0 + tl;
@@ -385,7 +388,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
       if (SYM) {
         const float4 tj = sTj[jl];
         const float t3[3] = {tj.x, tj.y, tj.z};
-        for (int task = tid; task < TI * M * M; task += blockDim.x) {
+        for (int task = tid; task < TI * M * M; task += S::NT) {
           const int tl = task / (M * M), rem = task % (M * M);
           const int kIp = rem / M, kJp = rem % M;
           const int ii = i0 + tl;
@@ -415,7 +418,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
       // Pairs that do not exist (i >= N, i >= j on a diagonal tile) came out
       // of phases 1-2 as exact zeros
       float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
-      for (int v = tid; v < S::NQ32 * TI / 4; v += blockDim.x) {
+      for (int v = tid; v < S::NQ32 * TI / 4; v += S::NT) {
         const int q = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
         reinterpret_cast<float4*>(d32)[v] = *reinterpret_cast<const float4*>(&sTflat[sMapS[q] * TI + g4]);
       }
@@ -423,7 +426,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
       // 64-byte runs of 8 records
       constexpr int NW = s16_record_words(M);
       uint32_t* d16 = out.S16 + rec * (int64_t)(NW * TI);
-      for (int v = tid; v < TI * NW / 4; v += blockDim.x) {
+      for (int v = tid; v < TI * NW / 4; v += S::NT) {
         const int tl = v % TI, w4 = v / TI;
         uint32_t w[4];
 #pragma unroll
@@ -485,7 +488,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     }
   }
   if (SYM && !diag) {
-    for (int k = tid; k < TI * FF; k += blockDim.x) {
+    for (int k = tid; k < TI * FF; k += S::NT) {
       const int jl = k / FF;
       if (j0 + jl < N) ffpart[((int64_t)I * N + j0) * FF + k] = (&sfJ[0][0])[k];
     }
