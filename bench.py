@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--serve-max-active", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-graphs", type=int, default=2,
-                    help="CUDA graph mode of the served requests: 2 restart cycles only (default), 1 whole steps, 0 off")
+                    help="CUDA graph mode of the served requests: 2 restart cycles (default), 1 whole steps built "
+                         "at admission, 0 off")
     ap.add_argument("--serve-pack-fibers", type=int, default=0,
                     help="requests of at most this many fibers step together with packed solves (0: off)")
     ap.add_argument("--serve-pack-compare", type=int, default=64,
@@ -650,6 +651,7 @@ def serve_ensemble(args, dist, pack_fibers=None):
     wall_max = dist.max(wall)
     fiber_steps = dist.sum(st["fiber_steps"])
     return {"p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"],
+            "p50_setup_ms": st["p50_setup_ms"], "p99_setup_ms": st["p99_setup_ms"],
             "fiber_steps_per_s": fiber_steps / wall_max, "requests": len(reqs) * dist.world,
             "completed": int(dist.sum(st["completed"])), "failed": int(dist.sum(st["failed"])),
             "steps": int(dist.sum(st["steps"])), "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
@@ -659,7 +661,8 @@ def serve_ensemble(args, dist, pack_fibers=None):
                 "pack_max_ms": st["pack_max_ms"], "pack_mean_members": st["pack_mean_members"]} if pack else {}),
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps 0.01 or 0.005, 5-50 steps, Poisson arrivals; latency = "
-                        "host wall time of one step while others run"}
+                        "host wall time of one step while others run; setup = admission to ready (handle created, "
+                        "step graphs built)"}
 
 
 def direct_leg(args, n=None, integration="analytical", solvers=("direct", "gmres")):

@@ -244,6 +244,20 @@ int rf_set_assembly_variant(rf_handle* h, int variant);
  * use; stage times measured).  mode 0: no graphs.  Stage-by-stage calls
  * (rf_assemble, rf_solve, ...) never use the whole-step graph. */
 int rf_set_cuda_graphs(rf_handle* h, int mode);
+/* Build the whole-step graphs of mode 1 now instead of on a step's second use
+ * (which: 1 the first, Euler, step; 2 the second-order steps; 3 both), so that
+ * no later rf_step pays for a capture and an instantiation (a serving loop
+ * calls it when it admits a request).  Nothing runs on the device.  RF_OK
+ * without building when the handle does not use whole-step graphs (mode 0 or
+ * 2, BiCGSTAB or direct solver, profiling on); a graph that cannot be built
+ * leaves rf_step on direct launches. */
+int rf_prepare_step_graphs(rf_handle* h, int which);
+/* How rf_step waits on the host for its results: 0 (default) polls the
+ * stream, 1 sleeps on a blocking-sync event.  Polling answers a few
+ * microseconds sooner; with many handles stepping from their own threads
+ * (a serving loop) the polling threads take the host cores from the threads
+ * that launch, so the server's handles sleep. */
+int rf_set_host_wait(rf_handle* h, int blocking);
 int rf_matvec_profile(rf_handle* h, int* launches, double* total_ms);
 
 /* Device-pointer entry points (no host copies; pointers are device memory
@@ -292,12 +306,18 @@ typedef struct rf_server_config {
   int max_active;            /* requests running at once on their own handles */
   int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
   int use_cuda_graphs;       /* rf_set_cuda_graphs mode of every request's handle
-                                (default 2: restart cycles only; whole-step graphs cost
-                                a capture and an instantiation per request) */
+                                (default 2: restart cycles; 1: whole-step graphs, built
+                                when the request is admitted, rf_prepare_step_graphs) */
   int pack_max_fibers;       /* requests of at most this many fibers (<= 128, mixed
                                 precision, GMRES, 5 terms, 8x3 quadrature) step together
                                 with packed solves (rf_step_packed); 0: off */
   int pack_max_members;      /* suspensions per pack */
+  int64_t reserve_bytes;     /* device memory taken into the handles' pool when the
+                                server starts (at most hbm_budget_bytes), so that
+                                admitting a large request does not grow the pool while
+                                others step: growing it maps new memory, which holds
+                                up every stream of the device.  Default: a quarter
+                                of the budget; 0: grow on demand */
 } rf_server_config;
 
 typedef struct rf_request_stats {
@@ -306,6 +326,7 @@ typedef struct rf_request_stats {
   double run_ms;        /* admission -> last step done */
   double mean_step_ms;  /* host wall time of rf_step, mean */
   int64_t device_bytes; /* admission estimate */
+  double setup_ms;      /* admission -> ready to step (handle created, graphs built) */
 } rf_request_stats;
 
 typedef struct rf_server_stats {
@@ -322,6 +343,8 @@ typedef struct rf_server_stats {
   int64_t pack_steps;
   double pack_p50_ms, pack_p99_ms, pack_max_ms;
   double pack_mean_members;
+  /* admission -> ready to step, percentiles over completed requests */
+  double p50_setup_ms, p99_setup_ms;
 } rf_server_stats;
 
 /* Device bytes a handle of this configuration and size allocates (an upper
@@ -340,6 +363,10 @@ int rf_server_drain(rf_server* s, double timeout_seconds);
 int rf_server_result(rf_server* s, int64_t request_id, double* pos, double* ori, double* tvel, double* rvel,
                      rf_request_stats* stats);
 int rf_server_get_stats(rf_server* s, rf_server_stats* stats);
+/* Host wall time of each step of a finished request, in step order: copies
+ * min(capacity, steps) values to ms (may be NULL) and the step count to
+ * *count.  RF_E_STATE while the request runs. */
+int rf_server_step_times(rf_server* s, int64_t request_id, double* ms, int capacity, int* count);
 /* Cancels what has not finished, waits for running steps, frees everything. */
 int rf_server_destroy(rf_server* s);
 

@@ -82,7 +82,8 @@ RF_REQ_QUEUED, RF_REQ_RUNNING, RF_REQ_DONE, RF_REQ_FAILED, RF_REQ_CANCELLED = ra
 
 class rf_server_config(ctypes.Structure):
     _fields_ = [("max_active", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_int64), ("use_cuda_graphs", ctypes.c_int),
-                ("pack_max_fibers", ctypes.c_int), ("pack_max_members", ctypes.c_int)]
+                ("pack_max_fibers", ctypes.c_int), ("pack_max_members", ctypes.c_int),
+                ("reserve_bytes", ctypes.c_int64)]
 
 
 class rf_request_stats(ctypes.Structure):
@@ -92,6 +93,7 @@ class rf_request_stats(ctypes.Structure):
         ("run_ms", ctypes.c_double),
         ("mean_step_ms", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
+        ("setup_ms", ctypes.c_double),
     ]
 
 
@@ -113,6 +115,7 @@ class rf_server_stats(ctypes.Structure):
         ("pack_p99_ms", ctypes.c_double),
         ("pack_max_ms", ctypes.c_double),
         ("pack_mean_members", ctypes.c_double),
+        ("p50_setup_ms", ctypes.c_double), ("p99_setup_ms", ctypes.c_double),
     ]
 
 
@@ -149,6 +152,8 @@ SIGNATURES = {
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_cuda_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_assembly_variant": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_prepare_step_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_set_host_wait": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_autotune": (ctypes.c_int, [_H, ctypes.POINTER(rf_tune_report)]),
     "rf_matvec_profile": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "rf_checkpoint_bytes": (ctypes.c_int64, [_H]),
@@ -165,6 +170,7 @@ SIGNATURES = {
     "rf_server_drain": (ctypes.c_int, [_S, ctypes.c_double]),
     "rf_server_result": (ctypes.c_int, [_S, ctypes.c_int64, _P, _P, _P, _P, ctypes.POINTER(rf_request_stats)]),
     "rf_server_get_stats": (ctypes.c_int, [_S, ctypes.POINTER(rf_server_stats)]),
+    "rf_server_step_times": (ctypes.c_int, [_S, ctypes.c_int64, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "rf_server_destroy": (ctypes.c_int, [_S]),
     "rf_debug_set_device_wait_limit": (ctypes.c_int, [ctypes.c_int64]),
     "rf_debug_fail_allocation_after": (ctypes.c_int, [ctypes.c_int]),

@@ -252,6 +252,8 @@ struct rf_handle {
   float* F = nullptr;        // force terms sum_j T^{ij}[k][P0] F/2
   float* svpart = nullptr;   // structured velocity partials
   int* vflag = nullptr;      // set when a velocity is not finite
+  int* host_vflag = nullptr; // its page-locked host copy (a pageable target would make the read synchronous)
+  cudaEvent_t wait_ev = nullptr;   // blocking-sync event of the step's host waits (rf_set_host_wait); null polls
   // Krylov scratch
   float* V = nullptr;
   float* ypart = nullptr;
@@ -353,12 +355,14 @@ struct rf_handle {
     pp.put(host_ctl, sizeof(GmresCtl));
     pp.put(host_bctl, sizeof(BicgCtl));
     pp.put(host_ir_norm, sizeof(double));
+    pp.put(host_vflag, sizeof(int));
     pp.put(lu.host_ipiv, (size_t)lu.R * sizeof(int));
     pp.put(lu.host_perm, (size_t)lu.R * sizeof(int));
     if (pooled) pools_release();
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (order_ev) cudaEventDestroy(order_ev);
+    if (wait_ev) cudaEventDestroy(wait_ev);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -589,6 +593,7 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   if (!rc) rc = h->alloc((void**)&h->fw, (size_t)N * h->Q * sizeof(float4));
   if (!rc) rc = h->alloc((void**)&h->vpart, (size_t)velocity_chunks(N) * N * 6 * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->vflag, sizeof(int));
+  if (!rc && !h->dry && !(h->host_vflag = static_cast<int*>(pinned_pool().get(sizeof(int))))) rc = RF_E_OOM;
   return rc;
 }
 
@@ -704,6 +709,7 @@ static GmresSetup gmres_setup(rf_handle* h) {
   s.ctl = h->ctl;
   s.host_ctl = h->host_ctl;
   s.coop_blocks = h->coop_blocks;
+  s.wait_ev = h->wait_ev;
   // per-matvec profiling events are recorded by the callbacks, so profiling runs
   // launch every cycle directly; otherwise the cycles replay captured graphs
   // (an injected device-wait limit is a kernel argument: no capture or replay then)
@@ -999,6 +1005,18 @@ static int build_step_graph(rf_handle* h, int first_step, rf_handle::StepGraph* 
   return RF_OK;
 }
 
+int rf_prepare_step_graphs(rf_handle* h, int which) {
+  if (!h || which < 0 || which > 3) return RF_E_INPUT;
+  if (!step_graph_eligible(h)) return RF_OK;
+  for (int first = 0; first < 2; ++first) {
+    if (!(which & (first ? 1 : 2))) continue;
+    rf_handle::StepGraph& g = h->step_graph[first];
+    if (g.state == 1 || g.state == -1) continue;
+    build_step_graph(h, first, &g);   // state 1, or -1: direct launches
+  }
+  return RF_OK;
+}
+
 int rf_update_fibers(rf_handle* h, int first_step) {
   if (!h) return RF_E_INPUT;
   if (!h->vel_fresh) { set_last_error_str("rf_update_fibers before rf_update_velocities"); return RF_E_STATE; }
@@ -1018,10 +1036,10 @@ static int run_step_graph(rf_handle* h, const rf_handle::StepGraph& g) {
   RF_CUDA_TRY(cudaEventRecord(h->ev[0], h->st));
   RF_CUDA_TRY(cudaGraphLaunch(g.exec, h->st));
   RF_CUDA_TRY(cudaEventRecord(h->ev[7], h->st));
-  int vbad = 0;
   RF_CUDA_TRY(cudaMemcpyAsync(h->host_ctl, h->ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, h->st));
-  RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  RF_CUDA_TRY(cudaMemcpyAsync(h->host_vflag, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(host_wait(h->st, h->wait_ev));
+  const int vbad = *h->host_vflag;
   const GmresCtl c = *h->host_ctl;
   GmresResult res;
   const int rc = gmres_result_from_ctl(c, h->mixed, &res);
@@ -1088,9 +1106,9 @@ int rf_step(rf_handle* h, int t) {
     Range r("update_fibers");
     RF_TRY(rf_update_fibers(h, t == 0));
   }
-  int vbad = 0;
-  RF_CUDA_TRY(cudaMemcpyAsync(&vbad, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
-  RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+  RF_CUDA_TRY(cudaMemcpyAsync(h->host_vflag, h->vflag, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  RF_CUDA_TRY(host_wait(h->st, h->wait_ev));
+  const int vbad = *h->host_vflag;
   if (vbad) {
     set_last_error_str("non-finite velocity");
     return RF_E_NAN;
@@ -1782,6 +1800,18 @@ int rf_set_assembly_variant(rf_handle* h, int variant) {
   if (!h || variant < 0 || variant >= kAsmVariants) return RF_E_INPUT;
   if (h->asm_variant != variant) h->release_step_graphs();   // captured steps hold the old kernel
   h->asm_variant = variant;
+  return RF_OK;
+}
+
+int rf_set_host_wait(rf_handle* h, int blocking) {
+  if (!h || blocking < 0 || blocking > 1) return RF_E_INPUT;
+  if (blocking && !h->wait_ev)
+    RF_CUDA_TRY(cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+  if (!blocking && h->wait_ev) {
+    RF_CUDA_TRY(cudaStreamSynchronize(h->st));
+    RF_CUDA_TRY(cudaEventDestroy(h->wait_ev));
+    h->wait_ev = nullptr;
+  }
   return RF_OK;
 }
 

@@ -63,6 +63,17 @@ int64_t device_wait_limit();
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Host wait for the work queued on st so far.  ev null: cudaStreamSynchronize
+// (the thread polls); else ev, an event created with cudaEventBlockingSync, is
+// recorded and waited on, which puts the thread to sleep until the work is
+// done -- many threads waiting at once (a serving loop) then leave the host
+// cores to the threads that launch.
+inline cudaError_t host_wait(cudaStream_t st, cudaEvent_t ev) {
+  if (!ev) return cudaStreamSynchronize(st);
+  const cudaError_t e = cudaEventRecord(ev, st);
+  return e != cudaSuccess ? e : cudaEventSynchronize(ev);
+}
+
 // Symmetric 3x3 stored as (11, 22, 33, 12, 13, 23) -- the order of
 // fortran/compute_inner_integral_numerically.incl:179-184.
 __device__ __forceinline__ float sym_get(const float* s6, int a, int b) {

@@ -550,7 +550,7 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   };
   auto read_ctl = [&]() -> int {
     RF_CUDA_TRY(cudaMemcpyAsync(s.host_ctl, s.ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, st));
-    RF_CUDA_TRY(cudaStreamSynchronize(st));
+    RF_CUDA_TRY(host_wait(st, s.wait_ev));
     h = *s.host_ctl;
     return RF_OK;
   };

@@ -70,6 +70,7 @@ struct GmresSetup {
   GmresCtl* host_ctl;  // pinned host
   int coop_blocks;
   GmresGraphCache* graphs = nullptr;   // null: launch every cycle directly
+  cudaEvent_t wait_ev = nullptr;       // host waits (host_wait): null polls
 };
 
 struct GmresResult {

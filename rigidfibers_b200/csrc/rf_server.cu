@@ -47,7 +47,7 @@ struct Request {
   int error = RF_OK;
   int steps_done = 0;
   bool cancel = false;
-  double t_submit = 0, t_start = 0, t_end = 0;
+  double t_submit = 0, t_start = 0, t_ready = 0, t_end = 0;   // ready: handle and graphs built
   std::vector<double> step_ms;
   bool packed = false;                // stepped by the pack worker
   std::thread worker;
@@ -67,6 +67,9 @@ struct rf_server {
   rf_server_config cfg;
   int device = 0;
   std::mutex mu;
+  std::mutex setup_mu;               // handle creation and graph building: at most setup_lanes at once
+  std::condition_variable setup_cv;
+  int setup_lanes = 1, setup_busy = 0;
   std::condition_variable cv;        // dispatcher wake-up
   std::condition_variable done_cv;   // waiters
   std::deque<int64_t> queue;
@@ -97,16 +100,49 @@ static double now_s() {
 
 static void finish_locked(rf_server* s, Request* r, int rc, const std::vector<double>& lat);
 
+// one of the server's setup lanes, held while a request is set up
+struct SetupLane {
+  rf_server* s;
+  explicit SetupLane(rf_server* srv) : s(srv) {
+    std::unique_lock<std::mutex> lk(s->setup_mu);
+    s->setup_cv.wait(lk, [&] { return s->setup_busy < s->setup_lanes; });
+    s->setup_busy += 1;
+  }
+  ~SetupLane() {
+    std::lock_guard<std::mutex> lk(s->setup_mu);
+    s->setup_busy -= 1;
+    s->setup_cv.notify_one();
+  }
+};
+
 static void run_request(rf_server* s, Request* r) {
   cudaSetDevice(s->device);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
   rf::set_coop_block_cap(std::max(1, sms / s->cfg.max_active));
   rf_handle* h = nullptr;
-  int rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
+  int rc;
+  {
+    // A few requests at a time create their handles and build their step
+    // graphs: the driver serialises stream, event and graph creation
+    // internally, and sixteen threads doing it at once each took ~100x longer
+    // than one alone (while slowing the others' launches).
+    SetupLane lane(s);
+    rc = rf_create(&r->cfg, r->N, r->pos.data(), r->ori.data(), &h);
+    if (rc == RF_OK) {
+      rf_set_host_wait(h, 1);
+      rf_set_cuda_graphs(h, s->cfg.use_cuda_graphs);
+      // whole-step graphs are built now, before the first step (a step then
+      // is one graph launch from the first on)
+      if (s->cfg.use_cuda_graphs == 1) rf_prepare_step_graphs(h, r->nsteps > 1 ? 3 : 1);
+    }
+  }
   std::vector<double> lat;
   if (rc == RF_OK) {
-    rf_set_cuda_graphs(h, s->cfg.use_cuda_graphs);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      r->t_ready = now_s();
+    }
     for (int t = 0; t < r->nsteps; ++t) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -193,6 +229,10 @@ static void pack_loop(rf_server* s) {
         finish_locked(s, r, mrc[q], {});
         s->packed_active -= 1;
         continue;
+      }
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->t_ready = now_s();
       }
       mem.push_back({r, made[q], 0, {}});
     }
@@ -319,25 +359,47 @@ int rf_server_config_default(rf_server_config* c) {
   if (!c) return RF_E_INPUT;
   std::memset(c, 0, sizeof(*c));
   c->max_active = 16;
-  c->use_cuda_graphs = 2;   // restart cycles only: short requests do not repay capturing whole steps
+  // restart cycles only: with sixteen requests sharing the GPU a step waits
+  // mostly for the others' kernels, and building whole-step graphs at every
+  // admission cost more aggregate rate (618k vs 881k fiber-steps/s on the
+  // served ensemble) than it saved in launches
+  c->use_cuda_graphs = 2;
   c->pack_max_fibers = 0;
   c->pack_max_members = 148;
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c->hbm_budget_bytes = (int64_t)(0.8 * (double)fr);
   else c->hbm_budget_bytes = (int64_t)64 << 30;
+  c->reserve_bytes = c->hbm_budget_bytes / 4;
   return RF_OK;
 }
 
 int rf_server_create(const rf_server_config* cfg, rf_server** out) {
   if (!cfg || !out || cfg->max_active < 1 || cfg->hbm_budget_bytes <= 0 || cfg->pack_max_fibers < 0 ||
-      (cfg->pack_max_fibers > 0 && cfg->pack_max_members < 1)) {
-    rf::set_last_error_str("rf_server_create: max_active >= 1, a positive memory budget, pack_max_members >= 1");
+      (cfg->pack_max_fibers > 0 && cfg->pack_max_members < 1) || cfg->reserve_bytes < 0) {
+    rf::set_last_error_str("rf_server_create: max_active >= 1, a positive memory budget, pack_max_members >= 1, "
+                           "reserve_bytes >= 0");
     return RF_E_INPUT;
   }
   rf_server* s = new rf_server();
   s->cfg = *cfg;
+  s->setup_lanes = std::max(1, cfg->max_active / 4);
   cudaGetDevice(&s->device);
   rf::pools_acquire();   // requests' memory stays in the handles' pool between requests
+  const int64_t reserve = std::min(cfg->reserve_bytes, cfg->hbm_budget_bytes);
+  if (reserve > 0) {
+    // one allocation of the reserve, freed at once: the pool keeps it (its
+    // release threshold is at the maximum while a server or handle lives)
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;
+    void* p = nullptr;
+    if (rf::handle_pool(s->device, &pool) == cudaSuccess &&
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+      if (cudaMallocFromPoolAsync(&p, (size_t)reserve, pool, st) == cudaSuccess) cudaFreeAsync(p, st);
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    cudaGetLastError();   // a reserve that does not fit only means growing on demand
+  }
   s->t0 = now_s();
   s->dispatcher = std::thread(dispatch_loop, s);
   if (cfg->pack_max_fibers > 0) s->pack_worker = std::thread(pack_loop, s);
@@ -437,7 +499,20 @@ int rf_server_result(rf_server* s, int64_t id, double* pos, double* ori, double*
     for (double v : r->step_ms) sum += v;
     st->mean_step_ms = r->step_ms.empty() ? 0.0 : sum / r->step_ms.size();
     st->device_bytes = r->bytes;
+    st->setup_ms = r->t_ready > 0 ? 1000.0 * (r->t_ready - r->t_start) : 0.0;
   }
+  return RF_OK;
+}
+
+int rf_server_step_times(rf_server* s, int64_t id, double* ms, int capacity, int* count) {
+  if (!s || !count || capacity < 0) return RF_E_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return RF_E_INPUT;
+  const Request* r = it->second.get();
+  if (r->status != RF_REQ_DONE && r->status != RF_REQ_CANCELLED && r->status != RF_REQ_FAILED) return RF_E_STATE;
+  *count = (int)r->step_ms.size();
+  if (ms) std::copy_n(r->step_ms.begin(), std::min<size_t>((size_t)capacity, r->step_ms.size()), ms);
   return RF_OK;
 }
 
@@ -460,6 +535,16 @@ int rf_server_get_stats(rf_server* s, rf_server_stats* out) {
   out->peak_active = s->peak_active;
   out->peak_bytes = s->peak_bytes;
   int done = 0, failed = 0, queued = 0;
+  std::vector<double> su;
+  for (auto& kv : s->reqs)
+    if (kv.second->status == RF_REQ_DONE && kv.second->t_ready > 0)
+      su.push_back(1000.0 * (kv.second->t_ready - kv.second->t_start));
+  std::sort(su.begin(), su.end());
+  if (!su.empty()) {
+    auto sq = [&](double p) { return su[(size_t)std::min<double>(su.size() - 1, std::ceil(p * su.size()) - 1)]; };
+    out->p50_setup_ms = sq(0.50);
+    out->p99_setup_ms = sq(0.99);
+  }
   for (auto& kv : s->reqs) {
     done += kv.second->status == RF_REQ_DONE;
     failed += kv.second->status == RF_REQ_FAILED;

@@ -36,7 +36,7 @@ def device_bytes(config, number_of_fibers):
 
 class Server:
     def __init__(self, max_active=None, hbm_budget_bytes=None, use_cuda_graphs=None, pack_max_fibers=None,
-                 pack_max_members=None):
+                 pack_max_members=None, reserve_bytes=None):
         self._lib = C.load()
         sc = C.rf_server_config()
         C.check(self._lib.rf_server_config_default(ctypes.byref(sc)), "rf_server_config_default")
@@ -52,6 +52,8 @@ class Server:
             sc.pack_max_fibers = int(pack_max_fibers)
         if pack_max_members is not None:
             sc.pack_max_members = int(pack_max_members)
+        if reserve_bytes is not None:
+            sc.reserve_bytes = int(reserve_bytes)
         self.pack_max_fibers = sc.pack_max_fibers
         self.max_active = sc.max_active
         self.hbm_budget_bytes = sc.hbm_budget_bytes
@@ -96,6 +98,15 @@ class Server:
                 "rf_server_result")
         stats = {k: getattr(st, k) for k, _ in C.rf_request_stats._fields_}
         return out[0], out[1], out[2], out[3], stats
+
+    def step_times(self, rid):
+        """Host wall time of each step of a finished request (ms, step order)."""
+        n = ctypes.c_int()
+        C.check(self._lib.rf_server_step_times(self._s, rid, None, 0, ctypes.byref(n)), "rf_server_step_times")
+        out = np.zeros(n.value, np.float64)
+        C.check(self._lib.rf_server_step_times(self._s, rid, C.ptr(out), n.value, ctypes.byref(n)),
+                "rf_server_step_times")
+        return out
 
     def stats(self):
         st = C.rf_server_stats()

@@ -172,6 +172,11 @@ class Simulation:
         C.check(self._lib.rf_operator_apply(self._h, C.ptr(xx), C.ptr(y), int(which)), "rf_operator_apply")
         return y
 
+    def prepare_step_graphs(self, which=3):
+        """Build the whole-step graphs now (1 first step, 2 second-order steps,
+        3 both; rf_prepare_step_graphs) instead of on a step's second use."""
+        C.check(self._lib.rf_prepare_step_graphs(self._h, int(which)), "rf_prepare_step_graphs")
+
     def set_cuda_graphs(self, mode):
         """0: no CUDA graphs; 1: each rf_step one graph (default); 2: graphs for
         the GMRES restart cycles only, so that the stage times are measured."""

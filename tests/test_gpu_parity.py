@@ -325,6 +325,38 @@ def test_whole_step_graph_equals_direct_launches(prec):
     assert np.array_equal(tv0, tv1) and np.array_equal(rv0, rv1)
 
 
+@pytest.mark.parametrize("prec", ["fp32", "mixed_bf16"])
+def test_prepared_step_graphs_run_every_step(prec):
+    """rf_prepare_step_graphs builds both whole-step graphs before the first
+    step (a serving loop does it at admission): every step, the first one
+    included, is then one graph launch, with the bits and iteration counts of
+    direct launches."""
+    from rigidfibers_b200 import Config, Simulation
+    from rigidfibers_b200 import _capi as C
+    pos, ori = sphere_layout(70, 3.5, seed=31)
+    runs = []
+    for prepared in (False, True):
+        sim = Simulation(Config(precision=prec, refinement_restart=20), pos, ori)
+        lib = C.load()
+        lib.rf_set_cuda_graphs(sim._h, 1 if prepared else 0)
+        if prepared:
+            C.check(lib.rf_prepare_step_graphs(sim._h, 3), "rf_prepare_step_graphs")
+        its, whole = [], 0
+        for t in range(4):
+            sim.step(t)
+            st = sim.stats()
+            its.append(st["iterations"])
+            whole += st["graph_replays"] == 1 and st["ms_solve_system"] == 0.0
+        runs.append((sim.state(), sim.velocities(), its, whole))
+        sim.close()
+    (p0, o0), (tv0, rv0), it0, w0 = runs[0]
+    (p1, o1), (tv1, rv1), it1, w1 = runs[1]
+    assert w0 == 0 and w1 == 4
+    assert it0 == it1
+    assert np.array_equal(p0, p1) and np.array_equal(o0, o1)
+    assert np.array_equal(tv0, tv1) and np.array_equal(rv0, rv1)
+
+
 @pytest.mark.parametrize("n", [100, 300, 600])
 def test_gmres_iterations_match_oracle_over_three_steps(n):
     """The plain FP32 path's GMRES(10) (tol 1e-5, x0 = 0) against the oracle's
