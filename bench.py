@@ -210,13 +210,16 @@ NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 NOMINAL_TF32_TFLOPS = 1100.0
 
 # Flops the structured assembly kernel k_assemble_pairs<5,24,FP16,numerical>
-# executes per unordered fiber pair, from one ncu capture of that kernel at
-# N=1000 (499,500 pairs): thread instructions FFMA 295 M x 2 + FMUL 77 M +
-# FADD 68 M warp-instructions x 32 lanes = 23.5 GFLOP.  The kernel evaluates
-# the Stokeslet once per unordered pair and folds mirror quadrature points,
-# so this is what its FP32 pipes actually do; the reference algorithm counts
-# 2 x 67,923 for the same pair.
-ASM_EXEC_FLOPS_PER_PAIR = (295e6 * 2 + 77e6 + 68e6) * 32 / 499500.0
+# executes per unordered fiber pair, from one ncu capture of its scalar variant
+# at N=1000 (499,500 pairs): thread instructions FFMA 7.15 G x 2 + FMUL 1.69 G
+# + FADD 1.92 G = 17.9 GFLOP.  The kernel evaluates the Stokeslet once per
+# unordered pair, folds mirror quadrature points and contracts four scalar
+# moments per point, so this is what its FP32 pipes actually do; the
+# reference algorithm counts 2 x 67,923 for the same pair.  The packed
+# (f32x2) variant executes the same flops in fewer instructions.
+ASM_EXEC_FLOPS_PER_PAIR = (7.15e9 * 2 + 1.69e9 + 1.92e9) / 499500.0
+# the same capture: 78.5 % of the issue slots busy, FMA pipe 56 %, DRAM 12 %
+ASM_BOUND = "FP32 instruction issue (ncu, N=1000: 78.5 % of issue slots busy, FMA pipe 56 %, DRAM 12 %)"
 
 
 def asm_flops_per_ordered_pair(M=5, Q=24):
@@ -243,6 +246,7 @@ def kernel_rooflines(N, head, hbm, mixed, direct=None):
                         "achieved_tflops": exec_flops / t_asm / 1e12 if t_asm else None,
                         "peak_tflops": NOMINAL_FP32_TFLOPS, "peak_kind": "nominal FP32 SIMT",
                         "frac": exec_flops / t_asm / 1e12 / NOMINAL_FP32_TFLOPS if t_asm else None,
+                        "bound": ASM_BOUND,
                         "reference_flops_per_ordered_pair": asm_flops_per_ordered_pair()}}
     iters = head["iters"] / steps
     if mixed:

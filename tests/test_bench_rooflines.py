@@ -23,7 +23,9 @@ def test_kernel_rooflines_of_a_mixed_step():
     k = bench.kernel_rooflines(N, head, hbm, True, {"fibers": 2000, "direct": {"tflops": 28.0}})
     pairs = N * (N - 1) / 2
     # executed flops per unordered pair from the kernel's instruction mix
-    per_pair = (295e6 * 2 + 77e6 + 68e6) * 32 / 499500
+    # (thread instructions FFMA 7.15 G, FMUL 1.69 G, FADD 1.92 G for 499,500 pairs)
+    per_pair = (7.15e9 * 2 + 1.69e9 + 1.92e9) / 499500
+    assert 35000 < per_pair < 37000
     assert abs(bench.ASM_EXEC_FLOPS_PER_PAIR - per_pair) < 1e-9
     flops = per_pair * pairs
     assert abs(k["assembly"]["achieved_tflops"] - flops / 11.2e-3 / 1e12) < 1e-6
