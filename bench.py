@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--radius", type=float, default=18.0)
     ap.add_argument("--precision", default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32-path", action="store_true",
+                    help="skip the plain FP32 comparison legs (the dense matrix of large N does not fit beside)")
     ap.add_argument("--no-error-leg", action="store_true",
                     help="skip the step errors against the FP64 reference at the benchmark configurations")
     ap.add_argument("--reference-cap-s", type=float, default=1500.0,
@@ -733,7 +735,7 @@ def run_ours(args, dist):
     e2e_value = total_fiber_steps / e2e_s
 
     comparison = matched = None
-    if precision != "fp32":
+    if precision != "fp32" and not args.no_fp32_path:
         comparison, plain = _plain(args, dist, total_fiber_steps, Config(precision="fp32"))
         # the mixed path runs mixed_restart Arnoldi steps between corrections;
         # FP32 GMRES with the same restart length separates precision from restart

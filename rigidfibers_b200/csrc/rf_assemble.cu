@@ -334,23 +334,51 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     __syncthreads();
 
     // ---- phase 2: T[ki][kj][c] = sum_qi W[ki][qi] G[qi][c][kj], folded over qi
-    // lanes (col, tl), tl fastest; column col = kj * 6 + c
-    for (int task = tid; task < TI * NC; task += S::NT) {
-      const int col = task / TI, tl = task % TI;
-      const int kj = col / 6, c = col % 6;
-      const float* gp = &sG[col][tl];
-      float acc[K1];
+    // lanes (col, tl), tl fastest; column col = kj * 6 + c.  P2: a lane takes
+    // columns col and col + NC/2 in the two lanes of packed FP32 instructions
+    // (lo - hi as fma(hi, -1, lo): the same rounding as the scalar subtraction)
+    if constexpr (P2 && NC % 2 == 0) {
+      constexpr int NC2 = NC / 2;
+      for (int task = tid; task < TI * NC2; task += S::NT) {
+        const int col = task / TI, tl = task % TI;
+        const float* ga = &sG[col][tl];
+        const float* gb = &sG[col + NC2][tl];
+        float2 acc[K1];
 #pragma unroll
-      for (int k = 0; k < K1; ++k) acc[k] = 0.f;
+        for (int k = 0; k < K1; ++k) acc[k] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int q = 0; q < H; ++q) {
-        const float lo = gp[q * TI], hi = gp[(Q - 1 - q) * TI];
-        const float ev = lo + hi, od = lo - hi;
+        for (int q = 0; q < H; ++q) {
+          const float2 lo = make_float2(ga[q * TI], gb[q * TI]);
+          const float2 hi = make_float2(ga[(Q - 1 - q) * TI], gb[(Q - 1 - q) * TI]);
+          const float2 ev = __fadd2_rn(lo, hi), od = __ffma2_rn(hi, make_float2(-1.f, -1.f), lo);
 #pragma unroll
-        for (int k = 0; k < K1; ++k) acc[k] = fmaf((k & 1) ? od : ev, tab.W[k][q], acc[k]);
+          for (int k = 0; k < K1; ++k) acc[k] = __ffma2_rn((k & 1) ? od : ev, tab.W2[k][q], acc[k]);
+        }
+        const int kja = col / 6, ca = col % 6, kjb = (col + NC2) / 6, cb = (col + NC2) % 6;
+#pragma unroll
+        for (int k = 0; k < K1; ++k) {
+          tv(tl, (k * K1 + kja) * 6 + ca) = acc[k].x;
+          tv(tl, (k * K1 + kjb) * 6 + cb) = acc[k].y;
+        }
       }
+    } else {
+      for (int task = tid; task < TI * NC; task += S::NT) {
+        const int col = task / TI, tl = task % TI;
+        const int kj = col / 6, c = col % 6;
+        const float* gp = &sG[col][tl];
+        float acc[K1];
 #pragma unroll
-      for (int k = 0; k < K1; ++k) tv(tl, (k * K1 + kj) * 6 + c) = acc[k];
+        for (int k = 0; k < K1; ++k) acc[k] = 0.f;
+#pragma unroll
+        for (int q = 0; q < H; ++q) {
+          const float lo = gp[q * TI], hi = gp[(Q - 1 - q) * TI];
+          const float ev = __fadd_rn(lo, hi), od = __fsub_rn(lo, hi);
+#pragma unroll
+          for (int k = 0; k < K1; ++k) acc[k] = __fmaf_rn((k & 1) ? od : ev, tab.W[k][q], acc[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < K1; ++k) tv(tl, (k * K1 + kj) * 6 + c) = acc[k];
+      }
     }
     __syncthreads();
 
