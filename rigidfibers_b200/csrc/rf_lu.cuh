@@ -32,7 +32,7 @@ struct LuSetup {
   int panel_blocks = 0;   // blocks of the shared-memory panel kernel (0: one per SM)
   // tensor-core factorization without row exchanges (used when it gives the
   // factors of partial pivoting; null buffers: the pivoted path only)
-  float* LT = nullptr;     // lu_tc_lt_floats(R): row-major copy of two panels' L21
+  float* LT = nullptr;     // lu_tc_lt_floats(R): row-major copy of one pass's panels' L21
   float* inv = nullptr;    // lu_tc_inv_floats(): the diagonal block's L^-1 and U^-T
   int* flags = nullptr;    // 2: largest |l| (float bits), status
   float* sinv = nullptr;   // lu_tc_sinv_floats(R): each diagonal block's L^-1 and U^-1 (triangular solves)

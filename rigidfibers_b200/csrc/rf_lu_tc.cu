@@ -16,18 +16,18 @@
 // within kStaticPivotLimit; the caller's FP64-residual refinement then
 // decides, and refactors with partial pivoting if it does not converge.
 //
-// Per pair of 128-column panels k, k2 = k + 128 (Golub & Van Loan, the
-// right-looking blocked LU, with the second panel's update looked ahead so the
-// trailing matrix is read and written once per 256 columns):
-//   diag(k):    LU of the 128 x 128 diagonal block in shared memory (one CTA),
-//               and the explicit inverses U11^-1, L11^-1 of its factors
-//   L21(k):     L21 = A21 U11^-1                                 (GEMM, K = 128)
-//   U12(k):     U12 = L11^-1 A12                                 (GEMM, K = 128)
-//   A(:, k2:k2+128) -= L21 U12 on the next panel's columns       (GEMM, K = 128)
-//   diag(k2), L21(k2)
-//   rows k2..k2+128 of the columns right of it -= L21 U12       (GEMM, K = 128)
-//   U12(k2)
-//   A22 -= [L21(k) L21(k2)] [U12(k); U12(k2)]                    (GEMM, K = 256)
+// Per pass of four 128-column panels k_p = k + 128 p (Golub & Van Loan, the
+// right-looking blocked LU, with the pass's later panels updated by its
+// earlier ones first, so the trailing matrix is read and written once per 512
+// columns):
+//   for p = 0 .. 3:
+//     A(k_p.., k_p:k_p+128) -= [L21(k_0..k_p-1)] [U12(...)]    (GEMM, K = 128 p)
+//     diag(k_p):  LU of the 128 x 128 diagonal block in shared memory (one
+//                 CTA), and the explicit inverses U11^-1, L11^-1 of its factors
+//     L21(k_p):   L21 = A21 U11^-1                             (GEMM, K = 128)
+//     rows k_p..k_p+128 right of the panel -= L21 U12          (GEMM, K = 128 p)
+//     U12(k_p):   U12 = L11^-1 A12                             (GEMM, K = 128)
+//   A22 -= [L21(k_0) .. L21(k_3)] [U12(k_0); ..; U12(k_3)]     (GEMM, K = 512)
 //
 // The GEMM: C (column-major) = or -= A B with A (M x K) and B (K x N) both
 // K-major in shared memory, loaded by TMA (cp.async.bulk.tensor, 128-byte
@@ -62,7 +62,8 @@ constexpr int kTcBM = 128;          // rows per tile (TMEM lanes)
 constexpr int kTcBK = 32;           // k per pipeline stage: 32 floats = one 128-byte swizzle row
 constexpr int kTcStages = 2;
 constexpr int kPanel = 128;         // panel width
-constexpr int kLtCols = 2 * kPanel; // columns of the row-major L21 copy
+constexpr int kPassPanels = 4;                 // panels factored per pass of the trailing update
+constexpr int kLtCols = kPassPanels * kPanel;  // columns of the row-major L21 copy
 constexpr uint64_t kDrainNs = 1000000000ull;
 // largest multiplier of factors kept without row exchanges (bounded growth)
 constexpr float kStaticPivotLimit = 64.f;
@@ -1169,27 +1170,29 @@ int lu_factor_tc(const LuSetup& s, cudaStream_t st, bool* clean, int* launches, 
   auto update = [&](int64_t r0, int64_t r1, int64_t c0, int64_t kk, int K, int lt_col) -> int {
     return launch_update<256>(mp.lt, mp.mat_b256, mp.mat_c32, up_args(r0, r1, c0, R, kk, K, lt_col), sms, st);
   };
-  auto update_cols = [&](int64_t r0, int64_t c0, int64_t c1, int64_t kk) -> int {
-    return launch_update<128>(mp.lt, mp.mat_b128, mp.mat_c32, up_args(r0, R, c0, c1, kk, kPanel, 0), sms, st);
+  auto update_cols = [&](int64_t r0, int64_t c0, int64_t c1, int64_t kk, int K) -> int {
+    return launch_update<128>(mp.lt, mp.mat_b128, mp.mat_c32, up_args(r0, R, c0, c1, kk, K, 0), sms, st);
   };
+  // One pass: panels p = 0 .. kPassPanels-1 at columns k + 128 p, each brought
+  // up to date by the pass's earlier panels (its columns below it, K = 128 p)
+  // and factored; the rows of each panel right of it updated the same way and
+  // turned into U12; then the trailing matrix by all the pass's panels at once
+  // (K = 512: C is read and written once per 512 columns of the factorization).
   for (int64_t k = 0; k < R;) {
-    const int w1 = (int)std::min<int64_t>(kPanel, R - k);
-    RF_TRY_RF(panel(k, w1, 0));
-    if (k + w1 >= R) break;
-    RF_TRY_RF(u12(k, w1, k + w1));
-    const int64_t k2 = k + w1;
-    const int w2 = (int)std::min<int64_t>(kPanel, R - k2);
-    // the second panel's columns, all rows below the first panel
-    RF_TRY_RF(update_cols(k2, k2, k2 + w2, k));
-    RF_TRY_RF(panel(k2, w2, kPanel));
-    if (k2 + w2 >= R) break;
-    const int64_t c0 = k2 + w2;
-    // rows of the second panel, columns right of it: the first panel's update
-    RF_TRY_RF(update(k2, k2 + w2, c0, k, kPanel, 0));
-    RF_TRY_RF(u12(k2, w2, c0));
-    // the trailing matrix: both panels at once (K = 256)
-    RF_TRY_RF(update(c0, R, c0, k, 2 * kPanel, 0));
-    k = c0;
+    int64_t end = k;
+    for (int p = 0; p < kPassPanels && end < R; ++p) {
+      const int64_t kk = end;
+      const int w = (int)std::min<int64_t>(kPanel, R - kk);
+      if (p > 0) RF_TRY_RF(update_cols(kk, kk, kk + w, k, kPanel * p));
+      RF_TRY_RF(panel(kk, w, kPanel * p));
+      end = kk + w;
+      if (end >= R) break;
+      if (p > 0) RF_TRY_RF(update(kk, kk + w, end, k, kPanel * p, 0));
+      RF_TRY_RF(u12(kk, w, end));
+    }
+    if (end >= R) break;
+    RF_TRY_RF(update(end, R, end, k, (int)(end - k), 0));
+    k = end;
   }
   unsigned int h[2] = {0, 0};
   RF_CUDA_TRY(cudaMemcpyAsync(h, s.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
