@@ -87,7 +87,8 @@ typedef struct rf_config {
                                                    ||b - A x|| / ||b|| */
   int refinement_max_iterations;
   int refinement_restart;                       /* mixed precision: Arnoldi steps between
-                                                   FP64 residual corrections; 0 = gmres_restart */
+                                                   FP64 residual corrections (default 20);
+                                                   0 = gmres_restart */
 } rf_config;
 
 typedef struct rf_stats {

@@ -441,7 +441,9 @@ int rf_config_default(rf_config* c) {
   c->velocity_integration = -1;
   c->refinement_tolerance = 1e-6;
   c->refinement_max_iterations = 20;
-  c->refinement_restart = 0;
+  // N=4000, FP16 blocks: 24.3 ms per step with 10 Arnoldi steps between
+  // corrections (3.2 corrections, 26.8 iterations), 21.2 ms with 20, 21.3 with 30
+  c->refinement_restart = 20;
   return RF_OK;
 }
 

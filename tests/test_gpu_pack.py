@@ -143,7 +143,7 @@ def test_packed_solve_refuses_what_it_does_not_take():
     with pytest.raises(C.RigidFibersError) as e:
         solve_packed([fresh])
     assert e.value.status == C.RF_E_STATE
-    m10 = _sim(pos, ori, precision="mixed_bf16")
+    m10 = _sim(pos, ori, precision="mixed_bf16", refinement_restart=10)
     m20 = _sim(pos, ori, precision="mixed_bf16", refinement_restart=20)
     m10.assembleSystem()
     m20.assembleSystem()
