@@ -641,6 +641,7 @@ def serve_ensemble(args, dist, pack_fibers=None):
     gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
     dist.barrier()
     pack = args.serve_pack_fibers if pack_fibers is None else pack_fibers
+    ids = []
     with Server(max_active=args.serve_max_active, use_cuda_graphs=args.serve_graphs, pack_max_fibers=pack) as srv:
         t0 = time.perf_counter()
         due = t0
@@ -649,10 +650,20 @@ def serve_ensemble(args, dist, pack_fibers=None):
             delay = due - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            srv.submit(c, p, o, r["nsteps"])
+            ids.append(srv.submit(c, p, o, r["nsteps"]))
         srv.drain()
         wall = time.perf_counter() - t0
         st = srv.stats()
+        # per-step latencies by request size (the mix spans 16..1000 fibers, so
+        # the overall tail is mostly the large requests' steps)
+        by_size = {}
+        for r, rid in zip(reqs, ids):
+            lo = next(b for b in (512, 256, 128, 64, 16) if r["n"] >= b)
+            by_size.setdefault(lo, []).extend(srv.step_times(rid).tolist())
+        size_classes = {"%d-%d" % (lo, {16: 63, 64: 127, 128: 255, 256: 511, 512: 1000}[lo]):
+                        {"steps": len(v), "p50_step_ms": float(np.percentile(v, 50)),
+                         "p99_step_ms": float(np.percentile(v, 99))}
+                        for lo, v in sorted(by_size.items()) if v}
     dist.barrier()
     wall_max = dist.max(wall)
     fiber_steps = dist.sum(st["fiber_steps"])
@@ -665,6 +676,7 @@ def serve_ensemble(args, dist, pack_fibers=None):
             "cuda_graph_mode": args.serve_graphs, "pack_max_fibers": pack,
             **({"pack_steps": st["pack_steps"], "pack_p50_ms": st["pack_p50_ms"], "pack_p99_ms": st["pack_p99_ms"],
                 "pack_max_ms": st["pack_max_ms"], "pack_mean_members": st["pack_mean_members"]} if pack else {}),
+            "by_size": size_classes,
             "peak_device_bytes": st["peak_bytes"], "storage": "mixed_bf16",
             "workload": "N log-uniform in [16, 1000], eps 0.01 or 0.005, 5-50 steps, Poisson arrivals; latency = "
                         "host wall time of one step while others run; setup = admission to ready (handle created, "
