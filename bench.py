@@ -741,13 +741,17 @@ def run_ours(args, dist):
     R = 15 * N
     precision = "mixed_fp16" if args.precision == "auto" else args.precision
     cfg = Config(precision=precision, refinement_restart=args.mixed_restart)
+    if precision == "matrix_free":
+        # the FP32 path's GMRES with the mixed path's restart length (GMRES(10)
+        # stalls on the largest systems)
+        cfg = Config(precision=precision, gmres_restart=args.mixed_restart or 10)
     head = time_path(args, dist, cfg, pos, ori, clocks=Clocks(dist.local))
     ms_max, total_fiber_steps, value = whole_job_rate(dist, head["ms"], N * args.steps)
     e2e_s, e2e_iters, ck_bytes = e2e_path(args, dist, cfg, pos, ori)
     e2e_value = total_fiber_steps / e2e_s
 
     comparison = matched = None
-    if precision != "fp32" and not args.no_fp32_path:
+    if precision not in ("fp32", "matrix_free") and not args.no_fp32_path:
         comparison, plain = _plain(args, dist, total_fiber_steps, Config(precision="fp32"))
         # the mixed path runs mixed_restart Arnoldi steps between corrections;
         # FP32 GMRES with the same restart length separates precision from restart
@@ -757,9 +761,14 @@ def run_ours(args, dist):
     hbm, peak_kind = peaks()
     mvn = max(head["mv_launches"], 1)
     mv_avg_ms = head["mv_ms"] / mvn
+    mfree = precision == "matrix_free"
     if precision == "fp32":
         kernel = "k_gemv_cm_f32 (dense FP32 column-major matvec, GMRES)"
         bytes_per_matvec = 4.0 * R * R
+    elif mfree:
+        kernel = ("k_assemble_pairs<5,24,apply> + k_sum_parts + k_struct_finalize (matrix-free product: the pair "
+                  "blocks recomputed and applied, nothing read but the fiber state and x)")
+        bytes_per_matvec = 0.0
     else:
         kernel = ("k_struct_z16_bulk<5> + k_sum_parts + k_struct_finalize (16-bit structured matvec, "
                   "TMA bulk-copy pipeline, GMRES)")
@@ -770,7 +779,7 @@ def run_ours(args, dist):
     # unordered pairs: 304-byte records for 300 algorithmic bytes, x, partial
     # rows), scaled by the pairs one launch processes; not captured for the
     # dense FP32 kernel
-    traffic = 357.4e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision != "fp32" else None
+    traffic = 357.4e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision not in ("fp32", "matrix_free") else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
             "kernel": kernel, "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
@@ -778,11 +787,19 @@ def run_ours(args, dist):
             "launches": head["mv_launches"], "share_of_step_time": head["mv_ms"] / head["ms"] if head["ms"] else None,
             "measured_in": "a profiled pass of the same K steps after the timed ones (CUDA events around each matvec "
                            "launch on the handle's stream; per-launch events rule out graph replay)"}
+    if mfree:
+        # the product recomputes every pair block: FP32 issue-bound like the assembly
+        fl = ASM_EXEC_FLOPS_PER_PAIR * N * (N - 1) / 2
+        ach = fl / (mv_avg_ms / 1000.0) / 1e12 if head["mv_launches"] else None
+        roof.update({"bound": "fp32", "achieved": ach, "peak": NOMINAL_FP32_TFLOPS, "unit": "TFLOP/s",
+                     "frac": ach / NOMINAL_FP32_TFLOPS if ach else None, "peak_kind": "nominal FP32 SIMT",
+                     "algorithmic_flops_per_launch": fl})
     out = {
         "metric": METRIC, "value": value, "unit": "fiber-steps/s", "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" if precision == "fp32" else "%s storage, f32 accumulate, f64 refinement" % precision[6:],
+        "dtype": "f32" if precision in ("fp32", "matrix_free") else
+                 "%s storage, f32 accumulate, f64 refinement" % precision[6:],
         "data": "synthetic",
         "config": {"workload": workload_name(args), "fibers": N, "radius": args.radius, "precision": precision,
                    "parallelism": "replicas x%d" % dist.world,
@@ -808,7 +825,8 @@ def run_ours(args, dist):
         if args.direct_large_fibers > 0:
             out["direct_solver_precision_config"] = direct_leg(args, args.direct_large_fibers, "numerical", ("direct",))
     head["steps"] = args.steps
-    out["kernels"] = kernel_rooflines(N, head, hbm, precision != "fp32", out.get("direct_solver"))
+    if not mfree:
+        out["kernels"] = kernel_rooflines(N, head, hbm, precision != "fp32", out.get("direct_solver"))
     if dist.rank == 0 and not args.no_cpu_baseline:
         res = cpu_steps(pos, ori, 1, untimed=0)
         out["cpu_baseline"] = {"value": res["value"], "unit": "fiber-steps/s", "cores": res["cores"],

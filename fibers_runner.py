@@ -13,7 +13,7 @@ recompilation: N, M, Q, the solver and the integration are runtime values):
 --magma selects the direct solver (the reference called MAGMA's sgesv).
 --D1/--D2/--D3 chose a CUDA thread mapping of the reference's assembly; they
 are accepted for compatibility and all run the same pair-tile kernel.
-Extra options of this build: --precision {fp32,mixed_fp16,mixed_bf16},
+Extra options of this build: --precision {fp32,mixed_fp16,mixed_bf16,matrix_free},
 --velocity-integration {same,numerical,analytical}, --output DIR.
 
 Outputs (same formats as the reference):
@@ -281,7 +281,7 @@ def build_parser():
         g.add_argument("--D1", action="store_true")
         g.add_argument("--D2", action="store_true")
         g.add_argument("--D3", action="store_true")
-        p.add_argument("--precision", default="fp32", choices=["fp32", "mixed_fp16", "mixed_bf16"])
+        p.add_argument("--precision", default="fp32", choices=["fp32", "mixed_fp16", "mixed_bf16", "matrix_free"])
         p.add_argument("--velocity-integration", default="same", choices=["same", "numerical", "analytical"])
         p.add_argument("--output", default=".", help="directory for the output files")
         if name == "run":

@@ -56,8 +56,12 @@ enum rf_integration { RF_NUMERICAL = 0, RF_ANALYTICAL = 1 };
  *      per unordered fiber pair in FP32 and in 16 bits; the Krylov matvec runs
  *      on the 16-bit copy with FP32 accumulation inside FP64-residual
  *      iterative refinement, with GMRES or BiCGSTAB (not the direct solver;
- *      numerical integration only). */
-enum rf_precision { RF_PREC_FP32 = 0, RF_PREC_MIXED_FP16 = 1, RF_PREC_MIXED_BF16 = 2 };
+ *      numerical integration only).
+ *  RF_PREC_MATRIX_FREE: no matrix stored; every Krylov product recomputes the
+ *      pair blocks (FP32, the assembly's kernel applied to the vector), for
+ *      suspensions whose operator does not fit in device memory (the FP32
+ *      path's GMRES / BiCGSTAB semantics; numerical integration only). */
+enum rf_precision { RF_PREC_FP32 = 0, RF_PREC_MIXED_FP16 = 1, RF_PREC_MIXED_BF16 = 2, RF_PREC_MATRIX_FREE = 3 };
 
 /* Mirrors the reference's .ini keys (tests/config.ini:18-37, read by
  * runner/cuda_runner.py:18-47) plus the runtime choices the reference made

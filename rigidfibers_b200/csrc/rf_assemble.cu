@@ -47,7 +47,9 @@ __device__ __forceinline__ void tile_pair(int64_t L, int& I, int& J) {
   I = (int)(L - j * (j + 1) / 2);
 }
 
-enum AsmMode { kAsmDense = 0, kAsmStructF16 = 1, kAsmStructBF16 = 2 };
+// kAsmApply: nothing stored; the pair blocks are applied to a vector (the
+// matrix-free product) or, without a vector, only the force terms are formed
+enum AsmMode { kAsmDense = 0, kAsmStructF16 = 1, kAsmStructBF16 = 2, kAsmApply = 3 };
 enum AsmInteg { kNumerical = 0, kAnalytical = 1 };
 
 template <int M, int Q>
@@ -93,6 +95,12 @@ struct AsmOut {
   // sensitive to the rounding of its inputs than the quadrature)
   const double4* pos64;
   const double4* ori64;
+  // kAsmApply: z partial rows of T x (null x: force terms only) into
+  // zpart[(assemble tiles + 1) x R]; skip: a device word that, when set,
+  // makes the launch return at once (a converged Krylov solve)
+  const float* x;
+  float* zpart;
+  const int* skip;
 };
 
 // Tile pair L of a suspension of N fibers: numerical, unordered pairs (I <= J)
@@ -253,7 +261,23 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     sD[a][c][2] = (float)(xi.z - xj.z);
   }
   for (int k = tid; k < TI * FF; k += S::NT) (&sfJ[0][0])[k] = 0.f;
-  if constexpr (MODE != kAsmDense) {
+  constexpr bool STRUCT = MODE == kAsmStructF16 || MODE == kAsmStructBF16;
+  constexpr bool APPLY = MODE == kAsmApply;
+  // kAsmApply with a vector applies the blocks; without one it forms the force terms
+  const bool do_apply = APPLY && out.x != nullptr;
+  const bool do_force = !do_apply;
+  constexpr int XW = APPLY ? TI * M3 : 1;
+  __shared__ float sXi[XW], sXj[XW], sZj[XW];   // x rows of the I and J tiles, z_j of this tile's j
+  if constexpr (APPLY) {
+    if (do_apply) {
+      for (int k = tid; k < TI * M3; k += S::NT) {
+        const int f = k / M3, c = k % M3;
+        sXi[k] = i0 + f < N ? out.x[(int64_t)(i0 + f) * M3 + c] : 0.f;
+        sXj[k] = j0 + f < N ? out.x[(int64_t)(j0 + f) * M3 + c] : 0.f;
+      }
+    }
+  }
+  if constexpr (STRUCT) {
     for (int q = tid; q < S::NQ32; q += S::NT) {
       const int c = q % 6, blk = q / 6;
       int row = 0, col = 0;
@@ -285,6 +309,8 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
 
   // force-term accumulator of task (tl, k) = (tid / K1, tid % K1): F_i[k]
   float facc[3] = {0.f, 0.f, 0.f};
+  // kAsmApply: z_i of task (tl, kI) = (tid / M, tid % M) over the tile's j
+  float zacc[3] = {0.f, 0.f, 0.f};
   __syncthreads();
 
   const int jcount = min(TI, N - j0);
@@ -295,7 +321,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     auto sT = [&](int tl, int k, int kj) -> float* { return sTflat + tl * S::TP + (k * K1 + kj) * 6; };
     // structured storage keeps T as [value q][i] (the storage record's own
     // order, so phase 3 is a straight copy); dense keeps [i][value]
-    constexpr bool QT = MODE != kAsmDense;
+    constexpr bool QT = STRUCT;
     auto tv = [&](int tl, int q) -> float& { return QT ? sTflat[q * TI + tl] : sTflat[tl * S::TP + q]; };
     const bool pair_ok = unit_ok && (!diag || (SYM ? il < jl : il != jl));
     // ---- phase 1: G[c][k] = sum_qj K_c(qi,qj) W[k][qj] (numerical, mirror-
@@ -435,6 +461,47 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
               dst[a + b * out.lda] = kJp == 0 ? coef * t3[a] * Qv[b] : coef * (sym_get(T6, a, b) - E * t3[a] * Qv[b]);
         }
       }
+    } else if constexpr (APPLY) {
+      // ---- phase 3 (matrix-free product): z_i[kI] += sum_kJ T(kI+1, kJ+1) x_j[kJ]
+      // for the i side and z_j[kJ] += sum_kI T(kI+1, kJ+1) x_i[kI] for the j side
+      // (each 3x3 block symmetric; blocks of pairs that do not exist are zero)
+      if (do_apply) {
+        if (tid < TI * M) {
+          const int tl = tid / M, kI = tid % M;
+#pragma unroll
+          for (int kJ = 0; kJ < M; ++kJ) {
+            const float* T6 = sT(tl, kI + 1, kJ + 1);
+            const float* xv = &sXj[jl * M3 + 3 * kJ];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              zacc[a] = fmaf(sym_get(T6, a, 0), xv[0], fmaf(sym_get(T6, a, 1), xv[1], fmaf(sym_get(T6, a, 2), xv[2], zacc[a])));
+          }
+        }
+        // j side: lanes (kJ, tl) of whole warps from thread 64, TI-lane sums
+        constexpr int JW = (M * TI + 31) / 32 * 32;
+        static_assert(64 + JW <= S::NT && 32 % TI == 0, "j-side lanes of the matrix-free product");
+        if (tid >= 64 && tid < 64 + JW) {
+          const int u = tid - 64, kJ = u / TI, tl = u % TI;
+          float zs[3] = {0.f, 0.f, 0.f};
+          if (kJ < M) {
+#pragma unroll
+            for (int kI = 0; kI < M; ++kI) {
+              const float* T6 = sT(tl, kI + 1, kJ + 1);
+              const float* xv = &sXi[tl * M3 + 3 * kI];
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                zs[a] = fmaf(sym_get(T6, a, 0), xv[0], fmaf(sym_get(T6, a, 1), xv[1], fmaf(sym_get(T6, a, 2), xv[2], zs[a])));
+            }
+          }
+#pragma unroll
+          for (int o = TI / 2; o > 0; o >>= 1)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) zs[a] += __shfl_xor_sync(0xffffffffu, zs[a], o);
+          if (tl == 0 && kJ < M)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) sZj[jl * M3 + 3 * kJ + a] = zs[a];
+        }
+      }
     } else {
       // ---- phase 3: the pair blocks into structured storage; one j, all i of
       // the tile: [jl][q][tl] is a contiguous run of NQ32*TI floats
@@ -475,7 +542,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
     }
     // ---- phase 3c: force terms F_i[k] += T^{ij}[k][P0] F/2 and
     //      F_j[kj] += T^{ij}[P0][kj] F/2 (F/2 = (0, 0, fz): column z of the block)
-    if (tid < TI * K1) {
+    if (do_force && tid < TI * K1) {
       const int tl = tid / K1, k = tid % K1;
       if (i0 + tl < N && (!diag || (SYM ? tl < jl : tl != jl))) {
         const int q0 = (k * K1 + 0) * 6;
@@ -484,7 +551,7 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
         facc[2] = fmaf(tv(tl, q0 + 2), fz, facc[2]);
       }
     }
-    if (SYM && tid < K1) {
+    if (SYM && do_force && tid < K1) {
       const int kj = tid;
       float s[3] = {0.f, 0.f, 0.f};
       for (int tl = 0; tl < TI; ++tl) {
@@ -500,6 +567,27 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
   }
   __syncthreads();
 
+  if constexpr (APPLY) {
+    if (do_apply) {
+      // partial rows of z: the i side of tile (I, J) to slot J, the j side to
+      // slot I (a diagonal tile's j side to slot T8): every slot of every
+      // fiber is written exactly once per product
+      const int64_t R = (int64_t)M3 * N;
+      const int T8 = (N + TI - 1) / TI;
+      if (tid < TI * M) {
+        const int tl = tid / M, kI = tid % M;
+        if (i0 + tl < N) {
+          float* dst = out.zpart + (int64_t)J * R + (int64_t)(i0 + tl) * M3 + 3 * kI;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) dst[a] = zacc[a];
+        }
+      }
+      float* zj = out.zpart + (int64_t)(diag ? T8 : I) * R + (int64_t)j0 * M3;
+      for (int k = tid; k < TI * M3; k += S::NT)
+        if (j0 + k / M3 < N) zj[k] = sZj[k];
+      return;
+    }
+  }
   // ---- partial force terms: ffpart[X][fiber of Y][k][3] written exactly once
   float* ffpart = out.ffpart;
   if (tid < TI * K1) {
@@ -527,6 +615,7 @@ template <int M, int Q, int MODE, int INTEG, bool P2>
 __global__ void __launch_bounds__(192, INTEG == kNumerical ? 4 : 2)
 k_assemble_pairs(const Tables tab, int N, const float4* __restrict__ pos, const float4* __restrict__ ori,
                  AsmOut out) {
+  if (MODE == kAsmApply && out.skip != nullptr && *out.skip) return;
   int I, J;
   asm_tile_of<Q, INTEG>(N, blockIdx.x, I, J);
   assemble_pair_tile<M, Q, MODE, INTEG, P2>(tab, N, pos, ori, out, I, J);
@@ -675,6 +764,7 @@ static int launch_assemble_mq(const Tables& tab, int N, const float4* pos, const
   } else {
     RF_TRY_RF((launch_pairs<M, Q, MODE, INTEG, false>(tab, N, pos, ori, out, st)));
   }
+  if (MODE == kAsmApply && out.x != nullptr) return RF_OK;   // the product: no force terms
   const int64_t n = (int64_t)N * (M + 1);
   k_force_terms<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 8), 256, 0, st>>>(tab, N, ori, out.ffpart,
                                                                                          (int)T, F, b);
@@ -719,6 +809,18 @@ int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, cons
   out.lda = lda;
   out.ffpart = ffpart;
   return dispatch_assemble<kAsmDense, kAnalytical>(tab, N, pos, ori, out, F, b, 0, st);
+}
+
+int launch_assemble_apply(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                          const float* x, float* zpart, const int* skip, float* ffpart, float* F, float* b,
+                          cudaStream_t st, int variant) {
+  AsmOut out{};
+  out.pos64 = pos64;
+  out.x = x;
+  out.zpart = zpart;
+  out.skip = skip;
+  out.ffpart = ffpart;
+  return dispatch_assemble<kAsmApply, kNumerical>(tab, N, pos, ori, out, F, b, variant, st);
 }
 
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,

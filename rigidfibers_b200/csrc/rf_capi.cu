@@ -240,6 +240,8 @@ struct rf_handle {
   bool vel_fresh = false;    // velocities computed since the last fiber update
   // linear system
   bool mixed = false;        // structured operator + refinement (RF_PREC_MIXED_*)
+  bool mfree = false;        // no operator stored (RF_PREC_MATRIX_FREE)
+  int zparts = 0;            // matrix-free: partial-row slots of a product
   float* A = nullptr;        // dense FP32 (RF_PREC_FP32)
   float* S32 = nullptr;      // structured FP32 blocks (mixed)
   uint32_t* S16 = nullptr;   // structured 16-bit blocks (mixed)
@@ -388,17 +390,18 @@ static int validate_config(const rf_config* c, int N) {
   if (c->solver < 0 || c->solver > 2 || c->integration < 0 || c->integration > 1) {
     set_last_error_str("solver / integration"); return RF_E_INPUT;
   }
-  if (c->precision < RF_PREC_FP32 || c->precision > RF_PREC_MIXED_BF16) { set_last_error_str("precision"); return RF_E_INPUT; }
+  if (c->precision < RF_PREC_FP32 || c->precision > RF_PREC_MATRIX_FREE) { set_last_error_str("precision"); return RF_E_INPUT; }
+  const bool is_mixed = c->precision == RF_PREC_MIXED_FP16 || c->precision == RF_PREC_MIXED_BF16;
   if (c->precision != RF_PREC_FP32 && c->integration != RF_NUMERICAL) {
-    set_last_error_str("mixed precision uses the symmetric pair blocks of numerical integration");
+    set_last_error_str("mixed precision and the matrix-free mode use the symmetric pair blocks of numerical integration");
     return RF_E_UNSUPPORTED;
   }
-  if (c->precision != RF_PREC_FP32 && c->number_of_quadrature_intervals != 8) {
+  if (is_mixed && c->number_of_quadrature_intervals != 8) {
     set_last_error_str("mixed precision is built for 8 quadrature intervals (24 points per fiber)");
     return RF_E_UNSUPPORTED;
   }
   if (c->precision != RF_PREC_FP32 && c->solver == RF_SOLVER_DIRECT) {
-    set_last_error_str("mixed precision refines inside GMRES or BiCGSTAB (the direct solver factors the dense FP32 matrix)");
+    set_last_error_str("the direct solver factors the dense FP32 matrix (RF_PREC_FP32 only)");
     return RF_E_UNSUPPORTED;
   }
   if (c->precision != RF_PREC_FP32 && !(c->refinement_tolerance > 0.0)) {
@@ -516,9 +519,15 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     rc = h->alloc((void**)&h->tv[s], b32);
     if (!rc) rc = h->alloc((void**)&h->rv[s], b32);
   }
-  h->mixed = cfg->precision != RF_PREC_FP32;
+  h->mixed = cfg->precision == RF_PREC_MIXED_FP16 || cfg->precision == RF_PREC_MIXED_BF16;
+  h->mfree = cfg->precision == RF_PREC_MATRIX_FREE;
   const int64_t T16 = ceil_div(N, kStoreTile);
-  if (!h->mixed) {
+  if (h->mfree) {
+    // partial rows of a product: one slot per assembly tile, one for the
+    // diagonal tiles' j side, one for the sum
+    h->zparts = assemble_tiles(h->M, h->Q, N) + 1;
+    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)(h->zparts + 1) * (size_t)R * sizeof(float));
+  } else if (!h->mixed) {
     if (!rc) rc = h->alloc((void**)&h->A, (size_t)h->lda * (size_t)R * sizeof(float));
   } else {
     if (!rc) rc = h->alloc((void**)&h->S32, (size_t)struct_floats32(h->M, N) * sizeof(float));
@@ -536,16 +545,15 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   if (!rc) rc = h->alloc((void**)&h->ffpart, (size_t)tiles * ffn * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->F, ffn * sizeof(float));
   // Krylov
-  const int m = (h->cfg.precision != RF_PREC_FP32 && cfg->refinement_restart > 0) ? cfg->refinement_restart
-                                                                                  : cfg->gmres_restart;
+  const int m = (h->mixed && cfg->refinement_restart > 0) ? cfg->refinement_restart : cfg->gmres_restart;
   h->restart = m;
   h->gemv_plan = plan_dense_gemv(R, h->num_sms);
-  if (h->mixed) h->gemv_plan.splits = 1;  // the structured matvec writes complete rows
+  if (h->mixed || h->mfree) h->gemv_plan.splits = 1;  // these products write complete rows
   h->coop_blocks = krylov_coop_blocks(R, h->num_sms);
   const int64_t ldv = ceil_div(R, 32) * 32;
   if (!rc) rc = h->alloc((void**)&h->V, (size_t)(m + 1) * (size_t)ldv * sizeof(float));
   // room for the most column splits rf_autotune tries
-  h->ypart_floats = (int64_t)(h->mixed ? 1 : plan_dense_gemv(R, h->num_sms, kTuneMaxCtasPerSm).splits) * R;
+  h->ypart_floats = (int64_t)(h->mixed || h->mfree ? 1 : plan_dense_gemv(R, h->num_sms, kTuneMaxCtasPerSm).splits) * R;
   h->ypart_floats = std::max<int64_t>(h->ypart_floats, (int64_t)h->gemv_plan.splits * R);
   if (!rc) rc = h->alloc((void**)&h->ypart, (size_t)h->ypart_floats * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->part, (size_t)3 * h->coop_blocks * (kMaxRestart + 2) * sizeof(double));
@@ -671,6 +679,9 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
 }
 
 static int enqueue_assemble(rf_handle* h) {
+  if (h->mfree)   // the force terms and b (the products recompute the blocks)
+    return launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], nullptr, h->zpart, nullptr,
+                                 h->ffpart, h->F, h->b, h->st, h->asm_variant);
   if (h->mixed)
     return launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
                                       h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st,
@@ -741,6 +752,11 @@ static MatvecFn make_matvec(rf_handle* h, int* launches) {
       const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
       rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
                                 &h->ctl->timeout, st, h->mv_variant);
+      *launches += 2;
+    } else if (h->mfree) {
+      rc = launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], xin, h->zpart, skip,
+                                 h->ffpart, h->F, h->b, st, h->asm_variant);
+      if (rc == RF_OK) rc = launch_parts_finalize(h->tab, h->N, h->ori32, xin, h->zpart, h->zparts, h->ypart, skip, st);
       *launches += 2;
     } else {
       rc = launch_dense_gemv(h->gemv_plan, h->A, h->lda, h->R, xin, h->ypart, skip, st);
@@ -1464,7 +1480,7 @@ static int fetch_vec(rf_handle* h, const float* dev, double* out) {
 int rf_get_system(rf_handle* h, float* A, double* b) {
   if (!h) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("no assembled system"); return RF_E_STATE; }
-  if (A && !h->A) { set_last_error_str("no dense matrix in mixed-precision mode"); return RF_E_STATE; }
+  if (A && !h->A) { set_last_error_str("no dense matrix in the mixed-precision and matrix-free modes"); return RF_E_STATE; }
   if (A) {
     RF_CUDA_TRY(cudaMemcpy2DAsync(A, (size_t)h->R * sizeof(float), h->A, (size_t)h->lda * sizeof(float),
                                   (size_t)h->R * sizeof(float), (size_t)h->R, cudaMemcpyDeviceToHost, h->st));
@@ -1499,7 +1515,7 @@ int rf_number_of_fibers(rf_handle* h) { return h ? h->N : -1; }
 int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
   if (!h || !x || !y || which < 0 || which > 1) return RF_E_INPUT;
   if (!h->assembled) { set_last_error_str("rf_operator_apply before rf_assemble"); return RF_E_STATE; }
-  if (which == 1 && !h->mixed) { set_last_error_str("no 16-bit operator in FP32 mode"); return RF_E_STATE; }
+  if (which == 1 && !h->mixed) { set_last_error_str("no 16-bit operator outside the mixed-precision modes"); return RF_E_STATE; }
   const int64_t R = h->R;
   std::vector<double> hx(x, x + R);
   std::vector<float> hxf(R), hy(R);
@@ -1508,7 +1524,11 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
   float* dxf = h->V;
   float* dy = h->V + ceil_div(R, 32) * 32;
   RF_CUDA_TRY(cudaMemcpyAsync(dxf, hxf.data(), R * sizeof(float), cudaMemcpyHostToDevice, h->st));
-  if (!h->mixed) {
+  if (h->mfree) {
+    RF_TRY(launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], dxf, h->zpart, nullptr,
+                                 h->ffpart, h->F, h->b, h->st, h->asm_variant));
+    RF_TRY(launch_parts_finalize(h->tab, h->N, h->ori32, dxf, h->zpart, h->zparts, dy, nullptr, h->st));
+  } else if (!h->mixed) {
     RF_TRY(launch_dense_gemv(h->gemv_plan, h->A, h->lda, R, dxf, h->ypart, nullptr, h->st));
     RF_TRY(launch_reduce_rows(h->ypart, h->gemv_plan.splits, R, dy, h->st));
   } else if (which == 1) {
@@ -1676,7 +1696,7 @@ static void apply_tuning(rf_handle* h, const rf_tune_report& t) {
   h->asm_variant = t.asm_variant;
   if (h->mixed) {
     h->mv_variant = t.matvec_variant;
-  } else {
+  } else if (!h->mfree) {
     h->gemv_plan = plan_dense_gemv(h->R, h->num_sms, t.gemv_ctas_per_sm);
   }
   h->gmres_graphs.release();   // the captured cycles hold the old launch parameters
@@ -1733,6 +1753,9 @@ int rf_autotune(rf_handle* h, rf_tune_report* out) {
     RF_CUDA_TRY(cudaStreamSynchronize(h->st));
     if (timeout) { set_last_error_str("rf_autotune: a bounded device-side wait timed out"); return RF_E_TIMEOUT; }
     t.gemv_ctas_per_sm = 0;
+  } else if (h->mfree) {
+    t.gemv_ctas_per_sm = 0;
+    t.matvec_variant = 0;
   } else {
     const int cand[4] = {2, 4, 8, 16};
     double best = 1e30;

@@ -42,6 +42,17 @@ int launch_assemble_numerical(const Tables& tab, int N, const float4* pos, const
 int launch_assemble_analytical(const Tables& tab, int N, const float4* pos, const float4* ori,
                                const double4* pos64, const double4* ori64, float* A, int64_t lda, float* ffpart,
                                float* F, float* b, cudaStream_t st);
+// Matrix-free (nothing stored): with x, z partial rows of T x into zpart
+// ((assemble_tiles(M,Q,N) + 1) x R floats, every row written) -- finish the
+// product with launch_parts_finalize; with x null, the force terms F and b
+// (ffpart as for the numerical assembly).  skip as for the structured matvec.
+int launch_assemble_apply(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
+                          const float* x, float* zpart, const int* skip, float* ffpart, float* F, float* b,
+                          cudaStream_t st, int variant = 0);
+// y = x + C z with z the fixed-order sum of nparts partial rows of zpart
+// (zpart holds nparts + 1 rows: the sum goes to row nparts).
+int launch_parts_finalize(const Tables& tab, int N, const float4* ori, const float* x, float* zpart, int nparts,
+                          float* y, const int* skip, cudaStream_t st);
 // Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
                                float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,

@@ -1076,6 +1076,18 @@ int launch_struct_matvec(const Tables& tab, int N, int smode, const float* S32, 
   return RF_OK;
 }
 
+int launch_parts_finalize(const Tables& tab, int N, const float4* ori, const float* x, float* zpart, int nparts,
+                          float* y, const int* skip, cudaStream_t st) {
+  const int64_t n = (int64_t)N * tab.M;
+  const int64_t R = 3 * n;
+  k_sum_parts<float><<<(unsigned)ceil_div(R, 64), 256, 0, st>>>(zpart, nparts, R, zpart + (int64_t)nparts * R, skip);
+  RF_LAUNCH_CHECK();
+  k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(tab, N, ori, x, zpart + (int64_t)nparts * R,
+                                                                        1, nullptr, y, skip);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
 template <int M>
 static int launch_r64_bulk(int N, const float* S32, const double* x, double* zpart, const int* skip, int* err,
                            cudaStream_t st) {

@@ -101,3 +101,37 @@ def test_noalloc_plan_rejects_sizes_beyond_its_scratch():
     splits, cps = ctypes.c_int(), ctypes.c_int64()
     assert lib.rf_debug_noalloc_plan(131073, 148, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_E_INPUT
     assert lib.rf_debug_noalloc_plan(0, 148, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_E_INPUT
+
+
+@pytest.mark.parametrize("field,value", [("integration", 1), ("solver", 2), ("precision", 4)])
+def test_matrix_free_mode_rejects_what_it_does_not_support(field, value):
+    """The matrix-free mode recomputes the symmetric pair blocks of numerical
+    integration inside GMRES or BiCGSTAB: analytical integration and the
+    direct solver (which factors a stored matrix) are refused before the
+    device is touched, as is an unknown precision."""
+    import numpy as np
+    lib = C.load()
+    c = C.rf_config()
+    lib.rf_config_default(ctypes.byref(c))
+    c.precision = C.PRECISIONS["matrix_free"]
+    setattr(c, field, value)
+    pos = np.zeros(3)
+    h = ctypes.c_void_p()
+    rc = lib.rf_create(ctypes.byref(c), 1, C.ptr(pos), C.ptr(pos), ctypes.byref(h))
+    assert rc in (C.RF_E_INPUT, C.RF_E_UNSUPPORTED)
+    assert not h.value
+
+
+def test_matrix_free_footprint_grows_with_the_vectors_only():
+    """Without a stored operator the device footprint is O(N) vectors plus
+    O(N^2 / 8) partial rows: at N=16000 well under the 155 GB the structured
+    operator would take, and far under the dense FP32 matrix."""
+    lib = C.load()
+    c = C.rf_config()
+    lib.rf_config_default(ctypes.byref(c))
+    sizes = {}
+    for prec in ("fp32", "mixed_fp16", "matrix_free"):
+        c.precision = C.PRECISIONS[prec]
+        sizes[prec] = [lib.rf_device_bytes_estimate(ctypes.byref(c), n) for n in (4000, 16000)]
+    assert sizes["matrix_free"][0] < sizes["mixed_fp16"][0] / 10 < sizes["fp32"][0]
+    assert sizes["matrix_free"][1] < 8e9 < 1.5e11 < sizes["mixed_fp16"][1]
