@@ -44,7 +44,7 @@ def parse():
                     help="skip the plain FP32 comparison legs (the dense matrix of large N does not fit beside)")
     ap.add_argument("--no-error-leg", action="store_true",
                     help="skip the step errors against the FP64 reference at the benchmark configurations")
-    ap.add_argument("--reference-cap-s", type=float, default=1500.0,
+    ap.add_argument("--reference-cap-s", type=float, default=300.0,
                     help="reference arm: stop timing CPU steps when the next one would end past this many seconds")
     ap.add_argument("--mixed-restart", type=int, default=20,
                     help="Arnoldi steps between FP64 residual corrections in mixed precision (0: GMRES restart)")
