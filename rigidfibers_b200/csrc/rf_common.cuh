@@ -74,6 +74,15 @@ inline cudaError_t host_wait(cudaStream_t st, cudaEvent_t ev) {
   return e != cudaSuccess ? e : cudaEventSynchronize(ev);
 }
 
+// FP32 -> FP64 without flushing subnormal inputs: with -ftz=true a plain cast
+// becomes a conversion plus a flushing multiply; the conversion alone is exact
+// for every FP32 value
+__device__ __forceinline__ double f2d(float v) {
+  double d;
+  asm("cvt.f64.f32 %0, %1;" : "=d"(d) : "f"(v));
+  return d;
+}
+
 // Symmetric 3x3 stored as (11, 22, 33, 12, 13, 23) -- the order of
 // fortran/compute_inner_integral_numerically.incl:179-184.
 __device__ __forceinline__ float sym_get(const float* s6, int a, int b) {

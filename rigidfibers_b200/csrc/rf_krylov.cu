@@ -159,10 +159,10 @@ __device__ __forceinline__ void partial_dots(const float* __restrict__ w, const 
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
-    const double wr = (double)w[r];
+    const double wr = f2d(w[r]);
 #pragma unroll
     for (int k = 0; k < NV; ++k)
-      if (k < nv) acc[k] = fma(wr, (double)V[(int64_t)(i0 + k) * ldv + r], acc[k]);
+      if (k < nv) acc[k] = fma(wr, f2d(V[(int64_t)(i0 + k) * ldv + r]), acc[k]);
   }
 }
 
@@ -186,7 +186,7 @@ __device__ void grid_partial_norm(const float* __restrict__ w, int64_t R, double
                                   int slot) {
   double acc[1] = {0.0};
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
-    const double v = (double)w[r];
+    const double v = f2d(w[r]);
     acc[0] = fma(v, v, acc[0]);
   }
   __shared__ double tmp[1];
@@ -292,8 +292,8 @@ __global__ void k_gmres_arnoldi(GmresArgs a, int j) {
   for (int k = threadIdx.x; k < nv; k += blockDim.x) h[k] = sum_parts(p0, gridDim.x, a.stride, k);
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
-    double s = (double)w[r];
-    for (int k = 0; k < nv; ++k) s -= h[k] * (double)a.V[(int64_t)k * a.ldv + r];
+    double s = f2d(w[r]);
+    for (int k = 0; k < nv; ++k) s -= h[k] * f2d(a.V[(int64_t)k * a.ldv + r]);
     w[r] = (float)s;
   }
   grid_partial_dots(w, a.V, a.ldv, nv, a.R, p1, a.stride);
@@ -301,8 +301,8 @@ __global__ void k_gmres_arnoldi(GmresArgs a, int j) {
   for (int k = threadIdx.x; k < nv; k += blockDim.x) h2[k] = sum_parts(p1, gridDim.x, a.stride, k);
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
-    double s = (double)w[r];
-    for (int k = 0; k < nv; ++k) s -= h2[k] * (double)a.V[(int64_t)k * a.ldv + r];
+    double s = f2d(w[r]);
+    for (int k = 0; k < nv; ++k) s -= h2[k] * f2d(a.V[(int64_t)k * a.ldv + r]);
     w[r] = (float)s;
   }
   grid_partial_norm(w, a.R, p2, a.stride, 0);
@@ -361,13 +361,13 @@ __global__ void k_gmres_update(GmresArgs a) {
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int k = 0; k < jc; ++k) s += y[k] * (double)a.V[(int64_t)k * a.ldv + r];
+    for (int k = 0; k < jc; ++k) s += y[k] * f2d(a.V[(int64_t)k * a.ldv + r]);
     if (a.x_double) {
       double* x = static_cast<double*>(a.x);
       x[r] += s;
     } else {
       float* x = static_cast<float*>(a.x);
-      x[r] = (float)((double)x[r] + s);
+      x[r] = (float)(f2d(x[r]) + s);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->restarts += 1;
@@ -738,8 +738,8 @@ __device__ void grid_partial_dot2(const float* __restrict__ a, const float* __re
                                   double* __restrict__ part, int stride, int slot) {
   double acc[2] = {0.0, 0.0};
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < R; r += (int64_t)gridDim.x * blockDim.x) {
-    acc[0] = fma((double)a[r], (double)b[r], acc[0]);
-    acc[1] = fma((double)c[r], (double)d[r], acc[1]);
+    acc[0] = fma(f2d(a[r]), f2d(b[r]), acc[0]);
+    acc[1] = fma(f2d(c[r]), f2d(d[r]), acc[1]);
   }
   __shared__ double tmp[2];
   block_reduce_store<2>(acc, tmp);

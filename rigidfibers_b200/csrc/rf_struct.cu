@@ -618,7 +618,7 @@ __device__ __forceinline__ void r64_half(const float* rec, const double* xjs, co
         const int blk = HF::BB + b, kI = blk / M, kJ = blk % M;
         double tv[6];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) tv[c] = (double)rec[kI * RS::CHF + (kJ * 6 + c) * 8];
+        for (int c = 0; c < 6; ++c) tv[c] = f2d(rec[kI * RS::CHF + (kJ * 6 + c) * 8]);
         sym_mv_acc(tv, xj + 3 * kJ, zi + 3 * (kI - HF::R0));
         sym_mv_acc(tv, xi + 3 * (kI - HF::R0), zj + 3 * kJ);
       }
