@@ -780,9 +780,15 @@ def run_ours(args, dist):
     # rows), scaled by the pairs one launch processes; not captured for the
     # dense FP32 kernel
     traffic = 357.4e6 / (1500 * 1499 / 2) * (N * (N - 1) / 2) if precision not in ("fp32", "matrix_free") else None
+    if precision == "fp32":
+        # one ncu capture of k_gemv_cm_f32 at N=1000: dram__bytes_read.sum 900.6 MB
+        # + dram__bytes_write.sum 5.0 MB for R^2 x 4 B = 900.0 MB, scaled by R^2
+        traffic = (900.6e6 + 5.0e6) / (4.0 * 15000 ** 2) * bytes_per_matvec
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
-            "kernel": kernel, "traffic_source": "ncu capture at N=1500 scaled by pairs" if traffic else None,
+            "kernel": kernel,
+            "traffic_source": None if traffic is None else ("ncu capture at N=1000 scaled by R^2" if precision == "fp32"
+                                                            else "ncu capture at N=1500 scaled by pairs"),
             "algorithmic_bytes_per_launch": bytes_per_matvec, "avg_launch_ms": mv_avg_ms,
             "launches": head["mv_launches"], "share_of_step_time": head["mv_ms"] / head["ms"] if head["ms"] else None,
             "measured_in": "a profiled pass of the same K steps after the timed ones (CUDA events around each matvec "
