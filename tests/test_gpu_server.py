@@ -147,3 +147,32 @@ def test_failed_request_reports_its_status():
         with pytest.raises(C.RigidFibersError) as e:
             srv.result(rid)
         assert e.value.status == C.RF_E_NAN
+
+
+def _serve_with_graph_mode(graphs):
+    from rigidfibers_b200 import Config
+    from rigidfibers_b200.server import Server
+    reqs = serving_requests(count=4, seed=19, n_min=16, n_max=200, steps_min=3, steps_max=6)
+    out = []
+    with Server(max_active=2, use_cuda_graphs=graphs, reserve_bytes=1 << 28) as srv:
+        ids = [srv.submit(Config(precision="mixed_bf16"), *request_layout(r), r["nsteps"]) for r in reqs]
+        srv.drain(timeout=300)
+        for r, rid in zip(reqs, ids):
+            t = srv.step_times(rid)
+            assert len(t) == r["nsteps"] and (t > 0).all()
+            out.append(srv.result(rid)[:2])
+        st = srv.stats()
+        assert st["p50_setup_ms"] > 0 and st["p99_setup_ms"] >= st["p50_setup_ms"]
+        assert st["completed"] == len(reqs)
+    return out
+
+
+def test_step_times_setup_and_graph_modes():
+    """rf_server_step_times returns one wall time per step of a finished
+    request; the server's set-up percentiles cover handle creation and, with
+    whole-step graphs (mode 1), building them before the first step; the
+    results of mode 1 and mode 2 (restart cycles) are the same bit for bit."""
+    a = _serve_with_graph_mode(1)
+    b = _serve_with_graph_mode(2)
+    for (pa, oa), (pb, ob) in zip(a, b):
+        assert np.array_equal(pa, pb) and np.array_equal(oa, ob)

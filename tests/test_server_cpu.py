@@ -62,6 +62,17 @@ def test_server_config_validation():
     assert lib.rf_server_create(ctypes.byref(sc), ctypes.byref(s)) == C.RF_E_INPUT
     sc = C.rf_server_config(max_active=4, hbm_budget_bytes=0)
     assert lib.rf_server_create(ctypes.byref(sc), ctypes.byref(s)) == C.RF_E_INPUT
+    sc = C.rf_server_config(max_active=4, hbm_budget_bytes=1 << 30, reserve_bytes=-1)
+    assert lib.rf_server_create(ctypes.byref(sc), ctypes.byref(s)) == C.RF_E_INPUT
+
+
+def test_server_defaults_reserve_a_quarter_of_the_budget():
+    lib = C.load()
+    sc = C.rf_server_config()
+    assert lib.rf_server_config_default(ctypes.byref(sc)) == C.RF_OK
+    assert sc.reserve_bytes == sc.hbm_budget_bytes // 4
+    assert sc.use_cuda_graphs == 2 and sc.max_active == 16
+    assert lib.rf_server_step_times(None, 1, None, 0, ctypes.byref(ctypes.c_int())) == C.RF_E_INPUT
 
 
 def test_requests_fail_cleanly_without_a_device():
