@@ -143,8 +143,8 @@ def validate(args):
     # tolerances relative to each field's largest magnitude; Krylov solutions
     # differ from a direct one by up to the solver tolerance
     tol = {"gmres": 1e-5, "direct": 1e-5, "bicgstab": 5e-5}[_solver(args)]
-    if args.precision != "fp32":
-        tol = 1e-4
+    if args.precision in ("mixed_fp16", "mixed_bf16"):
+        tol = 1e-4   # the 16-bit operator's bound; the matrix-free mode keeps the plain path's
     failed = []
     for t in range(2):
         sim.assembleSystem()
