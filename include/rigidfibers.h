@@ -389,6 +389,14 @@ int rf_debug_fail_allocation_after(int n);
  * columns per split, capped so that splits x R partial rows fit its fixed
  * scratch array.  RF_E_INPUT when R is outside [1, 131072] or sms < 1. */
 int rf_debug_noalloc_plan(int64_t R, int sms, int* splits, int64_t* cols_per_split);
+/* The CTAs (a thread-block cluster of 1, 2, 4 or 8) that rf_solve_packed and
+ * rf_step_packed give each member of a pack of n suspensions of fibers[i]
+ * fibers on a GPU with `sms` multiprocessors (no device needed): the member
+ * with the most 16 x 16-fiber storage tiles per CTA doubles its cluster while
+ * the pack's CTAs stay within sms and every CTA keeps two tiles.  A member's
+ * result is the same bits for every cluster size.  RF_E_INPUT when n < 1,
+ * sms < 1 or a size is outside [1, 128]. */
+int rf_debug_pack_plan(const int* fibers, int n, int sms, int* ctas);
 
 const char* rf_status_string(int status);
 const char* rf_last_error(void);

@@ -176,6 +176,8 @@ SIGNATURES = {
     "rf_debug_fail_allocation_after": (ctypes.c_int, [ctypes.c_int]),
     "rf_debug_noalloc_plan": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int64)]),
+    "rf_debug_pack_plan": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int)]),
     "rf_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "rf_last_error": (ctypes.c_char_p, []),
 }

@@ -279,6 +279,7 @@ struct rf_handle {
   float* vpart = nullptr;
   cudaEvent_t ev[8];
   cudaEvent_t order_ev = nullptr;   // orders this handle's stream before a packed solve
+  PackLanes pack_lanes;             // streams of a packed solve this handle leads
   int pack_status = RF_OK;          // this handle's result in the last packed solve
   rf_stats stats;
   // optional per-launch timing of the solve's matvec kernels
@@ -364,6 +365,9 @@ struct rf_handle {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     if (order_ev) cudaEventDestroy(order_ev);
+    for (auto& a : pack_lanes.aux)
+      if (a) cudaStreamSynchronize(a);
+    pack_lanes_release(pack_lanes);
     if (wait_ev) cudaEventDestroy(wait_ev);
     if (st) cudaStreamDestroy(st);
   }
@@ -1181,6 +1185,25 @@ static int pack_order_streams(rf_handle** hs, int n, cudaStream_t st) {
   return RF_OK;
 }
 
+// The packed solve's cluster sizes (pack_plan_ctas) and the members' order in
+// its descriptor array: clusters of 8 first, then 4, 2 and 1 (counts); pos[i]
+// is member i's place.
+static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (&counts)[4]) {
+  std::vector<int> fibers((size_t)n), ctas((size_t)n);
+  for (int i = 0; i < n; ++i) fibers[(size_t)i] = (int)hs[i]->N;
+  pack_plan_ctas(fibers.data(), n, hs[0]->num_sms, ctas.data());
+  pos.assign((size_t)n, 0);
+  int k = 0;
+  for (int c = 0; c < 4; ++c) {
+    counts[c] = 0;
+    for (int i = 0; i < n; ++i)
+      if (ctas[(size_t)i] == (8 >> c)) {
+        pos[(size_t)i] = k++;
+        ++counts[c];
+      }
+  }
+}
+
 // the packed solve's descriptor of h (out: 4 ints, relres: 1 double, on the device)
 static void pack_member(rf_handle* h, int* out, double* relres, PackMember* q) {
   std::memset(q, 0, sizeof(*q));
@@ -1219,9 +1242,10 @@ static int pack_record_solve(rf_handle* h, const int* o, double relres) {
   return h->pack_status;
 }
 
-// One launch solves every handle's assembled system (k_pack_gmres_ir: one CTA
-// per suspension, the rf_solve algorithm for the mixed modes); each handle's
-// result depends only on its own data.
+// One launch per cluster size solves every handle's assembled system
+// (k_pack_gmres_ir: one thread-block cluster per suspension, the rf_solve
+// algorithm for the mixed modes); each handle's result depends only on its
+// own data.
 int rf_solve_packed(rf_handle** hs, int n) {
   if (!hs || n < 1) return RF_E_INPUT;
   int m = 0, Rmax = 0;
@@ -1238,12 +1262,15 @@ int rf_solve_packed(rf_handle** hs, int n) {
   double* drel = reinterpret_cast<double*>(dbuf + bm);
   int* dout = reinterpret_cast<int*>(dbuf + bm + br);
   std::vector<PackMember> pm((size_t)n);
+  std::vector<int> pos;
+  int counts[4];
+  pack_solve_order(hs, n, pos, counts);
   for (int i = 0; i < n; ++i) {
-    pack_member(hs[i], dout + 4 * i, drel + i, &pm[(size_t)i]);
+    pack_member(hs[i], dout + 4 * i, drel + i, &pm[(size_t)pos[(size_t)i]]);
     RF_CUDA_TRY(cudaEventRecord(hs[i]->ev[2], st));
   }
   RF_CUDA_TRY(cudaMemcpyAsync(dm, pm.data(), bm, cudaMemcpyHostToDevice, st));
-  int rc = launch_pack_gmres_ir(dm, n, Rmax, m, st);
+  int rc = launch_pack_gmres_ir(dm, counts, Rmax, m, st, h0->pack_lanes);
   std::vector<int> out((size_t)n * 4, 0);
   std::vector<double> rel((size_t)n, 0.0);
   if (rc == RF_OK) {
@@ -1330,11 +1357,14 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   PackMember* pm = reinterpret_cast<PackMember*>(host.data());
   PackStepMember* sm = reinterpret_cast<PackStepMember*>(host.data() + bm);
   std::vector<int64_t> asm_blocks((size_t)ngroups, 0), vel_blocks((size_t)ngroups, 0);
+  std::vector<int> pos;
+  int counts[4];
+  pack_solve_order(hs, n, pos, counts);
   for (int g = 0; g < ngroups; ++g) {
     for (int k = gbeg[g]; k < gbeg[g + 1]; ++k) {
       const int i = order[(size_t)k];
       rf_handle* h = hs[i];
-      pack_member(h, dout + 4 * i, drel + i, &pm[i]);
+      pack_member(h, dout + 4 * i, drel + i, &pm[pos[(size_t)i]]);
       PackStepMember& q = sm[k];
       std::memset(&q, 0, sizeof(q));
       q.N = h->N;
@@ -1378,7 +1408,7 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
     launches += 2;
   }
   RF_CUDA_TRY(cudaEventRecord(ev[1], st));
-  if (rc == RF_OK) rc = launch_pack_gmres_ir(dpm, n, Rmax, m, st);
+  if (rc == RF_OK) rc = launch_pack_gmres_ir(dpm, counts, Rmax, m, st, h0->pack_lanes);
   RF_CUDA_TRY(cudaEventRecord(ev[3], st));
   for (int g = 0; g < ngroups && rc == RF_OK; ++g) {
     rf_handle* hg = hs[order[(size_t)gbeg[g]]];

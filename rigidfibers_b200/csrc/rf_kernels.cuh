@@ -81,8 +81,8 @@ int launch_struct_velocity(const Tables& tab, int N, const float* S32, const flo
                            const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t st);
 
-// Packed mixed-precision solves (csrc/rf_pack.cu): one CTA per suspension of
-// at most kPackMaxFibers fibers, M = 5, Q = 24 storage.
+// Packed mixed-precision solves (csrc/rf_pack.cu): one thread-block cluster
+// per suspension of at most kPackMaxFibers fibers, M = 5, Q = 24 storage.
 constexpr int kPackMaxFibers = 128;
 struct PackMember {
   int N, smode, maxit, pad;      // smode 1 FP16, 2 BF16 blocks; maxit: Arnoldi steps in total
@@ -99,8 +99,22 @@ struct PackMember {
   double* relres;                // ||b - A x|| / ||b|| at the last check
   float coef[5], eig[5];         // C_k = coef_k (I - E_k t t^T), k >= 1; coef_0 t t^T
 };
-size_t pack_smem_bytes(int Rmax, int m);
-int launch_pack_gmres_ir(const PackMember* members, int n, int Rmax, int m, cudaStream_t st);
+// CTAs (a thread-block cluster of 1, 2, 4 or 8) per member of a packed solve:
+// starting from one each, the member with the most storage tiles per CTA
+// doubles its cluster while the pack's CTAs stay within sms and each CTA keeps
+// at least two tiles.  A member's result does not depend on its cluster size.
+void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas);
+size_t pack_smem_bytes(int Rmax, int m, int csize);
+// Streams and events the packed solve forks its cluster-size classes onto.
+struct PackLanes {
+  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+};
+void pack_lanes_release(PackLanes& lanes);
+// members: counts[0] members with clusters of 8, then counts[1] of 4,
+// counts[2] of 2 and counts[3] of 1 CTA
+int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], int Rmax, int m, cudaStream_t st,
+                         PackLanes& lanes);
 
 // One suspension of a packed step: the buffers its assembly, velocities and
 // update read and write.  The packed stage kernels launch once per group of

@@ -79,6 +79,45 @@ def test_member_is_the_same_alone_and_in_a_pack():
     assert np.array_equal(p1, p2) and np.array_equal(o1, o2)
 
 
+def test_member_is_the_same_for_every_cluster_size():
+    """A member's packed solve is the same bits whatever cluster the pack's
+    plan gives it: alone a 128-fiber suspension runs on 8 CTAs and a 64-fiber
+    one on 4; beside 148 other members (more members than multiprocessors)
+    each runs on one."""
+    import ctypes
+    import torch
+    from rigidfibers_b200 import _capi as C
+    from rigidfibers_b200.simulation import solve_packed
+    lib = C.load()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    fibers = [128, 64] + [16] * max(148, sms - 1)
+
+    def plan(fs):
+        c = (ctypes.c_int * len(fs))()
+        assert lib.rf_debug_pack_plan((ctypes.c_int * len(fs))(*fs), len(fs), sms, c) == C.RF_OK
+        return list(c)
+
+    assert plan([128]) == [8] and plan([64]) == [4]
+    assert plan(fibers)[:2] == [1, 1]
+    lays = [_layout(n, 300 + k) for k, n in enumerate(fibers)]
+    alone = []
+    for k in range(2):
+        a = _sim(*lays[k], precision="mixed_fp16")
+        a.assembleSystem()
+        solve_packed([a])
+        alone.append((a.solution(), a.stats()["iterations"]))
+        a.close()
+    sims = [_sim(*lay, precision="mixed_fp16") for lay in lays]
+    for s in sims:
+        s.assembleSystem()
+    solve_packed(sims)
+    for k in range(2):
+        assert np.array_equal(sims[k].solution(), alone[k][0]), fibers[k]
+        assert sims[k].stats()["iterations"] == alone[k][1]
+    for s in sims:
+        s.close()
+
+
 def test_packed_steps_follow_rf_step():
     from rigidfibers_b200.simulation import step_packed
     pos, ori = _layout(60, 9)

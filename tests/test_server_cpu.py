@@ -124,3 +124,38 @@ def test_packed_requests_fail_cleanly_without_a_device():
         srv.drain(timeout=60)
         assert [srv.poll(i)[0] for i in ids] == ["failed"] * 5
         assert srv.stats()["active"] == 0
+
+
+def test_pack_plan_gives_large_members_clusters():
+    """rf_debug_pack_plan: a member's cluster doubles (1, 2, 4, 8 CTAs) while
+    the pack fits the multiprocessors and each CTA keeps two storage tiles."""
+    lib = C.load()
+
+    def plan(fibers, sms):
+        n = len(fibers)
+        f = (ctypes.c_int * n)(*fibers)
+        c = (ctypes.c_int * n)()
+        assert lib.rf_debug_pack_plan(f, n, sms, c) == C.RF_OK
+        return list(c)
+
+    assert plan([128], 148) == [8]
+    assert plan([64], 148) == [4]          # 10 tiles: 4 CTAs keep two each, 8 would not
+    assert plan([48], 148) == [2]
+    assert plan([32], 148) == [1]
+    assert plan([16] * 100, 148) == [1] * 100
+    assert plan([128] * 150, 148) == [1] * 150   # more members than multiprocessors
+    assert plan([128, 128], 4) == [2, 2]
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        n = int(rng.integers(1, 200))
+        sms = int(rng.integers(1, 300))
+        fibers = [int(v) for v in rng.integers(1, 129, n)]
+        c = plan(fibers, sms)
+        assert sum(c) <= max(n, sms)
+        for f, k in zip(fibers, c):
+            t = (f + 15) // 16
+            assert k in (1, 2, 4, 8) and (k == 1 or t * (t + 1) // 2 >= 2 * k)
+    f = (ctypes.c_int * 2)(16, 129)
+    c = (ctypes.c_int * 2)()
+    assert lib.rf_debug_pack_plan(f, 2, 148, c) == C.RF_E_INPUT
+    assert lib.rf_debug_pack_plan(f, 1, 0, c) == C.RF_E_INPUT
