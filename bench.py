@@ -50,16 +50,17 @@ def parse():
                     help="Arnoldi steps between FP64 residual corrections in mixed precision (0: GMRES restart)")
     ap.add_argument("--serve-requests", type=int, default=512,
                     help="suspensions in the served ensemble (0: skip the serving leg)")
-    ap.add_argument("--serve-max-active", type=int, default=16)
+    ap.add_argument("--serve-max-active", type=int, default=8,
+                    help="requests stepping on their own handles at once (the pack's members are not counted)")
     ap.add_argument("--serve-rate", type=float, default=400.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-graphs", type=int, default=2,
                     help="CUDA graph mode of the served requests: 2 restart cycles (default), 1 whole steps built "
                          "at admission, 0 off")
-    ap.add_argument("--serve-pack-fibers", type=int, default=0,
+    ap.add_argument("--serve-pack-fibers", type=int, default=128,
                     help="requests of at most this many fibers step together with packed solves (0: off)")
-    ap.add_argument("--serve-pack-compare", type=int, default=64,
-                    help="also run the ensemble with packed solves for requests of at most this many fibers, "
-                         "reported as serving_packed (0: skip)")
+    ap.add_argument("--serve-compare", default="0,16",
+                    help="PACK_FIBERS,MAX_ACTIVE: also run the ensemble so (default: no packing, 16 requests at "
+                         "once), reported as serving_compare ('': skip)")
     ap.add_argument("--direct-fibers", type=int, default=2000,
                     help="fibers of the direct-solver leg (0: skip it)")
     ap.add_argument("--direct-large-fibers", type=int, default=4000,
@@ -624,7 +625,7 @@ def error_vs_fp64(args, precision):
     return out
 
 
-def serve_ensemble(args, dist, pack_fibers=None):
+def serve_ensemble(args, dist, pack_fibers=None, max_active=None):
     """The served ensemble: independent suspensions (N log-uniform in
     [16, 1000], eps in {0.01, 0.005}, 5-50 steps, BF16 pair blocks) arriving
     as a Poisson stream into one rf_server; per-step latency percentiles and
@@ -641,8 +642,9 @@ def serve_ensemble(args, dist, pack_fibers=None):
     gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
     dist.barrier()
     pack = args.serve_pack_fibers if pack_fibers is None else pack_fibers
+    slots = args.serve_max_active if max_active is None else max_active
     ids = []
-    with Server(max_active=args.serve_max_active, use_cuda_graphs=args.serve_graphs, pack_max_fibers=pack) as srv:
+    with Server(max_active=slots, use_cuda_graphs=args.serve_graphs, pack_max_fibers=pack) as srv:
         t0 = time.perf_counter()
         due = t0
         for r, (p, o), c, g in zip(reqs, layouts, cfgs, gaps):
@@ -672,7 +674,7 @@ def serve_ensemble(args, dist, pack_fibers=None):
             "fiber_steps_per_s": fiber_steps / wall_max, "requests": len(reqs) * dist.world,
             "completed": int(dist.sum(st["completed"])), "failed": int(dist.sum(st["failed"])),
             "steps": int(dist.sum(st["steps"])), "wall_s": wall_max, "arrival_rate_per_s": args.serve_rate,
-            "max_active": args.serve_max_active, "peak_active": st["peak_active"],
+            "max_active": slots, "peak_active": st["peak_active"],
             "cuda_graph_mode": args.serve_graphs, "pack_max_fibers": pack,
             **({"pack_steps": st["pack_steps"], "pack_p50_ms": st["pack_p50_ms"], "pack_p99_ms": st["pack_p99_ms"],
                 "pack_max_ms": st["pack_max_ms"], "pack_mean_members": st["pack_mean_members"]} if pack else {}),
@@ -845,8 +847,9 @@ def run_ours(args, dist):
         out["fp32_path"] = comparison
         out["fp32_restart_matched"] = matched
     if args.serve_requests > 0:
-        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
-            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
+        if args.serve_compare:
+            cp, ca = (int(v) for v in args.serve_compare.split(","))
+            out["serving_compare"] = serve_ensemble(args, dist, cp, ca)
         out["serving"] = serve_ensemble(args, dist)
     # the headline figures once more, compact, at the end of the line
     summ = {"value": value, "e2e": e2e_value}
@@ -875,8 +878,9 @@ def run_legs(args, dist):
     out = {"legs": sorted(legs)}
     if "serving" in legs:
         out["serving"] = serve_ensemble(args, dist)
-        if args.serve_pack_compare > 0 and args.serve_pack_compare != args.serve_pack_fibers:
-            out["serving_packed"] = serve_ensemble(args, dist, args.serve_pack_compare)
+        if args.serve_compare:
+            cp, ca = (int(v) for v in args.serve_compare.split(","))
+            out["serving_compare"] = serve_ensemble(args, dist, cp, ca)
     if "direct" in legs and dist.rank == 0:
         out["direct_solver"] = direct_leg(args)
     if "error" in legs and dist.rank == 0:

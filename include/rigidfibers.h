@@ -153,9 +153,10 @@ int rf_step(rf_handle* h, int current_timestep);
 int rf_run(rf_handle* h, int first_timestep, int nsteps);
 
 /* Packed solves of many small suspensions (no reference counterpart: the
- * ensemble path of the serving loop).  One launch solves the assembled
- * systems of n handles, one CTA each, with the algorithm rf_solve runs in the
- * mixed modes (GMRES-IR, FP64 residual).  Members: mixed precision, GMRES,
+ * ensemble path of the serving loop).  One launch per cluster size solves
+ * the assembled systems of n handles, each on a thread-block cluster of 1 to
+ * 8 CTAs (rf_debug_pack_plan), with the algorithm rf_solve runs in the mixed
+ * modes (GMRES-IR, FP64 residual).  Members: mixed precision, GMRES,
  * 5 force terms, 8x3 quadrature, at most 128 fibers, one restart length.  A
  * member's result depends only on its own data, so it is the same alone and
  * in any pack (it may differ from rf_solve's in the last bits: the sums run
@@ -308,14 +309,16 @@ enum rf_request_status { RF_REQ_QUEUED = 0, RF_REQ_RUNNING = 1, RF_REQ_DONE = 2,
 typedef struct rf_server rf_server;
 
 typedef struct rf_server_config {
-  int max_active;            /* requests running at once on their own handles */
+  int max_active;            /* requests running at once on their own handles
+                                (default 8; the pack's members are not counted) */
   int64_t hbm_budget_bytes;  /* sum of the running requests' estimates */
   int use_cuda_graphs;       /* rf_set_cuda_graphs mode of every request's handle
                                 (default 2: restart cycles; 1: whole-step graphs, built
                                 when the request is admitted, rf_prepare_step_graphs) */
   int pack_max_fibers;       /* requests of at most this many fibers (<= 128, mixed
                                 precision, GMRES, 5 terms, 8x3 quadrature) step together
-                                with packed solves (rf_step_packed); 0: off */
+                                with packed solves (rf_step_packed); 0: off.
+                                Default 128 */
   int pack_max_members;      /* suspensions per pack */
   int64_t reserve_bytes;     /* device memory taken into the handles' pool when the
                                 server starts (at most hbm_budget_bytes), so that

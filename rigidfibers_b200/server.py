@@ -11,7 +11,7 @@ The reference runs one suspension per process (fibers_runner.py:17-162);
 here many suspensions share one GPU: admission in arrival order by free slot
 and device-memory budget, one handle and stream per running suspension; with
 pack_max_fibers > 0 the small ones step together, their systems solved by
-one launch per step (rf_step_packed).
+a few launches per step (rf_step_packed).
 """
 import ctypes
 

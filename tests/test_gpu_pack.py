@@ -1,5 +1,5 @@
 """Packed solves of many small suspensions: rf_solve_packed / rf_step_packed
-(one CTA per suspension) and the server's pack.
+(one thread-block cluster per suspension) and the server's pack.
 
 Bounds (written here): the packed solution within 1e-5 relative of rf_solve's
 (both run GMRES-IR to a relative residual of 1e-6; only the summation order

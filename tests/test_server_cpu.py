@@ -71,7 +71,7 @@ def test_server_defaults_reserve_a_quarter_of_the_budget():
     sc = C.rf_server_config()
     assert lib.rf_server_config_default(ctypes.byref(sc)) == C.RF_OK
     assert sc.reserve_bytes == sc.hbm_budget_bytes // 4
-    assert sc.use_cuda_graphs == 2 and sc.max_active == 16
+    assert sc.use_cuda_graphs == 2 and sc.max_active == 8
     assert lib.rf_server_step_times(None, 1, None, 0, ctypes.byref(ctypes.c_int())) == C.RF_E_INPUT
 
 
@@ -96,7 +96,7 @@ def test_pack_config_and_validation():
     lib = C.load()
     sc = C.rf_server_config()
     assert lib.rf_server_config_default(ctypes.byref(sc)) == C.RF_OK
-    assert sc.pack_max_fibers == 0 and sc.pack_max_members >= 1
+    assert sc.pack_max_fibers == 128 and sc.pack_max_members >= 1
     sc.pack_max_fibers = 64
     sc.pack_max_members = 0
     s = ctypes.c_void_p()
