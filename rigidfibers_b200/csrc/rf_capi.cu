@@ -1191,7 +1191,7 @@ static int pack_order_streams(rf_handle** hs, int n, cudaStream_t st) {
 static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (&counts)[4]) {
   std::vector<int> fibers((size_t)n), ctas((size_t)n);
   for (int i = 0; i < n; ++i) fibers[(size_t)i] = (int)hs[i]->N;
-  pack_plan_ctas(fibers.data(), n, hs[0]->num_sms, ctas.data());
+  pack_plan_ctas(fibers.data(), n, hs[0]->num_sms, ctas.data(), pack_max_cluster());
   pos.assign((size_t)n, 0);
   int k = 0;
   for (int c = 0; c < 4; ++c) {

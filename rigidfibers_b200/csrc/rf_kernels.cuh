@@ -101,9 +101,12 @@ struct PackMember {
 };
 // CTAs (a thread-block cluster of 1, 2, 4 or 8) per member of a packed solve:
 // starting from one each, the member with the most storage tiles per CTA
-// doubles its cluster while the pack's CTAs stay within sms and each CTA keeps
-// at least two tiles.  A member's result does not depend on its cluster size.
-void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas);
+// doubles its cluster while the pack's CTAs stay within sms, each CTA keeps
+// at least two tiles and the cluster stays within max_cluster.  A member's
+// result does not depend on its cluster size.
+void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas, int max_cluster);
+// the largest cluster of the packed solve this device can schedule (8, 4, 2 or 1)
+int pack_max_cluster();
 size_t pack_smem_bytes(int Rmax, int m, int csize);
 // Streams and events the packed solve forks its cluster-size classes onto.
 struct PackLanes {

@@ -25,6 +25,8 @@
 // Krylov basis stays in the suspension's V (L2-resident at these sizes), each
 // CTA writing its own rows of it.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <type_traits>
 
 #include <cooperative_groups.h>
@@ -489,7 +491,7 @@ __global__ void __launch_bounds__(kPT) k_pack_gmres_ir(const PackMember* __restr
 
 }  // namespace
 
-void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas) {
+void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas, int max_cluster) {
   int total = n;
   for (int i = 0; i < n; ++i) ctas[i] = 1;
   for (;;) {
@@ -497,7 +499,7 @@ void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas) {
     double most = 0.0;
     for (int i = 0; i < n; ++i) {
       const int T = (fibers[i] + 15) / 16, tiles = T * (T + 1) / 2;
-      if (ctas[i] >= kParts || tiles < 4 * ctas[i]) continue;   // at least two tiles per CTA after doubling
+      if (2 * ctas[i] > max_cluster || tiles < 4 * ctas[i]) continue;   // at least two tiles per CTA after doubling
       const double w = (double)tiles / ctas[i];
       if (w > most) {
         most = w;
@@ -515,6 +517,42 @@ size_t pack_smem_bytes(int Rmax, int m, int csize) {
   const size_t doubles = (1 + slots) * (size_t)Rmax + 8 * 16 * 16 + 16 * 16 + (size_t)(m + 1) * m + 2 * (size_t)m +
                          (size_t)(m + 1) + (size_t)m + 2 * (size_t)(m + 1) + 3 * kParts * (size_t)(m + 1) + 2;
   return doubles * sizeof(double) + 4 * sizeof(int);
+}
+
+int pack_max_cluster() {
+  // one query per device with the largest shared memory a pack can ask for
+  // (kPackMaxFibers rows, restart kMaxRestart): smaller packs fit wherever it does
+  static std::mutex mu;
+  static std::map<int, int> known;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = known.find(dev);
+  if (it != known.end()) return it->second;
+  int best = 1;
+  for (int c = kParts; c > 1 && best == 1; c /= 2) {
+    const size_t smem = pack_smem_bytes(kPM3 * kPackMaxFibers, kMaxRestart, c);
+    if (cudaFuncSetAttribute(k_pack_gmres_ir<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      break;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c);
+    cfg.blockDim = dim3(kPT);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_pack_gmres_ir<true>, &cfg) == cudaSuccess && clusters > 0)
+      best = c;
+  }
+  cudaGetLastError();   // a refused query leaves no error behind
+  known[dev] = best;
+  return best;
 }
 
 void pack_lanes_release(PackLanes& l) {
@@ -593,6 +631,6 @@ extern "C" int rf_debug_pack_plan(const int* fibers, int n, int sms, int* ctas) 
   if (!fibers || !ctas || n < 1 || sms < 1) return RF_E_INPUT;
   for (int i = 0; i < n; ++i)
     if (fibers[i] < 1 || fibers[i] > rf::kPackMaxFibers) return RF_E_INPUT;
-  rf::pack_plan_ctas(fibers, n, sms, ctas);
+  rf::pack_plan_ctas(fibers, n, sms, ctas, 8);
   return RF_OK;
 }

@@ -118,6 +118,32 @@ def test_member_is_the_same_for_every_cluster_size():
         s.close()
 
 
+def test_non_finite_member_of_a_clustered_pack_fails_alone():
+    """A member whose positions hold a NaN (a 128-fiber suspension, on a
+    cluster of CTAs) reports RF_E_NAN from rf_step_packed; the pack's other
+    members step exactly as they do alone."""
+    from rigidfibers_b200 import _capi as C
+    from rigidfibers_b200.simulation import step_packed
+    pb, ob = _layout(128, 41)
+    pb = pb.copy()
+    pb[5, 0] = np.nan
+    good = [_layout(64, 42), _layout(20, 43)]
+    alone = []
+    for lay in good:
+        a = _sim(*lay, precision="mixed_bf16")
+        assert step_packed([a], [0]) == [0]
+        alone.append(a.state())
+        a.close()
+    sims = [_sim(pb, ob, precision="mixed_bf16")] + [_sim(*lay, precision="mixed_bf16") for lay in good]
+    codes = step_packed(sims, [0, 0, 0])
+    assert codes[0] == C.RF_E_NAN and codes[1:] == [0, 0]
+    for sm, (pa, oa) in zip(sims[1:], alone):
+        p, o = sm.state()
+        assert np.array_equal(p, pa) and np.array_equal(o, oa)
+    for sm in sims:
+        sm.close()
+
+
 def test_packed_steps_follow_rf_step():
     from rigidfibers_b200.simulation import step_packed
     pos, ori = _layout(60, 9)
