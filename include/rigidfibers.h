@@ -157,7 +157,7 @@ int rf_run(rf_handle* h, int first_timestep, int nsteps);
  * the assembled systems of n handles, each on a thread-block cluster of 1 to
  * 8 CTAs (rf_debug_pack_plan), with the algorithm rf_solve runs in the mixed
  * modes (GMRES-IR, FP64 residual).  Members: mixed precision, GMRES,
- * 5 force terms, 8x3 quadrature, at most 128 fibers, one restart length.  A
+ * 5 force terms, 8x3 quadrature, at most 256 fibers, one restart length.  A
  * member's result depends only on its own data, so it is the same alone and
  * in any pack (it may differ from rf_solve's in the last bits: the sums run
  * in another order).  Returns RF_E_NAN / RF_E_NOCONV if a member ended so;
@@ -315,7 +315,7 @@ typedef struct rf_server_config {
   int use_cuda_graphs;       /* rf_set_cuda_graphs mode of every request's handle
                                 (default 2: restart cycles; 1: whole-step graphs, built
                                 when the request is admitted, rf_prepare_step_graphs) */
-  int pack_max_fibers;       /* requests of at most this many fibers (<= 128, mixed
+  int pack_max_fibers;       /* requests of at most this many fibers (<= 256, mixed
                                 precision, GMRES, 5 terms, 8x3 quadrature) step together
                                 with packed solves (rf_step_packed); 0: off.
                                 Default 128 */
@@ -394,11 +394,12 @@ int rf_debug_fail_allocation_after(int n);
 int rf_debug_noalloc_plan(int64_t R, int sms, int* splits, int64_t* cols_per_split);
 /* The CTAs (a thread-block cluster of 1, 2, 4 or 8) that rf_solve_packed and
  * rf_step_packed give each member of a pack of n suspensions of fibers[i]
- * fibers on a GPU with `sms` multiprocessors (no device needed): the member
- * with the most 16 x 16-fiber storage tiles per CTA doubles its cluster while
- * the pack's CTAs stay within sms and every CTA keeps two tiles.  A member's
- * result is the same bits for every cluster size.  RF_E_INPUT when n < 1,
- * sms < 1 or a size is outside [1, 128]. */
+ * fibers on a GPU with `sms` multiprocessors (no device needed): every member
+ * starts at one CTA (two above 128 fibers), then the member with the most
+ * 16 x 16-fiber storage tiles per CTA doubles its cluster while the pack's
+ * CTAs stay within sms and every CTA keeps two tiles.  A member's result is
+ * the same bits for every cluster size.  RF_E_INPUT when n < 1, sms < 1 or a
+ * size is outside [1, 256]. */
 int rf_debug_pack_plan(const int* fibers, int n, int sms, int* ctas);
 
 const char* rf_status_string(int status);

@@ -1146,7 +1146,8 @@ int rf_step(rf_handle* h, int t) {
 
 // ---- packed solves and steps of many small suspensions --------------------
 // The conditions of the packed solve (k_pack_gmres_ir): mixed precision,
-// GMRES, M = 5, Q = 24, at most kPackMaxFibers fibers, one restart length.
+// GMRES, M = 5, Q = 24, at most kPackMaxFibers fibers (more than
+// kPackSingleMaxFibers only where the device runs clusters), one restart length.
 static int pack_check(rf_handle** hs, int n, bool need_assembled, const char* who, int* m_out, int* Rmax_out) {
   int m = -1, Rmax = 0;
   for (int i = 0; i < n; ++i) {
@@ -1156,9 +1157,10 @@ static int pack_check(rf_handle** hs, int n, bool need_assembled, const char* wh
       set_last_error_str((std::string(who) + " before rf_assemble").c_str());
       return RF_E_STATE;
     }
-    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers) {
+    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers ||
+        (h->N > kPackSingleMaxFibers && pack_max_cluster() < 2)) {
       set_last_error_str(
-          (std::string(who) + ": mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 128 fibers").c_str());
+          (std::string(who) + ": mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 256 fibers").c_str());
       return RF_E_UNSUPPORTED;
     }
     if (m >= 0 && h->restart != m) {
@@ -1186,9 +1188,9 @@ static int pack_order_streams(rf_handle** hs, int n, cudaStream_t st) {
 }
 
 // The packed solve's cluster sizes (pack_plan_ctas) and the members' order in
-// its descriptor array: clusters of 8 first, then 4, 2 and 1 (counts); pos[i]
-// is member i's place.
-static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (&counts)[4]) {
+// its descriptor array: clusters of 8 first, then 4, 2 and 1 (counts, and the
+// largest system of each class in rmax); pos[i] is member i's place.
+static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (&counts)[4], int (&rmax)[4]) {
   std::vector<int> fibers((size_t)n), ctas((size_t)n);
   for (int i = 0; i < n; ++i) fibers[(size_t)i] = (int)hs[i]->N;
   pack_plan_ctas(fibers.data(), n, hs[0]->num_sms, ctas.data(), pack_max_cluster());
@@ -1196,10 +1198,12 @@ static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (
   int k = 0;
   for (int c = 0; c < 4; ++c) {
     counts[c] = 0;
+    rmax[c] = 0;
     for (int i = 0; i < n; ++i)
       if (ctas[(size_t)i] == (8 >> c)) {
         pos[(size_t)i] = k++;
         ++counts[c];
+        rmax[c] = std::max(rmax[c], (int)hs[i]->R);
       }
   }
 }
@@ -1263,14 +1267,14 @@ int rf_solve_packed(rf_handle** hs, int n) {
   int* dout = reinterpret_cast<int*>(dbuf + bm + br);
   std::vector<PackMember> pm((size_t)n);
   std::vector<int> pos;
-  int counts[4];
-  pack_solve_order(hs, n, pos, counts);
+  int counts[4], rmax[4];
+  pack_solve_order(hs, n, pos, counts, rmax);
   for (int i = 0; i < n; ++i) {
     pack_member(hs[i], dout + 4 * i, drel + i, &pm[(size_t)pos[(size_t)i]]);
     RF_CUDA_TRY(cudaEventRecord(hs[i]->ev[2], st));
   }
   RF_CUDA_TRY(cudaMemcpyAsync(dm, pm.data(), bm, cudaMemcpyHostToDevice, st));
-  int rc = launch_pack_gmres_ir(dm, counts, Rmax, m, st, h0->pack_lanes);
+  int rc = launch_pack_gmres_ir(dm, counts, rmax, m, st, h0->pack_lanes);
   std::vector<int> out((size_t)n * 4, 0);
   std::vector<double> rel((size_t)n, 0.0);
   if (rc == RF_OK) {
@@ -1358,8 +1362,8 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   PackStepMember* sm = reinterpret_cast<PackStepMember*>(host.data() + bm);
   std::vector<int64_t> asm_blocks((size_t)ngroups, 0), vel_blocks((size_t)ngroups, 0);
   std::vector<int> pos;
-  int counts[4];
-  pack_solve_order(hs, n, pos, counts);
+  int counts[4], rmax[4];
+  pack_solve_order(hs, n, pos, counts, rmax);
   for (int g = 0; g < ngroups; ++g) {
     for (int k = gbeg[g]; k < gbeg[g + 1]; ++k) {
       const int i = order[(size_t)k];
@@ -1408,7 +1412,7 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
     launches += 2;
   }
   RF_CUDA_TRY(cudaEventRecord(ev[1], st));
-  if (rc == RF_OK) rc = launch_pack_gmres_ir(dpm, counts, Rmax, m, st, h0->pack_lanes);
+  if (rc == RF_OK) rc = launch_pack_gmres_ir(dpm, counts, rmax, m, st, h0->pack_lanes);
   RF_CUDA_TRY(cudaEventRecord(ev[3], st));
   for (int g = 0; g < ngroups && rc == RF_OK; ++g) {
     rf_handle* hg = hs[order[(size_t)gbeg[g]]];

@@ -83,7 +83,10 @@ int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t s
 
 // Packed mixed-precision solves (csrc/rf_pack.cu): one thread-block cluster
 // per suspension of at most kPackMaxFibers fibers, M = 5, Q = 24 storage.
-constexpr int kPackMaxFibers = 128;
+constexpr int kPackMaxFibers = 256;
+// the largest member one CTA takes (its 8 partitions' rows in shared memory);
+// larger members run on clusters of at least two CTAs
+constexpr int kPackSingleMaxFibers = 128;
 struct PackMember {
   int N, smode, maxit, pad;      // smode 1 FP16, 2 BF16 blocks; maxit: Arnoldi steps in total
   double tol;                    // relative to ||b||
@@ -100,10 +103,11 @@ struct PackMember {
   float coef[5], eig[5];         // C_k = coef_k (I - E_k t t^T), k >= 1; coef_0 t t^T
 };
 // CTAs (a thread-block cluster of 1, 2, 4 or 8) per member of a packed solve:
-// starting from one each, the member with the most storage tiles per CTA
-// doubles its cluster while the pack's CTAs stay within sms, each CTA keeps
-// at least two tiles and the cluster stays within max_cluster.  A member's
-// result does not depend on its cluster size.
+// starting from one each (two above kPackSingleMaxFibers fibers), the member
+// with the most storage tiles per CTA doubles its cluster while the pack's
+// CTAs stay within sms, each CTA keeps at least two tiles and the cluster
+// stays within max_cluster.  A member's result does not depend on its
+// cluster size.
 void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas, int max_cluster);
 // the largest cluster of the packed solve this device can schedule (8, 4, 2 or 1)
 int pack_max_cluster();
@@ -115,9 +119,10 @@ struct PackLanes {
 };
 void pack_lanes_release(PackLanes& lanes);
 // members: counts[0] members with clusters of 8, then counts[1] of 4,
-// counts[2] of 2 and counts[3] of 1 CTA
-int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], int Rmax, int m, cudaStream_t st,
-                         PackLanes& lanes);
+// counts[2] of 2 and counts[3] of 1 CTA; rmax[c]: the largest system (rows)
+// of class c
+int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], const int (&rmax)[4], int m,
+                         cudaStream_t st, PackLanes& lanes);
 
 // One suspension of a packed step: the buffers its assembly, velocities and
 // update read and write.  The packed stage kernels launch once per group of

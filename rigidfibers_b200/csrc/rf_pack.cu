@@ -492,8 +492,11 @@ __global__ void __launch_bounds__(kPT) k_pack_gmres_ir(const PackMember* __restr
 }  // namespace
 
 void pack_plan_ctas(const int* fibers, int n, int sms, int* ctas, int max_cluster) {
-  int total = n;
-  for (int i = 0; i < n; ++i) ctas[i] = 1;
+  int total = 0;
+  for (int i = 0; i < n; ++i) {
+    ctas[i] = fibers[i] > kPackSingleMaxFibers ? 2 : 1;
+    total += ctas[i];
+  }
   for (;;) {
     int best = -1;
     double most = 0.0;
@@ -520,8 +523,10 @@ size_t pack_smem_bytes(int Rmax, int m, int csize) {
 }
 
 int pack_max_cluster() {
-  // one query per device with the largest shared memory a pack can ask for
-  // (kPackMaxFibers rows, restart kMaxRestart): smaller packs fit wherever it does
+  // one query per device and cluster size with the largest shared memory a
+  // pack can ask for (kPackMaxFibers rows, restart kMaxRestart): smaller packs
+  // fit wherever it does.  The answer is the largest C with every size from 2
+  // to C schedulable.
   static std::mutex mu;
   static std::map<int, int> known;
   int dev = 0;
@@ -530,7 +535,7 @@ int pack_max_cluster() {
   auto it = known.find(dev);
   if (it != known.end()) return it->second;
   int best = 1;
-  for (int c = kParts; c > 1 && best == 1; c /= 2) {
+  for (int c = 2; c <= kParts && best == c / 2; c *= 2) {
     const size_t smem = pack_smem_bytes(kPM3 * kPackMaxFibers, kMaxRestart, c);
     if (cudaFuncSetAttribute(k_pack_gmres_ir<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
@@ -563,17 +568,21 @@ void pack_lanes_release(PackLanes& l) {
   if (l.fork) cudaEventDestroy(l.fork), l.fork = nullptr;
 }
 
-int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], int Rmax, int m, cudaStream_t st,
-                         PackLanes& lanes) {
+int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], const int (&rmax)[4], int m,
+                         cudaStream_t st, PackLanes& lanes) {
   int n = 0;
-  for (int c = 0; c < 4; ++c) n += counts[c];
-  if (n < 1 || Rmax < 1 || Rmax > kPM3 * kPackMaxFibers || m < 1 || m > kMaxRestart) {
+  size_t smax = 0;
+  for (int c = 0; c < 4; ++c) {
+    n += counts[c];
+    if (counts[c] == 0) continue;
+    const int limit = kPM3 * (c == 3 ? kPackSingleMaxFibers : kPackMaxFibers);
+    if (rmax[c] < 1 || rmax[c] > limit) n = -1 << 20;
+    else smax = std::max(smax, pack_smem_bytes(rmax[c], m, kParts >> c));
+  }
+  if (n < 1 || m < 1 || m > kMaxRestart) {
     set_last_error_str("packed solve: bad sizes");
     return RF_E_INPUT;
   }
-  size_t smax = 0;
-  for (int c = 0; c < 4; ++c)
-    if (counts[c] > 0) smax = std::max(smax, pack_smem_bytes(Rmax, m, kParts >> c));
   RF_CUDA_TRY(cudaFuncSetAttribute(k_pack_gmres_ir<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
   RF_CUDA_TRY(cudaFuncSetAttribute(k_pack_gmres_ir<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
   // one launch per cluster size, the largest first; the classes after the
@@ -599,6 +608,7 @@ int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], int 
       s = lanes.aux[used - 1];
       RF_CUDA_TRY(cudaStreamWaitEvent(s, lanes.fork, 0));
     }
+    const int Rmax = rmax[c];
     if (csize == 1) {
       k_pack_gmres_ir<false><<<counts[c], kPT, pack_smem_bytes(Rmax, m, 1), s>>>(members + off, Rmax, m);
       RF_LAUNCH_CHECK();

@@ -370,7 +370,7 @@ int rf_server_config_default(rf_server_config* c) {
   // admission cost more aggregate rate (618k vs 881k fiber-steps/s on the
   // served ensemble) than it saved in launches
   c->use_cuda_graphs = 2;
-  c->pack_max_fibers = rf::kPackMaxFibers;
+  c->pack_max_fibers = rf::kPackSingleMaxFibers;
   c->pack_max_members = 148;
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c->hbm_budget_bytes = (int64_t)(0.8 * (double)fr);

@@ -32,7 +32,7 @@ def _sim(pos, ori, **kw):
 
 
 @pytest.mark.parametrize("prec", ["mixed_fp16", "mixed_bf16"])
-@pytest.mark.parametrize("n", [1, 7, 16, 33, 100, 128])
+@pytest.mark.parametrize("n", [1, 7, 16, 33, 100, 128, 200, 256])
 def test_packed_solve_matches_rf_solve_and_fp64(prec, n):
     from rigidfibers_b200.simulation import solve_packed
     pos, ori = _layout(n, 100 + n)
@@ -81,27 +81,27 @@ def test_member_is_the_same_alone_and_in_a_pack():
 
 def test_member_is_the_same_for_every_cluster_size():
     """A member's packed solve is the same bits whatever cluster the pack's
-    plan gives it: alone a 128-fiber suspension runs on 8 CTAs and a 64-fiber
-    one on 4; beside 148 other members (more members than multiprocessors)
-    each runs on one."""
+    plan gives it: alone a 128-fiber suspension runs on 8 CTAs, a 64-fiber one
+    on 4 and a 256-fiber one on 8; beside 148 other members (more members than
+    multiprocessors) the first two run on one CTA and the third on two."""
     import ctypes
     import torch
     from rigidfibers_b200 import _capi as C
     from rigidfibers_b200.simulation import solve_packed
     lib = C.load()
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    fibers = [128, 64] + [16] * max(148, sms - 1)
+    fibers = [128, 64, 256] + [16] * max(148, sms - 2)
 
     def plan(fs):
         c = (ctypes.c_int * len(fs))()
         assert lib.rf_debug_pack_plan((ctypes.c_int * len(fs))(*fs), len(fs), sms, c) == C.RF_OK
         return list(c)
 
-    assert plan([128]) == [8] and plan([64]) == [4]
-    assert plan(fibers)[:2] == [1, 1]
+    assert plan([128]) == [8] and plan([64]) == [4] and plan([256]) == [8]
+    assert plan(fibers)[:3] == [1, 1, 2]
     lays = [_layout(n, 300 + k) for k, n in enumerate(fibers)]
     alone = []
-    for k in range(2):
+    for k in range(3):
         a = _sim(*lays[k], precision="mixed_fp16")
         a.assembleSystem()
         solve_packed([a])
@@ -111,7 +111,7 @@ def test_member_is_the_same_for_every_cluster_size():
     for s in sims:
         s.assembleSystem()
     solve_packed(sims)
-    for k in range(2):
+    for k in range(3):
         assert np.array_equal(sims[k].solution(), alone[k][0]), fibers[k]
         assert sims[k].stats()["iterations"] == alone[k][1]
     for s in sims:
@@ -199,7 +199,7 @@ def test_packed_solve_refuses_what_it_does_not_take():
     with pytest.raises(C.RigidFibersError) as e:
         solve_packed([fp32])
     assert e.value.status == C.RF_E_UNSUPPORTED
-    big = _sim(*_layout(129, 6), precision="mixed_bf16")
+    big = _sim(*_layout(257, 6), precision="mixed_bf16")
     big.assembleSystem()
     with pytest.raises(C.RigidFibersError) as e:
         solve_packed([big])

@@ -145,17 +145,20 @@ def test_pack_plan_gives_large_members_clusters():
     assert plan([16] * 100, 148) == [1] * 100
     assert plan([128] * 150, 148) == [1] * 150   # more members than multiprocessors
     assert plan([128, 128], 4) == [2, 2]
+    assert plan([256], 148) == [8]
+    assert plan([200] * 150, 148) == [2] * 150   # above 128 fibers: never fewer than two CTAs
     rng = np.random.default_rng(3)
     for _ in range(50):
         n = int(rng.integers(1, 200))
         sms = int(rng.integers(1, 300))
-        fibers = [int(v) for v in rng.integers(1, 129, n)]
+        fibers = [int(v) for v in rng.integers(1, 257, n)]
         c = plan(fibers, sms)
-        assert sum(c) <= max(n, sms)
-        for f, k in zip(fibers, c):
+        least = [2 if f > 128 else 1 for f in fibers]
+        assert sum(c) <= max(sum(least), sms)
+        for f, k, k0 in zip(fibers, c, least):
             t = (f + 15) // 16
-            assert k in (1, 2, 4, 8) and (k == 1 or t * (t + 1) // 2 >= 2 * k)
-    f = (ctypes.c_int * 2)(16, 129)
+            assert k in (1, 2, 4, 8) and k >= k0 and (k == k0 or t * (t + 1) // 2 >= 2 * k)
+    f = (ctypes.c_int * 2)(16, 257)
     c = (ctypes.c_int * 2)()
     assert lib.rf_debug_pack_plan(f, 2, 148, c) == C.RF_E_INPUT
     assert lib.rf_debug_pack_plan(f, 1, 0, c) == C.RF_E_INPUT
