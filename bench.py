@@ -1,7 +1,7 @@
 """Benchmark of the rigid-fiber time step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--fibers 4000] [--radius 18] [--precision auto|fp32|mixed_fp16|mixed_bf16]
+                    [--fibers 4000] [--radius 18] [--precision auto|fp32|mixed_fp16|mixed_bf16|matrix_free|mixed_fp16_recompute]
 
 A "step" is the reference's time step (src/simulation.cu:286-329):
 assemble -> solve -> update velocities -> update fibers, on a seeded

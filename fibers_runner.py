@@ -13,7 +13,8 @@ recompilation: N, M, Q, the solver and the integration are runtime values):
 --magma selects the direct solver (the reference called MAGMA's sgesv).
 --D1/--D2/--D3 chose a CUDA thread mapping of the reference's assembly; they
 are accepted for compatibility and all run the same pair-tile kernel.
-Extra options of this build: --precision {fp32,mixed_fp16,mixed_bf16,matrix_free},
+Extra options of this build: --precision {fp32,mixed_fp16,mixed_bf16,matrix_free,
+mixed_fp16_recompute,mixed_bf16_recompute},
 --velocity-integration {same,numerical,analytical}, --output DIR.
 
 Outputs (same formats as the reference):
@@ -143,7 +144,7 @@ def validate(args):
     # tolerances relative to each field's largest magnitude; Krylov solutions
     # differ from a direct one by up to the solver tolerance
     tol = {"gmres": 1e-5, "direct": 1e-5, "bicgstab": 5e-5}[_solver(args)]
-    if args.precision in ("mixed_fp16", "mixed_bf16"):
+    if args.precision.startswith("mixed"):
         tol = 1e-4   # the 16-bit operator's bound; the matrix-free mode keeps the plain path's
     failed = []
     for t in range(2):
@@ -281,7 +282,9 @@ def build_parser():
         g.add_argument("--D1", action="store_true")
         g.add_argument("--D2", action="store_true")
         g.add_argument("--D3", action="store_true")
-        p.add_argument("--precision", default="fp32", choices=["fp32", "mixed_fp16", "mixed_bf16", "matrix_free"])
+        p.add_argument("--precision", default="fp32",
+                       choices=["fp32", "mixed_fp16", "mixed_bf16", "matrix_free", "mixed_fp16_recompute",
+                                "mixed_bf16_recompute"])
         p.add_argument("--velocity-integration", default="same", choices=["same", "numerical", "analytical"])
         p.add_argument("--output", default=".", help="directory for the output files")
         if name == "run":

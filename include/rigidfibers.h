@@ -60,8 +60,20 @@ enum rf_integration { RF_NUMERICAL = 0, RF_ANALYTICAL = 1 };
  *  RF_PREC_MATRIX_FREE: no matrix stored; every Krylov product recomputes the
  *      pair blocks (FP32, the assembly's kernel applied to the vector), for
  *      suspensions whose operator does not fit in device memory (the FP32
- *      path's GMRES / BiCGSTAB semantics; numerical integration only). */
-enum rf_precision { RF_PREC_FP32 = 0, RF_PREC_MIXED_FP16 = 1, RF_PREC_MIXED_BF16 = 2, RF_PREC_MATRIX_FREE = 3 };
+ *      path's GMRES / BiCGSTAB semantics; numerical integration only).
+ *  RF_PREC_MIXED_FP16_RECOMPUTE / _BF16_RECOMPUTE: the mixed modes with only
+ *      the 16-bit copy stored (304 bytes per fiber pair instead of 1168); the
+ *      FP64 refinement residual and the velocities recompute the FP32 blocks
+ *      from the fibers, for suspensions whose 16-bit operator fits in device
+ *      memory but whose FP32 blocks do not. */
+enum rf_precision {
+  RF_PREC_FP32 = 0,
+  RF_PREC_MIXED_FP16 = 1,
+  RF_PREC_MIXED_BF16 = 2,
+  RF_PREC_MATRIX_FREE = 3,
+  RF_PREC_MIXED_FP16_RECOMPUTE = 4,
+  RF_PREC_MIXED_BF16_RECOMPUTE = 5
+};
 
 /* Mirrors the reference's .ini keys (tests/config.ini:18-37, read by
  * runner/cuda_runner.py:18-47) plus the runtime choices the reference made

@@ -15,7 +15,8 @@ RF_OK, RF_E_INPUT, RF_E_CUDA, RF_E_OOM, RF_E_NOCONV, RF_E_NAN, RF_E_TIMEOUT, RF_
     RF_E_SINGULAR = range(10)
 SOLVERS = {"gmres": 0, "bicgstab": 1, "direct": 2, "magma": 2}
 INTEGRATIONS = {"numerical": 0, "analytical": 1}
-PRECISIONS = {"fp32": 0, "mixed_fp16": 1, "mixed_bf16": 2, "matrix_free": 3}
+PRECISIONS = {"fp32": 0, "mixed_fp16": 1, "mixed_bf16": 2, "matrix_free": 3,
+              "mixed_fp16_recompute": 4, "mixed_bf16_recompute": 5}
 
 
 class rf_config(ctypes.Structure):

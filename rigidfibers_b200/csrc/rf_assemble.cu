@@ -511,11 +511,14 @@ __device__ __forceinline__ void assemble_pair_tile(const Tables& tab, int N, con
       const int64_t rec = (L16 * S::SUB * S::SUB + sub) * TI + jl;
       // T is [q][tl] with q in (row, col) order; stored in s32_block order.
       // Pairs that do not exist (i >= N, i >= j on a diagonal tile) came out
-      // of phases 1-2 as exact zeros
-      float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
-      for (int v = tid; v < S::NQ32 * TI / 4; v += S::NT) {
-        const int q = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
-        reinterpret_cast<float4*>(d32)[v] = *reinterpret_cast<const float4*>(&sTflat[sMapS[q] * TI + g4]);
+      // of phases 1-2 as exact zeros.  No FP32 copy in the recompute modes
+      // (out.S32 null: the residual and the velocities form the blocks again)
+      if (out.S32 != nullptr) {
+        float* d32 = out.S32 + rec * (int64_t)(S::NQ32 * TI);
+        for (int v = tid; v < S::NQ32 * TI / 4; v += S::NT) {
+          const int q = v / (TI / 4), g4 = (v % (TI / 4)) * 4;
+          reinterpret_cast<float4*>(d32)[v] = *reinterpret_cast<const float4*>(&sTflat[sMapS[q] * TI + g4]);
+        }
       }
       // 16-bit records [tl][NW]: pair tl's words are contiguous; a warp stores
       // 64-byte runs of 8 records

@@ -220,6 +220,11 @@ static Tables make_tables(const rf_config& c) {
 
 using namespace rf;
 
+// 16-bit storage format of the mixed modes: 1 FP16, 2 BF16
+static int storage16(const rf_config& c) {
+  return c.precision == RF_PREC_MIXED_BF16 || c.precision == RF_PREC_MIXED_BF16_RECOMPUTE ? 2 : 1;
+}
+
 struct rf_handle {
   rf_config cfg;
   int N = 0, M = 0, Q = 0;
@@ -241,6 +246,8 @@ struct rf_handle {
   // linear system
   bool mixed = false;        // structured operator + refinement (RF_PREC_MIXED_*)
   bool mfree = false;        // no operator stored (RF_PREC_MATRIX_FREE)
+  bool recompute = false;    // mixed with the 16-bit copy only (RF_PREC_MIXED_*_RECOMPUTE)
+  float* xcast = nullptr;    // recompute: the FP32 copy of x for the residual's product
   int zparts = 0;            // matrix-free: partial-row slots of a product
   float* A = nullptr;        // dense FP32 (RF_PREC_FP32)
   float* S32 = nullptr;      // structured FP32 blocks (mixed)
@@ -394,8 +401,11 @@ static int validate_config(const rf_config* c, int N) {
   if (c->solver < 0 || c->solver > 2 || c->integration < 0 || c->integration > 1) {
     set_last_error_str("solver / integration"); return RF_E_INPUT;
   }
-  if (c->precision < RF_PREC_FP32 || c->precision > RF_PREC_MATRIX_FREE) { set_last_error_str("precision"); return RF_E_INPUT; }
-  const bool is_mixed = c->precision == RF_PREC_MIXED_FP16 || c->precision == RF_PREC_MIXED_BF16;
+  if (c->precision < RF_PREC_FP32 || c->precision > RF_PREC_MIXED_BF16_RECOMPUTE) {
+    set_last_error_str("precision");
+    return RF_E_INPUT;
+  }
+  const bool is_mixed = c->precision != RF_PREC_FP32 && c->precision != RF_PREC_MATRIX_FREE;
   if (c->precision != RF_PREC_FP32 && c->integration != RF_NUMERICAL) {
     set_last_error_str("mixed precision and the matrix-free mode use the symmetric pair blocks of numerical integration");
     return RF_E_UNSUPPORTED;
@@ -523,7 +533,8 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
     rc = h->alloc((void**)&h->tv[s], b32);
     if (!rc) rc = h->alloc((void**)&h->rv[s], b32);
   }
-  h->mixed = cfg->precision == RF_PREC_MIXED_FP16 || cfg->precision == RF_PREC_MIXED_BF16;
+  h->recompute = cfg->precision == RF_PREC_MIXED_FP16_RECOMPUTE || cfg->precision == RF_PREC_MIXED_BF16_RECOMPUTE;
+  h->mixed = cfg->precision == RF_PREC_MIXED_FP16 || cfg->precision == RF_PREC_MIXED_BF16 || h->recompute;
   h->mfree = cfg->precision == RF_PREC_MATRIX_FREE;
   const int64_t T16 = ceil_div(N, kStoreTile);
   if (h->mfree) {
@@ -534,13 +545,23 @@ static int allocate_buffers(rf_handle* h, const rf_config* cfg) {
   } else if (!h->mixed) {
     if (!rc) rc = h->alloc((void**)&h->A, (size_t)h->lda * (size_t)R * sizeof(float));
   } else {
-    if (!rc) rc = h->alloc((void**)&h->S32, (size_t)struct_floats32(h->M, N) * sizeof(float));
+    if (!h->recompute && !rc) rc = h->alloc((void**)&h->S32, (size_t)struct_floats32(h->M, N) * sizeof(float));
     if (!rc) rc = h->alloc((void**)&h->S16, (size_t)struct_words16(h->M, N) * sizeof(uint32_t));
-    // one extra row slot holds the summed partials
-    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)(T16 + 1) * (size_t)R * sizeof(float));
-    if (!rc) rc = h->alloc((void**)&h->zpart64, (size_t)(T16 + 1) * (size_t)R * sizeof(double));
+    // one extra row slot holds the summed partials; the recompute modes' residual
+    // product (launch_assemble_apply) needs one slot per assembly tile and one more
+    int64_t slots = T16 + 1;
+    if (h->recompute) {
+      h->zparts = assemble_tiles(h->M, h->Q, N) + 1;
+      slots = std::max<int64_t>(slots, h->zparts + 1);
+    }
+    if (!rc) rc = h->alloc((void**)&h->zpart, (size_t)slots * (size_t)R * sizeof(float));
+    if (!h->recompute && !rc) rc = h->alloc((void**)&h->zpart64, (size_t)(T16 + 1) * (size_t)R * sizeof(double));
     if (!rc) rc = h->alloc((void**)&h->x64, (size_t)R * sizeof(double));
-    if (!rc) rc = h->alloc((void**)&h->svpart, (size_t)T16 * N * 6 * sizeof(float));
+    if (h->recompute) {
+      if (!rc) rc = h->alloc((void**)&h->xcast, (size_t)R * sizeof(float));
+    } else if (!rc) {
+      rc = h->alloc((void**)&h->svpart, (size_t)T16 * N * 6 * sizeof(float));
+    }
   }
   if (!rc) rc = h->alloc((void**)&h->b, (size_t)R * sizeof(float));
   if (!rc) rc = h->alloc((void**)&h->x, (size_t)R * sizeof(float));
@@ -658,7 +679,8 @@ int rf_create(const rf_config* cfg, int N, const double* pos, const double* ori,
   if (h->mixed) {
     // records that the assembly never writes (fibers >= N, the lower sub-tile
     // of a diagonal storage tile) hold zeros rather than whatever the pool had
-    if (cudaMemsetAsync(h->S32, 0, (size_t)struct_floats32(h->M, N) * sizeof(float), h->st) != cudaSuccess ||
+    if ((h->S32 &&
+         cudaMemsetAsync(h->S32, 0, (size_t)struct_floats32(h->M, N) * sizeof(float), h->st) != cudaSuccess) ||
         cudaMemsetAsync(h->S16, 0, (size_t)struct_words16(h->M, N) * sizeof(uint32_t), h->st) != cudaSuccess)
       return fail(RF_E_CUDA);
   }
@@ -688,7 +710,7 @@ static int enqueue_assemble(rf_handle* h) {
                                  h->ffpart, h->F, h->b, h->st, h->asm_variant);
   if (h->mixed)
     return launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
-                                      h->cfg.precision == RF_PREC_MIXED_BF16, h->ffpart, h->F, h->b, h->st,
+                                      storage16(h->cfg) == 2, h->ffpart, h->F, h->b, h->st,
                                       h->asm_variant);
   if (h->cfg.integration == RF_ANALYTICAL)
     return launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
@@ -753,9 +775,9 @@ static MatvecFn make_matvec(rf_handle* h, int* launches) {
     ++*launches;
     int rc;
     if (h->mixed) {
-      const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+      const int smode = storage16(h->cfg);
       rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
-                                &h->ctl->timeout, st, h->mv_variant);
+                                &h->ctl->timeout, st, h->recompute ? 0 : h->mv_variant);
       *launches += 2;
     } else if (h->mfree) {
       rc = launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], xin, h->zpart, skip,
@@ -770,8 +792,18 @@ static MatvecFn make_matvec(rf_handle* h, int* launches) {
   };
 }
 
-// FP64-accumulated residual r = b - A x over the FP32 pair blocks (mixed modes)
+// FP64-accumulated residual r = b - A x over the FP32 pair blocks (mixed modes);
+// the recompute modes form the blocks again (the matrix-free product of an FP32
+// copy of x, its partial rows summed in FP64)
 static ResidualFn make_residual(rf_handle* h) {
+  if (h->recompute)
+    return [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
+      const double* x64 = static_cast<const double*>(xin);
+      RF_TRY(launch_cast_to_float(x64, h->xcast, h->R, st));
+      RF_TRY(launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->xcast, h->zpart, skip,
+                                   h->ffpart, h->F, h->b, st, h->asm_variant));
+      return launch_parts_residual64(h->tab, h->N, h->ori32, x64, h->zpart, h->zparts, h->b, r, skip, st);
+    };
   return [h](const void* xin, float* r, const int* skip, cudaStream_t st) -> int {
     return launch_struct_residual64(h->tab, h->N, h->S32, h->ori32, static_cast<const double*>(xin), h->zpart64,
                                     h->b, r, skip, &h->ctl->timeout, st);
@@ -900,7 +932,7 @@ static int enqueue_velocities(rf_handle* h, int* kernels) {
     RF_TRY(launch_velocity_analytical(h->tab, h->N, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->x,
                                       h->vpart, h->tv[h->vcur], h->rv[h->vcur], h->st));
     *kernels += 2;
-  } else if (h->mixed) {
+  } else if (h->mixed && !h->recompute) {
     RF_TRY(launch_struct_velocity(h->tab, h->N, h->S32, h->ori32, h->F, h->x, h->svpart, h->tv[h->vcur],
                                   h->rv[h->vcur], h->st));
     *kernels += 2;
@@ -1157,7 +1189,8 @@ static int pack_check(rf_handle** hs, int n, bool need_assembled, const char* wh
       set_last_error_str((std::string(who) + " before rf_assemble").c_str());
       return RF_E_STATE;
     }
-    if (!h->mixed || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 || h->N > kPackMaxFibers ||
+    if (!h->mixed || h->recompute || h->cfg.solver != RF_SOLVER_GMRES || h->M != 5 || h->tab.Q != 24 ||
+        h->N > kPackMaxFibers ||
         (h->N > kPackSingleMaxFibers && pack_max_cluster() < 2)) {
       set_last_error_str(
           (std::string(who) + ": mixed precision, GMRES, 5 force terms, 8x3 quadrature, at most 256 fibers").c_str());
@@ -1212,7 +1245,7 @@ static void pack_solve_order(rf_handle** hs, int n, std::vector<int>& pos, int (
 static void pack_member(rf_handle* h, int* out, double* relres, PackMember* q) {
   std::memset(q, 0, sizeof(*q));
   q->N = h->N;
-  q->smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+  q->smode = storage16(h->cfg);
   q->maxit = h->cfg.gmres_max_iterations;
   q->tol = h->cfg.refinement_tolerance;
   q->S16 = h->S16;
@@ -1408,7 +1441,7 @@ int rf_step_packed(rf_handle** hs, const int* timesteps, int n, int* status) {
   for (int g = 0; g < ngroups && rc == RF_OK; ++g) {
     rf_handle* hg = hs[order[(size_t)gbeg[g]]];
     rc = launch_pack_assemble(hg->tab, dsm + gbeg[g], gbeg[g + 1] - gbeg[g], asm_blocks[(size_t)g],
-                              hg->cfg.precision == RF_PREC_MIXED_BF16, st);
+                              storage16(hg->cfg) == 2, st);
     launches += 2;
   }
   RF_CUDA_TRY(cudaEventRecord(ev[1], st));
@@ -1558,7 +1591,7 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
   float* dxf = h->V;
   float* dy = h->V + ceil_div(R, 32) * 32;
   RF_CUDA_TRY(cudaMemcpyAsync(dxf, hxf.data(), R * sizeof(float), cudaMemcpyHostToDevice, h->st));
-  if (h->mfree) {
+  if (h->mfree || (h->recompute && which == 0)) {
     RF_TRY(launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], dxf, h->zpart, nullptr,
                                  h->ffpart, h->F, h->b, h->st, h->asm_variant));
     RF_TRY(launch_parts_finalize(h->tab, h->N, h->ori32, dxf, h->zpart, h->zparts, dy, nullptr, h->st));
@@ -1566,7 +1599,7 @@ int rf_operator_apply(rf_handle* h, const double* x, double* y, int which) {
     RF_TRY(launch_dense_gemv(h->gemv_plan, h->A, h->lda, R, dxf, h->ypart, nullptr, h->st));
     RF_TRY(launch_reduce_rows(h->ypart, h->gemv_plan.splits, R, dy, h->st));
   } else if (which == 1) {
-    const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+    const int smode = storage16(h->cfg);
     RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
     RF_TRY(launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, dxf, h->zpart, dy, nullptr,
                                 &h->ctl->timeout, h->st));
@@ -1769,10 +1802,10 @@ int rf_autotune(rf_handle* h, rf_tune_report* out) {
     return RF_OK;
   };
   if (h->mixed) {
-    const int smode = h->cfg.precision == RF_PREC_MIXED_BF16 ? 2 : 1;
+    const int smode = storage16(h->cfg);
     RF_CUDA_TRY(cudaMemsetAsync(&h->ctl->timeout, 0, sizeof(int), h->st));
     double best = 1e30;
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < (h->recompute ? 1 : 2); ++v) {   // the register-staged kernel reads the FP32 copy too
       const int variant = v == 0 ? 0 : 2;
       double ms = 0;
       RF_TRY(time_it([&]() {

@@ -53,6 +53,10 @@ int launch_assemble_apply(const Tables& tab, int N, const float4* pos, const flo
 // (zpart holds nparts + 1 rows: the sum goes to row nparts).
 int launch_parts_finalize(const Tables& tab, int N, const float4* ori, const float* x, float* zpart, int nparts,
                           float* y, const int* skip, cudaStream_t st);
+// r = b - (x + C z) with z the sum of nparts FP32 partial-row slots of a
+// matrix-free product (launch_assemble_apply), summed in FP64, x in FP64
+int launch_parts_residual64(const Tables& tab, int N, const float4* ori, const double* x, const float* zpart,
+                            int nparts, const float* b, float* r, const int* skip, cudaStream_t st);
 // Structured storage: S32 struct_floats32(M,N) floats, S16 struct_words16(M,N) words.
 int launch_assemble_structured(const Tables& tab, int N, const float4* pos, const float4* ori, const double4* pos64,
                                float* S32, uint32_t* S16, bool bf16, float* ffpart, float* F, float* b,

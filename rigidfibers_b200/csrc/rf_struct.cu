@@ -795,10 +795,11 @@ k_sum_parts(const ACC* part, int nparts, int64_t R, ACC* out, const int* __restr
   if (g == 0 && r < R) out[r] = ((red[0][rr] + red[1][rr]) + red[2][rr]) + red[3][rr];
 }
 
-// y = x + C z (z = sum of partials), or r = b - (x + C z).  One thread per (fiber, k).
-template <typename XT, typename ACC, bool RESIDUAL>
+// y = x + C z (z = sum of partials, added in ACC), or r = b - (x + C z).  One
+// thread per (fiber, k).
+template <typename XT, typename ACC, bool RESIDUAL, typename ZT = ACC>
 __global__ void k_struct_finalize(const Tables tab, int N, const float4* __restrict__ ori, const XT* __restrict__ x,
-                                  const ACC* __restrict__ zpart, int nparts, const float* __restrict__ b,
+                                  const ZT* __restrict__ zpart, int nparts, const float* __restrict__ b,
                                   float* __restrict__ out, const int* __restrict__ skip) {
   if (skip != nullptr && *skip) return;
   const int M = tab.M;
@@ -809,8 +810,8 @@ __global__ void k_struct_finalize(const Tables tab, int N, const float4* __restr
     const int64_t r0 = (int64_t)i * 3 * M + 3 * k;
     ACC z[3] = {0, 0, 0};
     for (int p = 0; p < nparts; ++p) {
-      const ACC* s = zpart + (int64_t)p * R + r0;
-      z[0] += s[0]; z[1] += s[1]; z[2] += s[2];
+      const ZT* s = zpart + (int64_t)p * R + r0;
+      z[0] += (ACC)s[0]; z[1] += (ACC)s[1]; z[2] += (ACC)s[2];
     }
     const float4 t = ori[i];
     const ACC t3[3] = {(ACC)t.x, (ACC)t.y, (ACC)t.z};
@@ -1084,6 +1085,15 @@ int launch_parts_finalize(const Tables& tab, int N, const float4* ori, const flo
   RF_LAUNCH_CHECK();
   k_struct_finalize<float, float, false><<<fin_blocks(n), 256, 0, st>>>(tab, N, ori, x, zpart + (int64_t)nparts * R,
                                                                         1, nullptr, y, skip);
+  RF_LAUNCH_CHECK();
+  return RF_OK;
+}
+
+int launch_parts_residual64(const Tables& tab, int N, const float4* ori, const double* x, const float* zpart,
+                            int nparts, const float* b, float* r, const int* skip, cudaStream_t st) {
+  const int64_t n = (int64_t)N * tab.M;
+  k_struct_finalize<double, double, true, float><<<fin_blocks(n), 256, 0, st>>>(tab, N, ori, x, zpart, nparts, b, r,
+                                                                                skip);
   RF_LAUNCH_CHECK();
   return RF_OK;
 }

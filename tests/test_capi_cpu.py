@@ -103,7 +103,7 @@ def test_noalloc_plan_rejects_sizes_beyond_its_scratch():
     assert lib.rf_debug_noalloc_plan(0, 148, ctypes.byref(splits), ctypes.byref(cps)) == C.RF_E_INPUT
 
 
-@pytest.mark.parametrize("field,value", [("integration", 1), ("solver", 2), ("precision", 4)])
+@pytest.mark.parametrize("field,value", [("integration", 1), ("solver", 2), ("precision", 6)])
 def test_matrix_free_mode_rejects_what_it_does_not_support(field, value):
     """The matrix-free mode recomputes the symmetric pair blocks of numerical
     integration inside GMRES or BiCGSTAB: analytical integration and the
@@ -120,6 +120,40 @@ def test_matrix_free_mode_rejects_what_it_does_not_support(field, value):
     rc = lib.rf_create(ctypes.byref(c), 1, C.ptr(pos), C.ptr(pos), ctypes.byref(h))
     assert rc in (C.RF_E_INPUT, C.RF_E_UNSUPPORTED)
     assert not h.value
+
+
+def test_recompute_modes_store_the_16_bit_copy_only():
+    """RF_PREC_MIXED_*_RECOMPUTE keep the 16-bit pair records (304 bytes per
+    unordered pair) and drop the FP32 blocks (864 bytes per pair) and the
+    structured velocity partials; they take what the mixed modes take (GMRES or
+    BiCGSTAB, numerical integration) and refuse the rest before the device is
+    touched."""
+    import numpy as np
+    lib = C.load()
+
+    def est(prec, n):
+        c = C.rf_config()
+        lib.rf_config_default(ctypes.byref(c))
+        c.precision = C.PRECISIONS[prec]
+        return lib.rf_device_bytes_estimate(ctypes.byref(c), n)
+
+    n = 2000
+    pairs = n * (n - 1) // 2
+    for p16 in ("fp16", "bf16"):
+        lean, full = est("mixed_%s_recompute" % p16, n), est("mixed_" + p16, n)
+        assert lean >= pairs * 304
+        assert full - lean >= pairs * 864 * 0.99
+        assert lean < 0.3 * full
+    for field, value in (("integration", 1), ("solver", 2), ("number_of_quadrature_intervals", 4)):
+        c = C.rf_config()
+        lib.rf_config_default(ctypes.byref(c))
+        c.precision = C.PRECISIONS["mixed_fp16_recompute"]
+        setattr(c, field, value)
+        pos = np.zeros(3)
+        h = ctypes.c_void_p()
+        rc = lib.rf_create(ctypes.byref(c), 1, C.ptr(pos), C.ptr(pos), ctypes.byref(h))
+        assert rc in (C.RF_E_INPUT, C.RF_E_UNSUPPORTED)
+        assert not h.value
 
 
 def test_matrix_free_footprint_grows_with_the_vectors_only():
