@@ -65,7 +65,8 @@ enum rf_integration { RF_NUMERICAL = 0, RF_ANALYTICAL = 1 };
  *      the 16-bit copy stored (304 bytes per fiber pair instead of 1168); the
  *      FP64 refinement residual and the velocities recompute the FP32 blocks
  *      from the fibers, for suspensions whose 16-bit operator fits in device
- *      memory but whose FP32 blocks do not. */
+ *      memory but whose FP32 blocks do not.  Each correction costs one
+ *      assembly, so these modes want a longer refinement_restart (40). */
 enum rf_precision {
   RF_PREC_FP32 = 0,
   RF_PREC_MIXED_FP16 = 1,
