@@ -84,7 +84,8 @@ def test_run_writes_json_step_log(tmp_path, golden):
 @pytest.mark.parametrize("flags", [["--gmres", "--numerical"], ["--gmres", "--analytical"], ["--bicgstab", "--numerical"],
                                    ["--gmres", "--numerical", "--precision", "mixed_fp16"],
                                    ["--bicgstab", "--numerical", "--precision", "mixed_fp16"],
-                                   ["--gmres", "--numerical", "--precision", "matrix_free"]])
+                                   ["--gmres", "--numerical", "--precision", "matrix_free"],
+                                   ["--bicgstab", "--numerical", "--precision", "mixed_bf16_recompute"]])
 def test_validate_passes_against_golden(tmp_path, golden, flags):
     ini, fib = write_inputs(tmp_path, golden)
     out = tmp_path / "v"
