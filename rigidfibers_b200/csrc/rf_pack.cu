@@ -571,15 +571,18 @@ void pack_lanes_release(PackLanes& l) {
 int launch_pack_gmres_ir(const PackMember* members, const int (&counts)[4], const int (&rmax)[4], int m,
                          cudaStream_t st, PackLanes& lanes) {
   int n = 0;
+  bool sizes_ok = m >= 1 && m <= kMaxRestart;
   size_t smax = 0;
   for (int c = 0; c < 4; ++c) {
+    if (counts[c] < 0) sizes_ok = false;
+    if (counts[c] <= 0) continue;
     n += counts[c];
-    if (counts[c] == 0) continue;
+    // one CTA holds all 8 partitions' rows: at most kPackSingleMaxFibers fibers
     const int limit = kPM3 * (c == 3 ? kPackSingleMaxFibers : kPackMaxFibers);
-    if (rmax[c] < 1 || rmax[c] > limit) n = -1 << 20;
+    if (rmax[c] < 1 || rmax[c] > limit) sizes_ok = false;
     else smax = std::max(smax, pack_smem_bytes(rmax[c], m, kParts >> c));
   }
-  if (n < 1 || m < 1 || m > kMaxRestart) {
+  if (n < 1 || !sizes_ok) {
     set_last_error_str("packed solve: bad sizes");
     return RF_E_INPUT;
   }
