@@ -248,6 +248,16 @@ typedef struct rf_tune_report {
   double asm_ms[2];         /* one assembly per candidate (-1: not tried, analytical) */
 } rf_tune_report;
 int rf_autotune(rf_handle* h, rf_tune_report* report);
+/* Near-field preconditioner (no reference counterpart: the reference's
+ * GMRES runs unpreconditioned).  neighbours = k in [1, 8]: at every assembly
+ * each fiber's k nearest fibers (centre distance) form a small block of the
+ * system from the stored FP32 blocks, and the solve applies each fiber's rows
+ * of that block's inverse on the right (flexible GMRES: the convergence tests
+ * see the true residual, so the tolerance means what it means without it).
+ * 0 turns it off (the default).  Stored mixed modes (not the recompute ones),
+ * GMRES, 5 force terms; RF_E_UNSUPPORTED otherwise.  Takes effect at the next
+ * rf_assemble. */
+int rf_set_near_field_preconditioner(rf_handle* h, int neighbours);
 /* Select the numerical assembly's pair-tile kernel by hand (the asm_variant
  * values of rf_tune_report); the operator is the same bit for bit either way.
  * RF_E_INPUT for an unknown variant. */

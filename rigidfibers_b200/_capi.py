@@ -152,6 +152,7 @@ SIGNATURES = {
     "rf_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "rf_set_profiling": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_cuda_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
+    "rf_set_near_field_preconditioner": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_assembly_variant": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_prepare_step_graphs": (ctypes.c_int, [_H, ctypes.c_int]),
     "rf_set_host_wait": (ctypes.c_int, [_H, ctypes.c_int]),

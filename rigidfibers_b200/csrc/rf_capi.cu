@@ -248,6 +248,13 @@ struct rf_handle {
   bool mfree = false;        // no operator stored (RF_PREC_MATRIX_FREE)
   bool recompute = false;    // mixed with the 16-bit copy only (RF_PREC_MIXED_*_RECOMPUTE)
   float* xcast = nullptr;    // recompute: the FP32 copy of x for the residual's product
+  // near-field preconditioner (rf_set_near_field_preconditioner): neighbours per
+  // fiber (0: off), neighbour lists, the fibers' rows of the neighbourhood
+  // inverses, and the preconditioned basis z_j of flexible GMRES
+  int nf_k = 0;
+  int* nf_nb = nullptr;
+  float* nf_w = nullptr;
+  float* nf_z = nullptr;
   int zparts = 0;            // matrix-free: partial-row slots of a product
   float* A = nullptr;        // dense FP32 (RF_PREC_FP32)
   float* S32 = nullptr;      // structured FP32 blocks (mixed)
@@ -708,10 +715,15 @@ static int enqueue_assemble(rf_handle* h) {
   if (h->mfree)   // the force terms and b (the products recompute the blocks)
     return launch_assemble_apply(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], nullptr, h->zpart, nullptr,
                                  h->ffpart, h->F, h->b, h->st, h->asm_variant);
-  if (h->mixed)
-    return launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
+  if (h->mixed) {
+    RF_TRY(launch_assemble_structured(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->S32, h->S16,
                                       storage16(h->cfg) == 2, h->ffpart, h->F, h->b, h->st,
-                                      h->asm_variant);
+                                      h->asm_variant));
+    // the preconditioner's blocks come from this step's FP32 records
+    if (h->nf_k > 0)
+      return launch_nf_setup(h->tab, h->N, h->nf_k, h->pos32, h->ori32, h->S32, h->nf_nb, h->nf_w, h->st);
+    return RF_OK;
+  }
   if (h->cfg.integration == RF_ANALYTICAL)
     return launch_assemble_analytical(h->tab, h->N, h->pos32, h->ori32, h->pos64[h->icur], h->ori64[h->icur], h->A,
                                       h->lda, h->ffpart, h->F, h->b, h->st);
@@ -738,6 +750,7 @@ static GmresSetup gmres_setup(rf_handle* h) {
   s.tol = h->mixed ? h->cfg.refinement_tolerance : h->cfg.gmres_tolerance;
   s.V = h->V;
   s.ldv = ceil_div(h->R, 32) * 32;
+  s.Z = h->nf_k > 0 ? h->nf_z : nullptr;
   s.ypart = h->ypart;
   s.nsplit = h->gemv_plan.splits;
   s.part = h->part;
@@ -776,7 +789,19 @@ static MatvecFn make_matvec(rf_handle* h, int* launches) {
     int rc;
     if (h->mixed) {
       const int smode = storage16(h->cfg);
-      rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xin, h->zpart, h->ypart, skip,
+      // flexible GMRES: the product of basis column j is A z_j with z_j = P v_j
+      // kept for the solution update (other vectors get the plain product)
+      const int64_t ldv = ceil_div(h->R, 32) * 32;
+      const int64_t off = ((intptr_t)xin - (intptr_t)h->V) / (int64_t)sizeof(float);
+      const float* xa = xin;
+      if (h->nf_k > 0 && (intptr_t)xin >= (intptr_t)h->V && off % ldv == 0 && off / ldv <= h->restart) {
+        float* zj = h->nf_z + off;
+        rc = launch_nf_apply(h->N, h->nf_k, h->nf_nb, h->nf_w, xin, zj, skip, st);
+        if (rc != RF_OK) return rc;
+        xa = zj;
+        ++*launches;
+      }
+      rc = launch_struct_matvec(h->tab, h->N, smode, h->S32, h->S16, h->ori32, xa, h->zpart, h->ypart, skip,
                                 &h->ctl->timeout, st, h->recompute ? 0 : h->mv_variant);
       *launches += 2;
     } else if (h->mfree) {
@@ -1885,6 +1910,32 @@ int rf_debug_set_device_wait_limit(int64_t limit) {
 int rf_debug_fail_allocation_after(int n) {
   if (n < -1) return RF_E_INPUT;
   g_fail_alloc_after.store(n);
+  return RF_OK;
+}
+
+int rf_set_near_field_preconditioner(rf_handle* h, int neighbours) {
+  if (!h || neighbours < 0 || neighbours > kNfMaxNeighbours) return RF_E_INPUT;
+  if (neighbours > 0 && (!h->mixed || h->recompute || h->M != 5 || h->cfg.solver != RF_SOLVER_GMRES)) {
+    set_last_error_str("the near-field preconditioner needs a stored mixed mode, GMRES and 5 force terms");
+    return RF_E_UNSUPPORTED;
+  }
+  if (neighbours > 0) {
+    const int64_t ldv = ceil_div(h->R, 32) * 32;
+    int rc = RF_OK;
+    if (!h->nf_nb) rc = h->alloc((void**)&h->nf_nb, (size_t)h->N * (kNfMaxNeighbours + 1) * sizeof(int));
+    if (!rc && !h->nf_w) rc = h->alloc((void**)&h->nf_w, (size_t)nf_w_floats(h->N) * sizeof(float));
+    if (!rc && !h->nf_z) rc = h->alloc((void**)&h->nf_z, (size_t)(h->restart + 1) * ldv * sizeof(float));
+    if (rc) return rc;
+    h->stats.device_bytes = h->device_bytes;
+  }
+  if (neighbours != h->nf_k) {
+    // captured cycles and steps hold the old launch parameters; the blocks of
+    // the current system are formed at the next rf_assemble
+    h->gmres_graphs.release();
+    h->release_step_graphs();
+    h->assembled = h->solved = false;
+  }
+  h->nf_k = neighbours;
   return RF_OK;
 }
 

@@ -85,6 +85,17 @@ int launch_struct_velocity(const Tables& tab, int N, const float* S32, const flo
                            const float* x, float* vpart, float4* tvel, float4* rvel, cudaStream_t st);
 int launch_cast_to_float(const double* in, float* out, int64_t n, cudaStream_t st);
 
+// Near-field preconditioner (csrc/rf_precond.cu; M = 5, stored FP32 blocks):
+// nb (N x (k+1) ints) the k nearest fibers of each fiber, W (nf_w_floats(N)
+// floats) each fiber's rows of the inverse of its neighbourhood block; the
+// apply writes z = P v (every row).
+constexpr int kNfMaxNeighbours = 8;
+int64_t nf_w_floats(int N);
+int launch_nf_setup(const Tables& tab, int N, int k, const float4* pos, const float4* ori, const float* S32, int* nb,
+                    float* W, cudaStream_t st);
+int launch_nf_apply(int N, int k, const int* nb, const float* W, const float* v, float* z, const int* skip,
+                    cudaStream_t st);
+
 // Packed mixed-precision solves (csrc/rf_pack.cu): one thread-block cluster
 // per suspension of at most kPackMaxFibers fibers, M = 5, Q = 24 storage.
 constexpr int kPackMaxFibers = 256;

@@ -205,6 +205,7 @@ struct GmresArgs {
   void* x;             // float or double (x_double)
   int x_double;
   float* V;            // (m+1) x ldv
+  const float* Z;      // basis of the solution update (V, or the preconditioned z_j)
   int64_t ldv;
   int64_t R;
   int m;
@@ -361,7 +362,7 @@ __global__ void k_gmres_update(GmresArgs a) {
   __syncthreads();
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < a.R; r += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int k = 0; k < jc; ++k) s += y[k] * f2d(a.V[(int64_t)k * a.ldv + r]);
+    for (int k = 0; k < jc; ++k) s += y[k] * f2d(a.Z[(int64_t)k * a.ldv + r]);
     if (a.x_double) {
       double* x = static_cast<double*>(a.x);
       x[r] += s;
@@ -428,6 +429,7 @@ int gmres_solve_ex(const GmresSetup& s, const MatvecFn& matvec, const ResidualFn
   a.x = x;
   a.x_double = x_double ? 1 : 0;
   a.V = s.V;
+  a.Z = s.Z ? s.Z : s.V;
   a.ldv = s.ldv;
   a.R = s.R;
   a.m = m;
@@ -618,6 +620,7 @@ static GmresArgs gmres_args(const GmresSetup& s, const float* b, void* x, bool x
   a.x = x;
   a.x_double = x_double ? 1 : 0;
   a.V = s.V;
+  a.Z = s.Z ? s.Z : s.V;
   a.ldv = s.ldv;
   a.R = s.R;
   a.m = s.m;

@@ -59,6 +59,9 @@ struct GmresSetup {
   double tol;
   float* V;            // (m+1) x ldv
   int64_t ldv;
+  // right-preconditioned (flexible) GMRES: the matvec of column j stores
+  // z_j = P v_j here and the solution update reads it; null: x += V y
+  const float* Z = nullptr;
   const float* ypart;  // written by the matvec
   int nsplit;
   double* part;        // 3 * coop_blocks * (kMaxRestart + 2)

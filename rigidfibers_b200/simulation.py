@@ -177,6 +177,13 @@ class Simulation:
         3 both; rf_prepare_step_graphs) instead of on a step's second use."""
         C.check(self._lib.rf_prepare_step_graphs(self._h, int(which)), "rf_prepare_step_graphs")
 
+    def set_near_field_preconditioner(self, neighbours):
+        """Right-precondition the solve with each fiber's rows of the inverse
+        of its neighbourhood block (k nearest fibers, 1..8; 0 off;
+        rf_set_near_field_preconditioner); takes effect at the next assembly."""
+        C.check(self._lib.rf_set_near_field_preconditioner(self._h, int(neighbours)),
+                "rf_set_near_field_preconditioner")
+
     def set_cuda_graphs(self, mode):
         """0: no CUDA graphs; 1: each rf_step one graph (default); 2: graphs for
         the GMRES restart cycles only, so that the stage times are measured."""
